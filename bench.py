@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark of the semi-analytic E_l assembly (pair-integrals/s).
+
+Workload: unit icosphere subdivided 3x (1280 triangles, 3840 unknowns per
+step), rho=1, mu=1, lambda=1, dt=0.025, T=1 (Nt=40, L=40 Toeplitz blocks),
+7-point outer Gauss-Hammer rule, plain FP64.  One step = assembly of
+E_0..E_39 (26.1 M non-null pair-lags, 4.7 GB of output, far larger than L2).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) each rank assembles a row panel of source triangles
+(no data-path collective); the job value is all ranks' pair-integrals over
+the slowest rank's device time.  ``--impl reference`` times the CPU
+restatement of the reference's MATLAB path (the oracle) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "E_l assembly pair-integrals/s (plain FP64 SA, sphere N=1280, L=40, GH7)"
+UNIT = "pair-integrals/s"
+
+# FP64 operation census of the SA path (oracle compiled with a counting
+# scalar; +,-,*,/,sqrt and each transcendental = 1 flop), on 5000 seeded
+# pairs of this workload: flops per non-null pair-lag when every time level
+# is evaluated once (the schedule the kernel runs), and under the
+# reference's three-instants-per-lag schedule.
+FLOPS_PER_PAIR_INTEGRAL = 19_232.0
+FLOPS_PER_PAIR_INTEGRAL_REF_SCHEDULE = 53_560.0
+
+# DRAM bytes per launch of sa_assemble_kernel from ncu (None until captured)
+NCU_TRAFFIC_PER_LAUNCH = None
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# --------------------------------------------------------------------------
+def fp64_peak_tflops(torch) -> float:
+    """Measured FP64 throughput: cuBLAS DGEMM (torch.matmul, float64,
+    8192^3, 2 n^3 flops), best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n ** 3 / best / 1e12
+
+
+def cpu_baseline(workload, target_s: float = 12.0, nthreads: int = 0):
+    """The oracle (C++ restatement of the reference's SA path, the reference's
+    three-instants-per-lag schedule) on a seeded sample of non-null pair-lags
+    of the same workload, all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    m, prm = workload.mesh, workload.params
+    L = O.num_blocks(m, prm)
+    N = m.numberTriangles
+    rng = np.random.default_rng(11)
+    ctr, ml = m.center, m.maxL
+
+    def sample(q):
+        src = rng.integers(0, N, 4 * q)
+        fld = rng.integers(0, N, 4 * q)
+        lag = rng.integers(0, L, 4 * q)
+        d = np.linalg.norm(ctr[fld] - ctr[src], axis=1)
+        ok = ((lag - 1) * prm.velS * prm.dt < d + ml[fld] + ml[src]) & \
+             ((lag + 1) * prm.velP * prm.dt >= d - ml[fld] - ml[src])
+        return src[ok][:q], fld[ok][:q], lag[ok][:q]
+    cores = os.cpu_count() if nthreads <= 0 else nthreads
+    s, f, l = sample(20000)
+    t0 = time.perf_counter()
+    O.assemble_sa_pairs(m, prm, workload.n_gh, s, f, l, nthreads=cores)
+    t1 = time.perf_counter()
+    q = int(min(5_000_000, max(20000, len(s) * target_s / max(t1 - t0, 1e-3))))
+    s, f, l = sample(q)
+    t0 = time.perf_counter()
+    O.assemble_sa_pairs(m, prm, workload.n_gh, s, f, l, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": len(s) / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(s)} seeded non-null (source, field, lag) blocks of the sphere N=1280 GH7 workload, "
+                      f"oracle (C++ restatement of BEMenerg_coreSA_calcMatrixSubBlock, 3 instants per lag), "
+                      f"{dt:.1f} s"}
+
+
+def reference_arm(args, rank: int):
+    from elastodynamicebem_b200 import problem
+    if rank != 0:
+        return
+    w = problem.sphere_workload(7)
+    vals = []
+    info = None
+    for _ in range(args.warmup):
+        cpu_baseline(w, target_s=2.0)
+    for _ in range(args.steps):
+        info = cpu_baseline(w, target_s=8.0)
+        vals.append(info["value"])
+    v = statistics.median(vals)
+    info["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "sphere_icosphere3_N1280_L40_GH7", "N": 1280, "L": 40, "n_gh": 7},
+            "cpu_baseline": info,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warning: fewer than 3 warm-up steps")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
+
+    from elastodynamicebem_b200 import core, problem
+
+    w = problem.sphere_workload(7)
+    m, prm = w.mesh, w.params
+    N = m.numberTriangles
+    src0 = rank * N // world
+    nsrc = (rank + 1) * N // world - src0
+    dm = core.DeviceMesh(m)
+    L = core.num_blocks(dm, prm)
+    n3 = 3 * N
+    out = torch.empty((L, n3, 3 * nsrc), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step(count=False):
+        return core.assemble_sa_panel(dm, prm, w.n_gh, 0, L, src0, nsrc, out=out, stream=stream, count=count)
+
+    _, my_pairs = step(count=True)
+    total_pairs = my_pairs
+    if world > 1:
+        t = torch.tensor([my_pairs], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        total_pairs = int(t.item())
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    sampler = ClockSampler(local_rank if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
+    sampler.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    my_s = ev0.elapsed_time(ev1) / 1e3
+    t_max = my_s
+    if world > 1:
+        t = torch.tensor([my_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = total_pairs * args.steps / t_max
+    kernel_s = my_s / args.steps          # one sa_assemble_kernel launch per step
+
+    # end to end through the C ABI with host buffers: mesh upload, assembly,
+    # copy of E to pinned host memory, every step
+    host = torch.empty((L, n3, 3 * nsrc), dtype=torch.float64).pin_memory()
+    h2d = m.coordinates.nbytes + m.triangles.astype(np.int32).nbytes
+    d2h = host.numel() * 8
+    e2e_times = []
+    for s in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        dme = core.DeviceMesh(m)
+        core.assemble_sa_panel(dme, prm, w.n_gh, 0, L, src0, nsrc, out=host)
+        dme.close()
+        dt = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        if s > 0:
+            e2e_times.append(dt)
+    e2e_value = total_pairs / statistics.median(e2e_times) if e2e_times else None
+
+    if rank == 0:
+        peak = fp64_peak_tflops(torch)
+        achieved = FLOPS_PER_PAIR_INTEGRAL * my_pairs / kernel_s / 1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "sphere_icosphere3_N1280_L40_GH7", "N": N, "L": L, "n_gh": w.n_gh,
+                       "rho": prm.rho, "mu": prm.mu, "lambda": prm.lam, "dt": prm.dt, "nT": prm.nT,
+                       "pair_integrals_per_step": total_pairs, "parallelism": f"source-row panels x{world}",
+                       "l2": "output 4.7 GB per step written to HBM, far larger than L2"},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak,
+                         "traffic": NCU_TRAFFIC_PER_LAUNCH,
+                         "peak_source": "measured: cuBLAS DGEMM 8192^3 via torch.matmul float64, best of 5",
+                         "flops_per_unit": FLOPS_PER_PAIR_INTEGRAL,
+                         "units_per_launch": my_pairs,
+                         "kernel": "sa_assemble_kernel", "kernel_ms": kernel_s * 1e3},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "path": "ebem_mesh_create + ebem_assemble_sa_panel into pinned host memory + ebem_mesh_destroy"},
+            "clocks": clocks,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(w)
+        print(json.dumps(line), flush=True)
+    del out, host
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

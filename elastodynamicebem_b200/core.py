@@ -1,0 +1,118 @@
+"""Device-side operators over the C ABI.
+
+torch provides device memory and streams here; every compute step is a
+libebem kernel reached through ctypes with plain pointers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import lib as _lib
+from .mesh import Mesh
+from .problem import ProblemParams
+
+
+def _stream_ptr(stream) -> int:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return int(stream.cuda_stream)
+
+
+class DeviceMesh:
+    """A mesh uploaded to the current CUDA device (an ``ebem_mesh`` handle)."""
+
+    def __init__(self, mesh: Mesh):
+        L = _lib.load()
+        self.mesh = mesh
+        self._h = C.c_void_p()
+        coords = np.ascontiguousarray(mesh.coordinates, np.float64)
+        tris = np.ascontiguousarray(mesh.triangles, np.int32)
+        _lib.check(L.ebem_mesh_create(coords.ctypes.data, mesh.number_nodes, tris.ctypes.data,
+                                      mesh.numberTriangles, C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def N(self) -> int:
+        return self.mesh.numberTriangles
+
+    def derived(self):
+        N = self.N
+        n = np.zeros((N, 3)); a = np.zeros(N); c = np.zeros((N, 3)); m = np.zeros(N)
+        _lib.check(_lib.load().ebem_mesh_derived(self._h, n.ctypes.data, a.ctypes.data, c.ctypes.data, m.ctypes.data))
+        return n, a, c, m
+
+    def close(self):
+        if self._h:
+            _lib.load().ebem_mesh_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def quad_gh(n_nodes: int, n_sub: int = 1):
+    nodes = np.zeros((n_sub * n_nodes, 3))
+    w = np.zeros(n_nodes)
+    _lib.check(_lib.load().ebem_quad_gh(n_nodes, n_sub, nodes.ctypes.data, w.ctypes.data))
+    return nodes, w
+
+
+def num_blocks(dmesh: DeviceMesh, prm: ProblemParams) -> int:
+    L = C.c_int()
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_num_blocks(dmesh.handle, C.byref(p), C.byref(L)))
+    return int(L.value)
+
+
+def assemble_sa(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, lag0: int = 0, nlag: int | None = None,
+                out: torch.Tensor | None = None, accumulate: bool = False, stream=None, count: bool = False):
+    """E_lag0..E_{lag0+nlag-1} on the device.
+
+    Returns a tensor ``E`` of shape (nlag, 3N, 3N) with ``E[l][row, col]``
+    (a transposed view of the column-major C-ABI buffer), and the number of
+    non-null pair-lags when ``count`` is set.
+    """
+    if nlag is None:
+        nlag = num_blocks(dmesh, prm) - lag0
+    n3 = 3 * dmesh.N
+    if out is None:
+        out = torch.empty((nlag, n3, n3), dtype=torch.float64, device="cuda")
+    if out.dtype != torch.float64 or not out.is_contiguous() or out.numel() != nlag * n3 * n3:
+        raise ValueError("out must be a contiguous float64 tensor of nlag*(3N)^2 elements")
+    p = _lib.problem_struct(prm)
+    cnt = C.c_longlong(0)
+    _lib.check(_lib.load().ebem_assemble_sa(dmesh.handle, C.byref(p), int(n_gh), int(lag0), int(nlag),
+                                            out.data_ptr(), int(bool(accumulate)),
+                                            _stream_ptr(stream) if out.is_cuda else None,
+                                            C.byref(cnt) if count else None))
+    E = out.view(nlag, n3, n3).transpose(1, 2)
+    return (E, int(cnt.value)) if count else E
+
+
+def assemble_sa_panel(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, lag0: int, nlag: int, src0: int, nsrc: int,
+                      out: torch.Tensor | None = None, accumulate: bool = False, stream=None, count: bool = False):
+    """Source-row panel [src0, src0+nsrc) of E_lag0..: a buffer of nlag x 3N x
+    3 nsrc doubles (column-major per lag, leading dimension 3 nsrc).  Returns
+    ``(out, nonnull)`` when ``count`` is set, else ``out``."""
+    n3 = 3 * dmesh.N
+    if out is None:
+        out = torch.empty((nlag, n3, 3 * nsrc), dtype=torch.float64, device="cuda")
+    if out.dtype != torch.float64 or not out.is_contiguous() or out.numel() != nlag * n3 * 3 * nsrc:
+        raise ValueError("out must be a contiguous float64 tensor of nlag*3N*3nsrc elements")
+    p = _lib.problem_struct(prm)
+    cnt = C.c_longlong(0)
+    _lib.check(_lib.load().ebem_assemble_sa_panel(dmesh.handle, C.byref(p), int(n_gh), int(lag0), int(nlag),
+                                                  int(src0), int(nsrc), out.data_ptr(), 3 * int(nsrc),
+                                                  int(bool(accumulate)),
+                                                  _stream_ptr(stream) if out.is_cuda else None,
+                                                  C.byref(cnt) if count else None))
+    return (out, int(cnt.value)) if count else out

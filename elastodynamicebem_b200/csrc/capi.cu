@@ -1,0 +1,291 @@
+// C-ABI entry points of libebem (declared in include/ebem.h): argument
+// checking, device-resident mesh handles, host/device output staging and the
+// thread-local error message.  Every compute step runs as a CUDA kernel; a
+// call with no visible CUDA device fails with EBEM_ERR_NODEVICE (there is no
+// CPU path).
+#include "ebem_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+struct ebem_mesh {
+    ebem::MeshData d;
+};
+
+namespace ebem {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+PhysParams phys_from(const ebem_problem* p) {
+    PhysParams P;
+    P.rho = p->rho;
+    P.velP = std::sqrt((p->lambda + 2 * p->mu) / p->rho);
+    P.velS = std::sqrt(p->mu / p->rho);
+    P.dt = p->tfin / p->nt;
+    P.nT = p->nt;
+    return P;
+}
+
+namespace {
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+        else prev = -1;
+    }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+int check_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(EBEM_ERR_NODEVICE, "no CUDA device visible");
+    }
+    return EBEM_OK;
+}
+
+int check_problem(const ebem_problem* p) {
+    if (!p) return fail(EBEM_ERR_INVALID, "problem is NULL");
+    if (!(p->rho > 0) || !(p->mu > 0) || !(p->lambda + 2 * p->mu > 0))
+        return fail(EBEM_ERR_INVALID, "material parameters must give rho > 0, mu > 0, lambda + 2 mu > 0");
+    if (!(p->tfin > 0) || p->nt < 1) return fail(EBEM_ERR_INVALID, "need tfin > 0 and nt >= 1");
+    return EBEM_OK;
+}
+
+bool is_device_ptr(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+__global__ void max_vertex_dist_kernel(const double* __restrict__ c, int nv, unsigned long long* out) {
+    // max over vertex pairs of |P_a - P_b| (calcNumBlocks.m:8-14); distances
+    // are non-negative, so their IEEE bit patterns order like the values
+    double best = 0.0;
+    long long total = (long long)nv * nv;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        int a = (int)(q / nv), b = (int)(q % nv);
+        double v0 = c[3 * a] - c[3 * b], v1 = c[3 * a + 1] - c[3 * b + 1], v2 = c[3 * a + 2] - c[3 * b + 2];
+        double d = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        best = fmax(best, d);
+    }
+    for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(best));
+}
+
+}  // namespace
+}  // namespace ebem
+
+using namespace ebem;
+
+extern "C" {
+
+int ebem_version(void) { return EBEM_VERSION; }
+
+const char* ebem_last_error(void) { return g_last_error.c_str(); }
+
+int ebem_quad_gh(int n_nodes, int n_sub, double* nodes, double* weights) {
+    if (!nodes || !weights) return fail(EBEM_ERR_INVALID, "NULL output");
+    int rc = gh_composite(n_nodes, n_sub, nodes, weights);
+    if (rc) return fail(rc, "unsupported Gauss-Hammer rule (n_nodes in {1,3,7,12,19,28}, n_sub a square >= 1)");
+    return EBEM_OK;
+}
+
+int ebem_mesh_create(const double* coords, int n_vertices, const int32_t* tris, int n_triangles, ebem_mesh** out) {
+    if (!out) return fail(EBEM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!coords || !tris || n_vertices < 3 || n_triangles < 1)
+        return fail(EBEM_ERR_INVALID, "mesh needs >= 3 vertices and >= 1 triangle");
+    for (long long k = 0; k < 3LL * n_triangles; k++)
+        if (tris[k] < 0 || tris[k] >= n_vertices) return fail(EBEM_ERR_INVALID, "triangle vertex index out of range");
+    for (long long k = 0; k < 3LL * n_vertices; k++)
+        if (!std::isfinite(coords[k])) return fail(EBEM_ERR_INVALID, "non-finite vertex coordinate");
+    for (int t = 0; t < n_triangles; t++) {
+        const int32_t* v = tris + 3 * t;
+        if (v[0] == v[1] || v[1] == v[2] || v[0] == v[2]) return fail(EBEM_ERR_INVALID, "degenerate triangle (repeated vertex)");
+    }
+    if (int rc = check_device()) return rc;
+    ebem_mesh* m = new ebem_mesh();
+    cudaGetDevice(&m->d.device);
+    m->d.nv = n_vertices;
+    m->d.nt = n_triangles;
+    auto cleanup = [&](int code, const char* msg) {
+        ebem_mesh_destroy(m);
+        return fail(code, msg);
+    };
+    if (cudaMalloc(&m->d.d_coords, sizeof(double) * 3 * (size_t)n_vertices) != cudaSuccess ||
+        cudaMalloc(&m->d.d_tris, sizeof(int32_t) * 3 * (size_t)n_triangles) != cudaSuccess ||
+        cudaMalloc(&m->d.d_geo, sizeof(TriGeom) * (size_t)n_triangles) != cudaSuccess) {
+        cudaGetLastError();
+        return cleanup(EBEM_ERR_NOMEM, "device allocation failed");
+    }
+    if (cudaMemcpy(m->d.d_coords, coords, sizeof(double) * 3 * (size_t)n_vertices, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(m->d.d_tris, tris, sizeof(int32_t) * 3 * (size_t)n_triangles, cudaMemcpyHostToDevice) != cudaSuccess)
+        return cleanup(EBEM_ERR_CUDA, "mesh upload failed");
+    if (prep_mesh(m->d, 0) != EBEM_OK) { std::string e = g_last_error; ebem_mesh_destroy(m); return fail(EBEM_ERR_CUDA, e); }
+    if (cudaDeviceSynchronize() != cudaSuccess) return cleanup(EBEM_ERR_CUDA, "mesh preparation kernel failed");
+    // reject zero-area triangles (the frame would divide by zero)
+    std::vector<TriGeom> g(n_triangles);
+    if (cudaMemcpy(g.data(), m->d.d_geo, sizeof(TriGeom) * n_triangles, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return cleanup(EBEM_ERR_CUDA, "mesh download failed");
+    for (int t = 0; t < n_triangles; t++)
+        if (!(g[t].area > 0) || !std::isfinite(g[t].area)) return cleanup(EBEM_ERR_INVALID, "zero-area triangle in mesh");
+    *out = m;
+    return EBEM_OK;
+}
+
+int ebem_mesh_destroy(ebem_mesh* m) {
+    if (!m) return EBEM_OK;
+    DeviceGuard dg(m->d.device);
+    if (m->d.d_coords) cudaFree(m->d.d_coords);
+    if (m->d.d_tris) cudaFree(m->d.d_tris);
+    if (m->d.d_geo) cudaFree(m->d.d_geo);
+    if (m->d.d_nodes) cudaFree(m->d.d_nodes);
+    delete m;
+    return EBEM_OK;
+}
+
+int ebem_mesh_info(const ebem_mesh* m, int* nv, int* nt) {
+    if (!m) return fail(EBEM_ERR_INVALID, "mesh is NULL");
+    if (nv) *nv = m->d.nv;
+    if (nt) *nt = m->d.nt;
+    return EBEM_OK;
+}
+
+int ebem_mesh_derived(const ebem_mesh* m, double* normal, double* area, double* center, double* maxl) {
+    if (!m) return fail(EBEM_ERR_INVALID, "mesh is NULL");
+    DeviceGuard dg(m->d.device);
+    std::vector<TriGeom> g(m->d.nt);
+    EBEM_CUDA_TRY(cudaMemcpy(g.data(), m->d.d_geo, sizeof(TriGeom) * m->d.nt, cudaMemcpyDeviceToHost));
+    for (int t = 0; t < m->d.nt; t++) {
+        for (int c = 0; c < 3; c++) {
+            if (normal) normal[3 * t + c] = g[t].n[c];
+            if (center) center[3 * t + c] = g[t].ctr[c];
+        }
+        if (area) area[t] = g[t].area;
+        if (maxl) maxl[t] = g[t].maxL;
+    }
+    return EBEM_OK;
+}
+
+int ebem_num_blocks(const ebem_mesh* m, const ebem_problem* p, int* num_blocks) {
+    if (!m || !num_blocks) return fail(EBEM_ERR_INVALID, "NULL argument");
+    if (int rc = check_problem(p)) return rc;
+    DeviceGuard dg(m->d.device);
+    unsigned long long* d = nullptr;
+    EBEM_CUDA_TRY(cudaMalloc(&d, sizeof(unsigned long long)));
+    EBEM_CUDA_TRY(cudaMemset(d, 0, sizeof(unsigned long long)));
+    max_vertex_dist_kernel<<<296, 256>>>(m->d.d_coords, m->d.nv, d);
+    unsigned long long bits = 0;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, cudaGetErrorString(e));
+    double maxD;
+    std::memcpy(&maxD, &bits, sizeof(double));
+    PhysParams P = phys_from(p);
+    long long maxInd = (long long)std::ceil(maxD / (P.velS * P.dt)) + 1;
+    *num_blocks = (int)std::min<long long>(p->nt, maxInd);
+    return EBEM_OK;
+}
+
+static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, int lag0, int nlag, int src0,
+                         int nsrc, double* E, long long ld, int accumulate, void* stream, long long* nonnull) {
+    if (!m || !E) return fail(EBEM_ERR_INVALID, "NULL mesh or output");
+    if (int rc = check_problem(p)) return rc;
+    if (n_gh != 3 && n_gh != 7 && n_gh != 12 && n_gh != 19)
+        return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+    if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
+    if (src0 < 0 || nsrc < 1 || src0 + nsrc > m->d.nt) return fail(EBEM_ERR_INVALID, "source panel outside the mesh");
+    if (ld < 3LL * nsrc) return fail(EBEM_ERR_INVALID, "leading dimension smaller than 3 nsrc");
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MeshData& md = const_cast<MeshData&>(m->d);
+    if (int rc = map_nodes(md, n_gh, s)) return rc;
+    PhysParams P = phys_from(p);
+    const size_t n3 = 3 * (size_t)md.nt;
+    const size_t lag_elems = (size_t)ld * n3;
+    unsigned long long* d_count = nullptr;
+    if (nonnull) {
+        EBEM_CUDA_TRY(cudaMalloc(&d_count, sizeof(unsigned long long)));
+        EBEM_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
+    }
+    int rc = EBEM_OK;
+    if (is_device_ptr(E)) {
+        rc = launch_sa_assemble(md, P, n_gh, lag0, nlag, src0, nsrc, E, (size_t)ld, lag_elems, accumulate, d_count, s);
+    } else {
+        if (ld != 3LL * nsrc) {
+            if (d_count) cudaFree(d_count);
+            return fail(EBEM_ERR_INVALID, "host output needs ld == 3 nsrc");
+        }
+        // host output: assemble chunks of lags in device memory and copy back
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        size_t per_lag = lag_elems * sizeof(double);
+        size_t budget = std::max<size_t>(per_lag, std::min<size_t>(free_b / 2, (size_t)16 << 30));
+        int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nlag, budget / per_lag));
+        double* d_buf = nullptr;
+        if (cudaMalloc(&d_buf, per_lag * chunk) != cudaSuccess) {
+            cudaGetLastError();
+            if (d_count) cudaFree(d_count);
+            return fail(EBEM_ERR_NOMEM, "device staging buffer allocation failed");
+        }
+        for (int q0 = 0; q0 < nlag && rc == EBEM_OK; q0 += chunk) {
+            int nq = std::min(chunk, nlag - q0);
+            double* hE = E + (size_t)q0 * lag_elems;
+            if (accumulate &&
+                cudaMemcpyAsync(d_buf, hE, per_lag * nq, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+                rc = fail(EBEM_ERR_CUDA, "upload failed");
+                break;
+            }
+            rc = launch_sa_assemble(md, P, n_gh, lag0 + q0, nq, src0, nsrc, d_buf, (size_t)ld, lag_elems, accumulate,
+                                    d_count, s);
+            if (rc) break;
+            if (cudaMemcpyAsync(hE, d_buf, per_lag * nq, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+                rc = fail(EBEM_ERR_CUDA, "download failed");
+                break;
+            }
+        }
+        cudaError_t e = cudaStreamSynchronize(s);
+        cudaFree(d_buf);
+        if (rc == EBEM_OK && e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (d_count) {
+        unsigned long long c = 0;
+        cudaError_t e = cudaMemcpyAsync(&c, d_count, sizeof(c), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaFree(d_count);
+        if (rc == EBEM_OK && e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, cudaGetErrorString(e));
+        *nonnull = (long long)c;
+    }
+    return rc;
+}
+
+int ebem_assemble_sa(const ebem_mesh* m, const ebem_problem* p, int n_gh, int lag0, int nlag, double* E,
+                     int accumulate, void* stream, long long* nonnull) {
+    if (!m) return fail(EBEM_ERR_INVALID, "mesh is NULL");
+    return assemble_impl(m, p, n_gh, lag0, nlag, 0, m->d.nt, E, 3LL * m->d.nt, accumulate, stream, nonnull);
+}
+
+int ebem_assemble_sa_panel(const ebem_mesh* m, const ebem_problem* p, int n_gh, int lag0, int nlag, int src0,
+                           int nsrc, double* E, long long ld, int accumulate, void* stream, long long* nonnull) {
+    return assemble_impl(m, p, n_gh, lag0, nlag, src0, nsrc, E, ld, accumulate, stream, nonnull);
+}
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+/*
+ * libebem — C ABI of the B200-native energetic space-time Galerkin BEM for 3D
+ * elastodynamics (Lamé single-layer operator, piecewise-constant space/time).
+ *
+ * Plain C types only: host or device pointers and sizes.  Every function
+ * returns an int status (EBEM_OK = 0, negative on error) and leaves a
+ * thread-local message for ebem_last_error().  Matrices use the reference's
+ * byte layouts so that a MATLAB/MEX caller can `reshape` them unchanged:
+ *
+ *   E   column-major 3N x 3N per lag, lags slowest:
+ *       E[l*(3N)^2 + (3*j + c)*3N + 3*i + r] = block (source i, field j, lag l),
+ *       row component r, column component c
+ *       (reference: functions/BEMenerg_indir/BEMenerg_core/BEMenerg_coreGPU/
+ *        CUDAkernels/kernelGHC.cu:162, BEMenerg_coreSA_calcMatrixBlock.m:41,80)
+ *   phi column-major 3N x nT, phi[n*3N + 3*i + c]
+ *       (BEMenerg_coreGPU_timeMarching.m:156)
+ *
+ * Output pointers may be device pointers (the call is asynchronous on
+ * `stream` unless it returns a count) or host pointers (the library stages
+ * through device memory and returns after the copy).  `stream` is a
+ * cudaStream_t passed as void*; NULL is the legacy default stream.
+ *
+ * Reference paths are relative to the IvanDB/ElastodynamicEBEM project root;
+ * "f/" abbreviates "functions/".
+ */
+#ifndef EBEM_H
+#define EBEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EBEM_VERSION 1
+
+#define EBEM_OK 0
+#define EBEM_ERR_INVALID (-1)   /* bad argument, unsupported rule, size limit */
+#define EBEM_ERR_CUDA (-2)      /* CUDA runtime/library failure */
+#define EBEM_ERR_NOMEM (-3)     /* device or host allocation failed */
+#define EBEM_ERR_NODEVICE (-4)  /* no CUDA device visible */
+#define EBEM_ERR_SINGULAR (-5)  /* E_0 factorisation found a zero pivot */
+
+/* Opaque device-resident mesh: vertices, triangles and per-triangle frames. */
+typedef struct ebem_mesh ebem_mesh;
+
+/* The reference's pbParam (f/utility/fileRead/readInputFile.m:12-74):
+ * c_P = sqrt((lambda+2 mu)/rho), c_S = sqrt(mu/rho), dt = tfin/nt. */
+typedef struct ebem_problem {
+    double rho;
+    double mu;
+    double lambda;
+    double tfin;
+    int nt;
+} ebem_problem;
+
+/* Library version (EBEM_VERSION). */
+int ebem_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* ebem_last_error(void);
+
+/* Gauss-Hammer composite rule.  Replaces f/utility/quadRules/
+ * GaussHammerComposite.m:1 (with the base tables of GaussHammer_base.m).
+ * n_nodes in {1,3,7,12,19,28}; n_sub in {1,4,16,64,...} (a square);
+ * nodes: host array n_sub*n_nodes x 3 barycentric coordinates (row-major);
+ * weights: host array n_nodes, (2/n_sub) x base weights. */
+int ebem_quad_gh(int n_nodes, int n_sub, double* nodes, double* weights);
+
+/* Upload a surface mesh and derive normals, areas, centroids, longest edges
+ * and in-plane frames on the device.  Replaces the derived-field part of
+ * f/utility/fileRead/readSpaceMesh.m:93-151 and the per-triangle constants of
+ * .../BEMenerg_coreSA/BEMenerg_coreSA_calcCostantData.m:1-26.
+ * coords: host n_vertices x 3; tris: host n_triangles x 3, 0-based. */
+int ebem_mesh_create(const double* coords, int n_vertices, const int32_t* tris, int n_triangles,
+                     ebem_mesh** out);
+int ebem_mesh_destroy(ebem_mesh* mesh);
+int ebem_mesh_info(const ebem_mesh* mesh, int* n_vertices, int* n_triangles);
+/* Derived fields copied to host arrays (any may be NULL): normal (N x 3),
+ * area (N), center (N x 3), maxl (N); readSpaceMesh.m:114-139. */
+int ebem_mesh_derived(const ebem_mesh* mesh, double* normal, double* area, double* center, double* maxl);
+
+/* Number of non-zero Toeplitz blocks L = min(nT, ceil(maxDist/(c_S dt)) + 1).
+ * Replaces .../BEMenerg_coreGPU/BEMenerg_coreGPU_calcNumBlocks.m:1-20. */
+int ebem_num_blocks(const ebem_mesh* mesh, const ebem_problem* prob, int* num_blocks);
+
+/* Semi-analytic assembly of E_lag0 ... E_{lag0+nlag-1}: outer Gauss-Hammer
+ * rule with n_gh nodes (3, 7, 12 or 19) on the source triangle, closed-form
+ * inner integral on the field triangle, P- and S-fronts, energetic second
+ * difference in time, null test and 1e-14 clean-up of the reference.
+ * Replaces BEMenerg_coreSA_calcMatrixBlock(matrix, methodInfo, indTemp,
+ * deltaT, pbParam, domainMesh, constValues)
+ * (.../BEMenerg_coreSA/calcoloMatrice/BEMenerg_coreSA_calcMatrixBlock.m:1),
+ * one call per lag there, and the feval of the assembly kernel in
+ * .../BEMenerg_coreGPU/BEMenerg_coreGPU_launchKernel.m:11 (same layout).
+ * E: 9 N^2 nlag doubles, host or device.  accumulate = 0 overwrites every
+ * entry (zeros included); 1 adds (E += block), as the reference kernels do.
+ * nonnull (may be NULL): number of (source, field, lag) blocks that pass the
+ * null test; requesting it synchronises the stream. */
+int ebem_assemble_sa(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag,
+                     double* E, int accumulate, void* stream, long long* nonnull);
+
+/* Row panel of the same assembly: source triangles [src0, src0+nsrc) only,
+ * written column-major as (3 nsrc) x 3N per lag with leading dimension ld
+ * (ld >= 3 nsrc; lag stride ld*3N).  E + 3*src0 with ld = 3N writes the
+ * panel into a full matrix.  Used to shard the assembly across GPUs by
+ * source rows; the reference's parfor over all N^2 pairs
+ * (BEMenerg_coreSA_calcMatrixBlock.m:38) restricted to one row range.
+ * Host E requires ld == 3 nsrc. */
+int ebem_assemble_sa_panel(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag,
+                           int src0, int nsrc, double* E, long long ld, int accumulate, void* stream,
+                           long long* nonnull);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EBEM_H */

@@ -1,0 +1,194 @@
+"""ctypes front-end of the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
+this module, and only as the checker.  The oracle is a C++ restatement of the
+reference's MATLAB semi-analytic path (see sa_oracle.hpp / ebem_oracle.cpp for
+the file:line each routine follows).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBS = {}
+# "f64": the restatement in double precision (the reference's own arithmetic);
+# "q": the same formulas in binary128 on the same double inputs (arbiter for
+# the exact value of the reference's formulas).
+_FILES = {"f64": "liboracle.so", "q": "liboracle_q.so"}
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    """Compile the oracle (make in this directory); returns the .so path."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return os.path.join(_HERE, "liboracle.so")
+
+
+def lib(variant: str = "f64"):
+    if variant not in _LIBS:
+        path = os.path.join(_HERE, _FILES[variant])
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        mesh_args = [_dp, C.c_int, _ip, C.c_int]
+        par = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]
+        L.or_gh.argtypes = [C.c_int, C.c_int, _dp, _dp]
+        L.or_gh.restype = C.c_int
+        L.or_mesh_derived.argtypes = mesh_args + [_dp, _dp, _dp, _dp]
+        L.or_num_blocks.argtypes = [_dp, C.c_int, C.c_double, C.c_double, C.c_int]
+        L.or_num_blocks.restype = C.c_int
+        L.or_assemble_sa.argtypes = mesh_args + par + [C.c_int, C.c_int, C.c_int, _dp, C.c_int]
+        L.or_assemble_sa.restype = C.c_longlong
+        L.or_assemble_sa_pairs.argtypes = mesh_args + par + [C.c_int, C.c_int, _ip, _ip, _ip, _dp, C.c_int]
+        L.or_rhs.argtypes = mesh_args + par + [C.c_int, C.c_int, _dp]
+        L.or_march.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, _dp]
+        L.or_pp_sa.argtypes = mesh_args + par + [_dp, _dp, C.c_int, _dp, C.c_int, _dp, C.c_int]
+        L.or_assemble_ghc.argtypes = mesh_args + par + [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_int]
+        L.or_count_nonnull.argtypes = mesh_args + par + [C.c_int]
+        L.or_count_nonnull.restype = C.c_longlong
+        L.or_field_integrals.argtypes = [_dp, C.c_int, _ip, C.c_int, C.c_double, C.c_double, C.c_int, _dp,
+                                         C.c_double, _dp]
+        L.or_field_integrals.restype = C.c_int
+        _LIBS[variant] = L
+    return _LIBS[variant]
+
+
+def _m(mesh):
+    return (np.ascontiguousarray(mesh.coordinates, np.float64), mesh.number_nodes,
+            np.ascontiguousarray(mesh.triangles, np.int32), mesh.numberTriangles)
+
+
+def _p(prm):
+    return (float(prm.rho), float(prm.mu), float(prm.lam), float(prm.dt), int(prm.nT))
+
+
+def gauss_hammer(n_nodes: int, n_sub: int = 1):
+    nodes = np.zeros((n_sub * n_nodes, 3))
+    w = np.zeros(n_nodes)
+    rc = lib().or_gh(n_nodes, n_sub, nodes, w)
+    if rc:
+        raise ValueError(f"invalid Gauss-Hammer rule ({n_nodes}, {n_sub})")
+    return nodes, w
+
+
+def num_blocks(mesh, prm) -> int:
+    vs = (prm.mu / prm.rho) ** 0.5
+    return lib().or_num_blocks(np.ascontiguousarray(mesh.coordinates), mesh.number_nodes, vs, prm.dt, prm.nT)
+
+
+def assemble_sa(mesh, prm, n_gh: int, lag0: int, nlag: int, nthreads: int = 0, variant: str = "f64"):
+    n3 = 3 * mesh.numberTriangles
+    E = np.zeros(n3 * n3 * nlag)
+    nn = lib(variant).or_assemble_sa(*_m(mesh), *_p(prm), n_gh, lag0, nlag, E, nthreads)
+    if nn < 0:
+        raise ValueError("oracle assembly failed")
+    return E.reshape(nlag, n3, n3).transpose(0, 2, 1), int(nn)   # E[l][row, col]
+
+
+def assemble_sa_pairs(mesh, prm, n_gh: int, src, fld, lag, nthreads: int = 0, variant: str = "f64"):
+    src = np.ascontiguousarray(src, np.int32)
+    fld = np.ascontiguousarray(fld, np.int32)
+    lag = np.ascontiguousarray(lag, np.int32)
+    out = np.zeros(9 * len(src))
+    lib(variant).or_assemble_sa_pairs(*_m(mesh), *_p(prm), n_gh, len(src), src, fld, lag, out, nthreads)
+    return out.reshape(len(src), 3, 3).transpose(0, 2, 1)    # block[q][r, c]
+
+
+def rhs(mesh, prm, n_gh: int, datum_id: int):
+    n3 = 3 * mesh.numberTriangles
+    b = np.zeros(n3 * prm.nT)
+    lib().or_rhs(*_m(mesh), *_p(prm), n_gh, datum_id, b)
+    return b.reshape(prm.nT, n3).T.copy()        # (3N, nT)
+
+
+def march(E, b):
+    """E: (L, 3N, 3N) with E[l][row, col]; b: (3N, nT).  Returns phi (3N, nT)."""
+    L, n3, _ = E.shape
+    nT = b.shape[1]
+    Ecm = np.ascontiguousarray(E.transpose(0, 2, 1)).ravel()
+    bcm = np.ascontiguousarray(b.T).ravel()
+    phi = np.zeros(n3 * nT)
+    rc = lib().or_march(Ecm, n3, L, bcm, nT, phi)
+    if rc:
+        raise ValueError("singular E_0")
+    return phi.reshape(nT, n3).T.copy()
+
+
+def pp_sa(mesh, prm, phi, points, times, nthreads: int = 0):
+    """u(x, t): returns (3, npts, ntimes)."""
+    n3 = 3 * mesh.numberTriangles
+    phicm = np.ascontiguousarray(np.asarray(phi).T).ravel()
+    pts = np.ascontiguousarray(points, np.float64)
+    tms = np.ascontiguousarray(times, np.float64)
+    u = np.zeros(3 * len(pts) * len(tms))
+    lib().or_pp_sa(*_m(mesh), *_p(prm), phicm, pts, len(pts), tms, len(tms), u, nthreads)
+    return u.reshape(len(tms), len(pts), 3).transpose(2, 1, 0).copy()
+
+
+def assemble_ghc(mesh, prm, n_gh: int, n_sub: int, n_sing: int, lag0: int, nlag: int, nthreads: int = 0):
+    n3 = 3 * mesh.numberTriangles
+    E = np.zeros(n3 * n3 * nlag)
+    rc = lib().or_assemble_ghc(*_m(mesh), *_p(prm), n_gh, n_sub, n_sing, lag0, nlag, E, nthreads)
+    if rc:
+        raise ValueError("invalid rule")
+    return E.reshape(nlag, n3, n3).transpose(0, 2, 1)
+
+
+def count_nonnull(mesh, prm, L: int) -> int:
+    return int(lib().or_count_nonnull(*_m(mesh), *_p(prm), L))
+
+
+_CLIB = None
+
+
+def flop_census(mesh, prm, n_gh: int, npairs: int = 2000, seed: int = 0, L: int | None = None):
+    """FP64 operation census of the SA path on a seeded sample of (source,
+    field) pairs.  Returns a dict with flops per evaluated (pair, level), per
+    non-null pair-lag under level reuse and under the reference's
+    three-instants-per-lag schedule, and the transcendental share."""
+    global _CLIB
+    if _CLIB is None:
+        path = os.path.join(_HERE, "liboracle_count.so")
+        if not os.path.exists(path):
+            build()
+        _CLIB = C.CDLL(path)
+        _CLIB.or_flop_census.argtypes = [_dp, C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp,
+                                         C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp,
+                                         C.c_int, _ip, _ip, _dp]
+    if L is None:
+        L = num_blocks(mesh, prm)
+    rng = np.random.default_rng(seed)
+    N = mesh.numberTriangles
+    src = rng.integers(0, N, npairs).astype(np.int32)
+    fld = rng.integers(0, N, npairs).astype(np.int32)
+    nodes, w = gauss_hammer(n_gh, 1)
+    out = np.zeros(5)
+    _CLIB.or_flop_census(*_m(mesh), np.ascontiguousarray(mesh.normal), np.ascontiguousarray(mesh.area),
+                         np.ascontiguousarray(mesh.center), np.ascontiguousarray(mesh.maxL),
+                         prm.velP, prm.velS, prm.dt, int(L), int(n_gh), np.ascontiguousarray(nodes.ravel()),
+                         np.ascontiguousarray(w), npairs, src, fld, out)
+    flops, trans, nlev, nlag, fref = out
+    return {
+        "flops_per_level_eval": flops / max(nlev, 1),
+        "level_evals_per_pair_lag": nlev / max(nlag, 1),
+        "flops_per_pair_integral": flops / max(nlag, 1),
+        "flops_per_pair_integral_reference_schedule": fref / max(nlag, 1),
+        "transcendental_share": trans / max(flops, 1),
+        "sample_pairs": npairs, "sample_pair_lags": int(nlag),
+    }
+
+
+def field_integrals(mesh, velP: float, velS: float, j: int, x, t: float, variant: str = "f64"):
+    """Closed-form ris1..ris6 (each 3x3, global axes) of field triangle j seen
+    from point x at time t, and the case id (0 none, 1 SP_SP, 2 SP_P, 3 P)."""
+    L = lib(variant)
+    out = np.zeros(54)
+    typ = L.or_field_integrals(*_m(mesh), float(velP), float(velS), int(j),
+                               np.ascontiguousarray(x, np.float64), float(t), out)
+    return out.reshape(6, 3, 3), int(typ)

@@ -1,0 +1,90 @@
+"""CPU-side checks: the C-ABI library loads and exports every entry point of
+include/ebem.h, host-only entry points agree with the oracle bit for bit, the
+quadrature tables are exact to their degree, and compute entry points refuse
+to run without a device (no CPU fallback)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, cuda_available
+
+HEADER = os.path.join(ROOT, "include", "ebem.h")
+
+
+def header_symbols():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ebem_[a-z0-9_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from elastodynamicebem_b200 import lib as L
+    return L.load()
+
+
+def test_library_exports_header_symbols(lib):
+    syms = header_symbols()
+    assert len(syms) >= 8
+    for s in syms:
+        assert hasattr(lib, s), f"libebem.so does not export {s}"
+    from elastodynamicebem_b200 import lib as L
+    assert set(syms) <= set(L.PROTOTYPES), "ctypes prototypes missing for some header symbols"
+    assert lib.ebem_version() == 1
+
+
+@pytest.mark.parametrize("n", [1, 3, 7, 12, 19, 28])
+@pytest.mark.parametrize("nsub", [1, 4, 16, 64])
+def test_quad_matches_oracle(lib, oracle, n, nsub):
+    from elastodynamicebem_b200 import core
+    nodes, w = core.quad_gh(n, nsub)
+    on, ow = oracle.gauss_hammer(n, nsub)
+    assert np.array_equal(nodes, on) and np.array_equal(w, ow)
+    assert abs(w.sum() * nsub - 1.0) < 1e-12
+
+
+@pytest.mark.parametrize("n,deg", [(1, 1), (3, 2), (7, 5), (12, 6), (19, 9), (28, 11)])
+def test_quad_exactness(n, deg):
+    """Integrate x^a y^b over the reference triangle (area 1/2) exactly."""
+    from math import factorial
+    from elastodynamicebem_b200 import core
+    for nsub in (1, 4):
+        nodes, w = core.quad_gh(n, nsub)
+        W = np.tile(w, nsub) / nsub * 0.5 * nsub / 1.0   # composite weights sum to 1 -> area 1/2
+        W = np.tile(w, nsub) * 0.5
+        x, y = nodes[:, 0], nodes[:, 1]
+        tol = 1e-12 if n != 7 else 1e-11     # the 7-point table carries 13 digits
+        for a in range(deg + 1):
+            for b in range(deg + 1 - a):
+                exact = factorial(a) * factorial(b) / factorial(a + b + 2)
+                got = (W * x ** a * y ** b).sum()
+                assert abs(got - exact) <= tol, (n, nsub, a, b, got, exact)
+
+
+def test_invalid_rule_rejected(lib):
+    from elastodynamicebem_b200 import lib as L
+    out = np.zeros(100)
+    rc = lib.ebem_quad_gh(5, 1, out.ctypes.data, out.ctypes.data)
+    assert rc == -1 and b"Gauss-Hammer" in lib.ebem_last_error()
+    rc = lib.ebem_quad_gh(7, 3, out.ctypes.data, out.ctypes.data)
+    assert rc == -1
+
+
+@pytest.mark.skipif(cuda_available(), reason="checks the no-device error path")
+def test_no_device_no_fallback(lib):
+    from elastodynamicebem_b200 import mesh as M, core
+    from elastodynamicebem_b200.lib import EbemError
+    with pytest.raises(EbemError) as ei:
+        core.DeviceMesh(M.screen_uniform(2))
+    assert ei.value.code == -4
+
+
+def test_mesh_validation(lib):
+    coords = np.zeros((3, 3))
+    tris = np.array([[0, 1, 5]], np.int32)
+    h = C.c_void_p()
+    rc = lib.ebem_mesh_create(coords.ctypes.data, 3, tris.ctypes.data, 1, C.byref(h))
+    assert rc == -1 and b"out of range" in lib.ebem_last_error()
