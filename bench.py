@@ -182,6 +182,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak measurement")
+    ap.add_argument("--workload", default="sphere1280", choices=["sphere1280", "sphere320"],
+                    help="sphere1280 is the benchmark; sphere320 (icosphere 2) is the small profiling case")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warning: fewer than 3 warm-up steps")
@@ -205,7 +208,7 @@ def main():
 
     from elastodynamicebem_b200 import core, problem
 
-    w = problem.sphere_workload(7)
+    w = problem.sphere_workload(7, subdivisions=3 if args.workload == "sphere1280" else 2)
     m, prm = w.mesh, w.params
     N = m.numberTriangles
     src0 = rank * N // world
@@ -280,13 +283,13 @@ def main():
     e2e_value = total_pairs / statistics.median(e2e_times) if e2e_times else None
 
     if rank == 0:
-        peak = fp64_peak_tflops(torch)
+        peak = float("nan") if args.no_peak else fp64_peak_tflops(torch)
         achieved = FLOPS_PER_PAIR_INTEGRAL * my_pairs / kernel_s / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "sphere_icosphere3_N1280_L40_GH7", "N": N, "L": L, "n_gh": w.n_gh,
+            "config": {"workload": f"sphere_icosphere{3 if N == 1280 else 2}_N{N}_L{L}_GH7", "N": N, "L": L, "n_gh": w.n_gh,
                        "rho": prm.rho, "mu": prm.mu, "lambda": prm.lam, "dt": prm.dt, "nT": prm.nT,
                        "pair_integrals_per_step": total_pairs, "parallelism": f"source-row panels x{world}",
                        "l2": "output 4.7 GB per step written to HBM, far larger than L2"},

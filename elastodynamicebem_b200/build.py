@@ -15,8 +15,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libebem.so")
 
-SOURCES = ["capi.cu", "quadrature.cu", "sa_assemble.cu"]
-HEADERS = ["sa_device.cuh", "ebem_internal.h"]
+SOURCES = ["capi.cu", "quadrature.cu", "sa_assemble.cu", "march.cu", "ghc.cu"]
+HEADERS = ["sa_device.cuh", "sa_edge.cuh", "sa_pair.cuh", "ebem_internal.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
@@ -38,15 +38,19 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
-    if not force and not _stale():
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False,
+          defines: tuple = (), out: str | None = None) -> str:
+    """Compile and link libebem.so.  ``defines`` adds -D flags and ``out``
+    redirects the library (used to compare code-generation options)."""
+    target = out or LIB
+    if not force and out is None and not _stale():
         return LIB
-    objdir = os.path.join(PKG, "_build")
+    objdir = os.path.join(PKG, "_build" if out is None else "_build_" + os.path.basename(out).replace(".so", ""))
     os.makedirs(objdir, exist_ok=True)
     objs = []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [nvcc(), *ARCH, *FLAGS, *[f"-D{d}" for d in defines], "-c", os.path.join(CSRC, src), "-o", obj]
         if ptxas_info:
             cmd += ["-Xptxas", "-v"]
         if verbose:
@@ -57,13 +61,13 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if ptxas_info or verbose:
             print(r.stderr, file=sys.stderr)
         objs.append(obj)
-    tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+    tmp = target + ".tmp"
+    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-lcusolver", "-lcublas"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, target)
+    return target
 
 
 if __name__ == "__main__":

@@ -116,3 +116,83 @@ def assemble_sa_panel(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, lag0: in
                                                   _stream_ptr(stream) if out.is_cuda else None,
                                                   C.byref(cnt) if count else None))
     return (out, int(cnt.value)) if count else out
+
+
+def _ptr(a):
+    """Data pointer of a torch tensor or a C-contiguous numpy array."""
+    if isinstance(a, torch.Tensor):
+        if not a.is_contiguous() or a.dtype != torch.float64:
+            raise ValueError("expected a contiguous float64 tensor")
+        return a.data_ptr()
+    a = np.asarray(a)
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("expected a C-contiguous float64 array")
+    return a.ctypes.data
+
+
+def rhs(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, datum: int, out: torch.Tensor | None = None, stream=None):
+    """Right-hand side b (nT, 3N): row n is b_n (column n of the C-ABI's
+    column-major 3N x nT array)."""
+    n3 = 3 * dmesh.N
+    if out is None:
+        out = torch.empty((prm.nT, n3), dtype=torch.float64, device="cuda")
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_rhs(dmesh.handle, C.byref(p), int(n_gh), int(datum), _ptr(out),
+                                    _stream_ptr(stream) if out.is_cuda else None))
+    return out
+
+
+def march(E: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None, stream=None):
+    """Density phi (nT, 3N) from the blocks E (L, 3N, 3N storage of
+    assemble_sa, i.e. E[l] transposed view) and the right-hand side b (nT, 3N)."""
+    Eraw = E.transpose(1, 2).contiguous()      # column-major blocks of the C ABI (no copy for assemble_sa's view)
+    L, n3 = Eraw.shape[0], Eraw.shape[1]
+    nT = b.shape[0]
+    if out is None:
+        out = torch.empty((nT, n3), dtype=torch.float64, device=b.device)
+    _lib.check(_lib.load().ebem_march(_ptr(Eraw), int(n3), int(L), _ptr(b.contiguous()), int(nT), _ptr(out),
+                                      _stream_ptr(stream) if out.is_cuda else None))
+    return out
+
+
+def timemarch_sa(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, datum: int, out: torch.Tensor | None = None,
+                 stream=None):
+    """BEMenerg_coreSA_timeMarching: assembly + right-hand side + marching.
+    Returns (phi (nT, 3N), L)."""
+    n3 = 3 * dmesh.N
+    if out is None:
+        out = torch.empty((prm.nT, n3), dtype=torch.float64, device="cuda")
+    p = _lib.problem_struct(prm)
+    L = C.c_int()
+    _lib.check(_lib.load().ebem_timemarch_sa(dmesh.handle, C.byref(p), int(n_gh), int(datum), _ptr(out), C.byref(L),
+                                             _stream_ptr(stream) if out.is_cuda else None))
+    return out, int(L.value)
+
+
+def pp_sa(dmesh: DeviceMesh, prm: ProblemParams, phi: torch.Tensor, points, times, stream=None):
+    """Displacement u (ntimes, npts, 3) at the points and times from the
+    density phi (nT, 3N)."""
+    pts = torch.as_tensor(np.ascontiguousarray(points, np.float64)).to(phi.device)
+    tms = np.ascontiguousarray(times, np.float64)
+    u = torch.empty((len(tms), pts.shape[0], 3), dtype=torch.float64, device=phi.device)
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_pp_sa(dmesh.handle, C.byref(p), _ptr(phi.contiguous()), _ptr(pts), int(pts.shape[0]),
+                                      tms.ctypes.data, len(tms), _ptr(u),
+                                      _stream_ptr(stream) if u.is_cuda else None))
+    return u
+
+
+def assemble_ghc(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, n_sub: int, n_sing: int, lag0: int = 0,
+                 nlag: int | None = None, out: torch.Tensor | None = None, sa_diagonal: bool = True, stream=None):
+    """Numerical-inner E_lag0.. (the reference's GPU method): returns E[l][row, col]
+    (added into ``out`` when given, else into zeros)."""
+    if nlag is None:
+        nlag = num_blocks(dmesh, prm) - lag0
+    n3 = 3 * dmesh.N
+    if out is None:
+        out = torch.zeros((nlag, n3, n3), dtype=torch.float64, device="cuda")
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_assemble_ghc(dmesh.handle, C.byref(p), int(n_gh), int(n_sub), int(n_sing), int(lag0),
+                                             int(nlag), _ptr(out), int(bool(sa_diagonal)),
+                                             _stream_ptr(stream) if out.is_cuda else None))
+    return out.view(nlag, n3, n3).transpose(1, 2)

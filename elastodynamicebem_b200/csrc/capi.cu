@@ -89,6 +89,50 @@ __global__ void max_vertex_dist_kernel(const double* __restrict__ c, int nv, uns
     if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(best));
 }
 
+// A host-or-device input array made available on the device.
+struct DevIn {
+    const double* d = nullptr;
+    double* owned = nullptr;
+    int init(const double* p, size_t n, cudaStream_t s) {
+        if (is_device_ptr(p)) { d = p; return EBEM_OK; }
+        if (cudaMalloc(&owned, n * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(EBEM_ERR_NOMEM, "device staging allocation failed");
+        }
+        EBEM_CUDA_TRY(cudaMemcpyAsync(owned, p, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        d = owned;
+        return EBEM_OK;
+    }
+    ~DevIn() { if (owned) cudaFree(owned); }
+};
+
+// A host-or-device output array: device pointer used directly, host pointer
+// staged and copied back by finish().
+struct DevOut {
+    double* d = nullptr;
+    double* host = nullptr;
+    size_t n = 0;
+    int init(double* p, size_t count) {
+        n = count;
+        if (is_device_ptr(p)) { d = p; return EBEM_OK; }
+        host = p;
+        if (cudaMalloc(&d, n * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            d = nullptr;
+            return fail(EBEM_ERR_NOMEM, "device staging allocation failed");
+        }
+        return EBEM_OK;
+    }
+    int finish(cudaStream_t s) {
+        if (host) {
+            EBEM_CUDA_TRY(cudaMemcpyAsync(host, d, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+            EBEM_CUDA_TRY(cudaStreamSynchronize(s));
+        }
+        return EBEM_OK;
+    }
+    ~DevOut() { if (host && d) cudaFree(d); }
+};
+
 }  // namespace
 }  // namespace ebem
 
@@ -281,6 +325,102 @@ int ebem_assemble_sa(const ebem_mesh* m, const ebem_problem* p, int n_gh, int la
                      int accumulate, void* stream, long long* nonnull) {
     if (!m) return fail(EBEM_ERR_INVALID, "mesh is NULL");
     return assemble_impl(m, p, n_gh, lag0, nlag, 0, m->d.nt, E, 3LL * m->d.nt, accumulate, stream, nonnull);
+}
+
+int ebem_assemble_ghc(const ebem_mesh* m, const ebem_problem* p, int n_gh, int n_sub, int n_sing, int lag0,
+                      int nlag, double* E, int sa_diagonal, void* stream) {
+    if (!m || !E) return fail(EBEM_ERR_INVALID, "NULL mesh or output");
+    if (int rc = check_problem(p)) return rc;
+    if (n_gh != 3 && n_gh != 7 && n_gh != 12 && n_gh != 19) return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+    if ((n_sub != 1 && n_sub != 4 && n_sub != 16 && n_sub != 64) ||
+        (n_sing != 1 && n_sing != 3 && n_sing != 7 && n_sing != 12 && n_sing != 19))
+        return fail(EBEM_ERR_INVALID, "inner rule: n_sub in {1,4,16,64}, n_sing in {1,3,7,12,19}");
+    if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MeshData& md = const_cast<MeshData&>(m->d);
+    PhysParams P = phys_from(p);
+    const size_t n3 = 3 * (size_t)md.nt;
+    DevOut out;
+    if (int rc = out.init(E, n3 * n3 * nlag)) return rc;
+    if (out.host) EBEM_CUDA_TRY(cudaMemcpyAsync(out.d, E, n3 * n3 * nlag * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (int rc = launch_ghc_assemble(md, P, n_gh, n_sub, n_sing, lag0, nlag, out.d, n3, n3 * n3, s)) return rc;
+    if (sa_diagonal) {
+        if (int rc = map_nodes(md, n_gh, s)) return rc;
+        if (int rc = launch_sa_assemble(md, P, n_gh, lag0, nlag, 0, md.nt, out.d, n3, n3 * n3, 0, nullptr, s, 1)) return rc;
+    }
+    return out.finish(s);
+}
+
+int ebem_rhs(const ebem_mesh* m, const ebem_problem* p, int n_gh, int datum, double* rhs, void* stream) {
+    if (!m || !rhs) return fail(EBEM_ERR_INVALID, "NULL mesh or output");
+    if (int rc = check_problem(p)) return rc;
+    if (n_gh != 3 && n_gh != 7 && n_gh != 12 && n_gh != 19) return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+    if (datum < 0 || datum > 7) return fail(EBEM_ERR_INVALID, "unknown datum id (0..7)");
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MeshData& md = const_cast<MeshData&>(m->d);
+    if (int rc = map_nodes(md, n_gh, s)) return rc;
+    PhysParams P = phys_from(p);
+    DevOut out;
+    if (int rc = out.init(rhs, 3 * (size_t)md.nt * P.nT)) return rc;
+    if (int rc = launch_rhs(md, P, n_gh, datum, out.d, s)) return rc;
+    return out.finish(s);
+}
+
+int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double* phi, void* stream) {
+    if (!E || !rhs || !phi || n3 < 1 || L < 1 || nT < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
+    if (int rc = check_device()) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevIn dE, dr;
+    if (int rc = dE.init(E, (size_t)n3 * n3 * L, s)) return rc;
+    if (int rc = dr.init(rhs, (size_t)n3 * nT, s)) return rc;
+    DevOut out;
+    if (int rc = out.init(phi, (size_t)n3 * nT)) return rc;
+    if (int rc = march_device(dE.d, n3, L, dr.d, nT, out.d, s)) return rc;
+    return out.finish(s);
+}
+
+int ebem_timemarch_sa(const ebem_mesh* m, const ebem_problem* p, int n_gh, int datum, double* phi, int* num_blocks,
+                      void* stream) {
+    if (!m || !phi) return fail(EBEM_ERR_INVALID, "NULL mesh or output");
+    if (int rc = check_problem(p)) return rc;
+    int L = 0;
+    if (int rc = ebem_num_blocks(m, p, &L)) return rc;
+    if (num_blocks) *num_blocks = L;
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t n3 = 3 * (size_t)m->d.nt;
+    double *dE = nullptr, *dr = nullptr;
+    if (cudaMalloc(&dE, n3 * n3 * L * sizeof(double)) != cudaSuccess || cudaMalloc(&dr, n3 * p->nt * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        if (dE) cudaFree(dE);
+        return fail(EBEM_ERR_NOMEM, "device allocation of E or the right-hand side failed");
+    }
+    int rc = ebem_assemble_sa(m, p, n_gh, 0, L, dE, 0, stream, nullptr);
+    if (!rc) rc = ebem_rhs(m, p, n_gh, datum, dr, stream);
+    if (!rc) rc = ebem_march(dE, (int)n3, L, dr, p->nt, phi, stream);
+    cudaStreamSynchronize(s);
+    cudaFree(dE);
+    cudaFree(dr);
+    return rc;
+}
+
+int ebem_pp_sa(const ebem_mesh* m, const ebem_problem* p, const double* phi, const double* pts, int npts,
+               const double* times, int ntimes, double* u, void* stream) {
+    if (!m || !phi || !pts || !times || !u || npts < 1 || ntimes < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
+    if (int rc = check_problem(p)) return rc;
+    if (is_device_ptr(times)) return fail(EBEM_ERR_INVALID, "times must be a host array");
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    PhysParams P = phys_from(p);
+    DevIn dphi, dpts;
+    if (int rc = dphi.init(phi, 3 * (size_t)m->d.nt * P.nT, s)) return rc;
+    if (int rc = dpts.init(pts, 3 * (size_t)npts, s)) return rc;
+    DevOut out;
+    if (int rc = out.init(u, 3 * (size_t)npts * ntimes)) return rc;
+    if (int rc = launch_pp_sa(m->d, P, dphi.d, dpts.d, npts, times, ntimes, out.d, s)) return rc;
+    return out.finish(s);
 }
 
 int ebem_assemble_sa_panel(const ebem_mesh* m, const ebem_problem* p, int n_gh, int lag0, int nlag, int src0,

@@ -55,6 +55,13 @@ PhysParams phys_from(const ebem_problem* p);
 // (column-major 3 nsrc x 3N per lag, leading dimension ld, lag stride ld_lag).
 int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
-                       cudaStream_t s);
+                       cudaStream_t s, int diag_only = 0);
+int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_sub, int n_sing, int lag0, int nlag,
+                        double* d_E, size_t ld, size_t ld_lag, cudaStream_t s);
+
+int launch_rhs(const MeshData& m, const PhysParams& P, int n_gh, int datum, double* d_rhs, cudaStream_t s);
+int march_device(const double* dE, int n3, int L, const double* drhs, int nT, double* dphi, cudaStream_t s);
+int launch_pp_sa(const MeshData& m, const PhysParams& P, const double* d_phi, const double* d_pts, int npts,
+                 const double* h_times, int ntimes, double* d_u, cudaStream_t s);
 
 }  // namespace ebem

@@ -1,0 +1,172 @@
+// Numerical-inner assembly of E_l: outer Gauss-Hammer rule on the source
+// triangle, composite Gauss-Hammer rule on the field triangle, the Lamé kernel
+// integrated twice in time with separate P and S Heaviside fronts.
+//
+// Reference: functions/BEMenerg_indir/BEMenerg_core/BEMenerg_coreGPU/CUDAkernels/
+// kernelGHC.cu:5-259 (identical copies: BEMenerg_coreFN/CUDAkernels/kernelGHC.cu,
+// functions/BEMenerg_dir/CUDAkernels/kernelV.cu), launched by
+// BEMenerg_coreGPU_launchKernel.m:11 with grid (N, N, lags) and one thread
+// per inner node.  Semantics kept: off-diagonal pairs only (the diagonal
+// comes from the semi-analytic path, BEMenerg_coreGPU_timeMarching.m:101-131),
+// the null test (lag-1) c_S dt > max vertex distance (kernelGHC.cu:171-201),
+// instants dt (lag + {-1, 0, 1}) with weights (1, -2, 1) and t >= 0
+// (:88-99), entries written only when |value| > 1e-14 before the division by
+// 4 pi rho (:164-165), accumulated into the output (+=).
+//
+// B200 design: one thread per (source, field) pair (consecutive lanes take
+// consecutive sources of one field triangle); the thread evaluates the
+// node-pair sum K(t_k) once per time level and emits
+// E_l = K_{l+1} - 2 K_l + K_{l-1} from a sliding window (the reference
+// recomputes each instant for three lags and reduces through shared memory).
+#include "ebem_internal.h"
+#include "sa_pair.cuh"
+
+namespace ebem {
+
+struct GHCArgs {
+    const double* coords;
+    const int32_t* tris;
+    const TriGeom* geo;
+    const double* outer;    // n_out x 3 barycentric
+    const double* wout;     // n_out
+    const double* inner;    // n_in x 3 barycentric (n_sub sub-triangles x n_sing nodes)
+    const double* win;      // n_sing
+    int n_out, n_sub, n_sing;
+    int N;
+    double velP, velS, dt, c4pirho;
+    int lag0, nlag;
+    double* E;
+    size_t ld, ld_lag;
+};
+
+// kernelGHC.cu:204-259 (nucleo) for one node pair, symmetric entries
+// (11,12,13,22,23,33), at instant t.
+__device__ __forceinline__ void nucleo_sym(double nu[6], const double x[3], double r, double t, double cP,
+                                           double cS) {
+    const double r3 = r * r * r, r5 = r3 * r * r;
+    const double HP = (t - (r / cP) > 0) ? 1.0 : 0.0, HS = (t - (r / cS) > 0) ? 1.0 : 0.0;
+    const double tail = (cP * cP * t * t - r * r) / (cP * cP) * HP - (cS * cS * t * t - r * r) / (cS * cS) * HS;
+    const double icP2 = 1 / (cP * cP), icS2 = 1 / (cS * cS);
+    const int ii[6] = {0, 0, 0, 1, 1, 2}, jj[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for (int e = 0; e < 6; e++) {
+        const double xx = x[ii[e]] * x[jj[e]];
+        const double dlt = (ii[e] == jj[e]) ? 1.0 : 0.0;
+        nu[e] = (xx / r3) * icP2 * HP + (dlt / r - xx / r3) * icS2 * HS - 0.5 * (dlt / r3 - 3 * (xx / r5)) * tail;
+    }
+}
+
+__global__ void __launch_bounds__(128) ghc_assemble_kernel(GHCArgs A) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (long long)A.N * A.N) return;
+    const int i = (int)(p % A.N);          // source (outer rule)
+    const int j = (int)(p / A.N);          // field (inner rule)
+    if (i == j) return;
+    double VS[3][3], VF[3][3];
+    for (int v = 0; v < 3; v++)
+        for (int c = 0; c < 3; c++) {
+            VS[v][c] = A.coords[3 * A.tris[3 * i + v] + c];
+            VF[v][c] = A.coords[3 * A.tris[3 * j + v] + c];
+        }
+    double distMax = 0;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            double d0 = VS[a][0] - VF[b][0], d1 = VS[a][1] - VF[b][1], d2 = VS[a][2] - VF[b][2];
+            distMax = fmax(distMax, sqrt(d0 * d0 + d1 * d1 + d2 * d2));
+        }
+    // lags computed: not null, i.e. (l-1) c_S dt <= distMax
+    int lhi = A.lag0 + A.nlag - 1;
+    while (lhi >= A.lag0 && (lhi - 1) * A.velS * A.dt > distMax) lhi--;
+    if (lhi < A.lag0) return;
+    const int klo = max(0, A.lag0 - 1), khi = lhi + 1;
+    const double aS = A.geo[i].area, aF = A.geo[j].area;
+    double Km2[6] = {0, 0, 0, 0, 0, 0}, Km1[6] = {0, 0, 0, 0, 0, 0}, K[6];
+    const size_t n3 = A.ld;
+    const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    for (int k = klo; k <= khi; k++) {
+        const double t = A.dt * k;
+#pragma unroll
+        for (int e = 0; e < 6; e++) K[e] = 0.0;
+        for (int q = 0; q < A.n_sub * A.n_sing; q++) {
+            const double* bq = A.inner + 3 * q;
+            double y[3];
+            for (int c = 0; c < 3; c++) y[c] = bq[0] * VF[0][c] + bq[1] * VF[1][c] + bq[2] * VF[2][c];
+            const double wq = A.win[q % A.n_sing] * aF;
+            for (int l = 0; l < A.n_out; l++) {
+                const double* bl = A.outer + 3 * l;
+                double x[3];
+                for (int c = 0; c < 3; c++) x[c] = y[c] - (bl[0] * VS[0][c] + bl[1] * VS[1][c] + bl[2] * VS[2][c]);
+                const double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+                const double w = (A.wout[l] * aS) * wq;
+                double nu[6];
+                nucleo_sym(nu, x, r, t, A.velP, A.velS);
+#pragma unroll
+                for (int e = 0; e < 6; e++) K[e] += w * nu[e];
+            }
+        }
+        const int l = k - 1;               // lag completed by K_k
+        if (l >= A.lag0 && l <= lhi) {
+            double* base = A.E + (size_t)(l - A.lag0) * A.ld_lag + (3 * (size_t)j) * n3 + 3 * (size_t)i;
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    const int e = map[3 * c + r];
+                    const double prev = (l - 1 >= 0) ? Km2[e] : 0.0;
+                    const double v = (K[e] + (-2.0) * Km1[e]) + prev;
+                    if (fabs(v) > 1.0e-14) base[c * n3 + r] += v / A.c4pirho;
+                }
+        }
+#pragma unroll
+        for (int e = 0; e < 6; e++) { Km2[e] = Km1[e]; Km1[e] = K[e]; }
+    }
+}
+
+int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_sub, int n_sing, int lag0, int nlag,
+                        double* d_E, size_t ld, size_t ld_lag, cudaStream_t s) {
+    double ob[28 * 3], ow[28];
+    if (gh_composite(n_gh, 1, ob, ow)) return fail(EBEM_ERR_INVALID, "unsupported outer rule");
+    std::vector<double> ib((size_t)3 * n_sub * n_sing), iw(n_sing);
+    if (gh_composite(n_sing, n_sub, ib.data(), iw.data())) return fail(EBEM_ERR_INVALID, "unsupported inner rule");
+    size_t nb = 3 * n_gh + n_gh + ib.size() + iw.size();
+    std::vector<double> tab(nb);
+    size_t o = 0;
+    for (int k = 0; k < 3 * n_gh; k++) tab[o++] = ob[k];
+    for (int k = 0; k < n_gh; k++) tab[o++] = ow[k];
+    for (double v : ib) tab[o++] = v;
+    for (double v : iw) tab[o++] = v;
+    double* d_tab = nullptr;
+    EBEM_CUDA_TRY(cudaMalloc(&d_tab, nb * sizeof(double)));
+    EBEM_CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), nb * sizeof(double), cudaMemcpyHostToDevice, s));
+    GHCArgs A;
+    A.coords = m.d_coords;
+    A.tris = m.d_tris;
+    A.geo = m.d_geo;
+    A.outer = d_tab;
+    A.wout = d_tab + 3 * n_gh;
+    A.inner = d_tab + 4 * n_gh;
+    A.win = d_tab + 4 * n_gh + ib.size();
+    A.n_out = n_gh;
+    A.n_sub = n_sub;
+    A.n_sing = n_sing;
+    A.N = m.nt;
+    A.velP = P.velP;
+    A.velS = P.velS;
+    A.dt = P.dt;
+    A.c4pirho = 4 * kPi * P.rho;
+    A.lag0 = lag0;
+    A.nlag = nlag;
+    A.E = d_E;
+    A.ld = ld;
+    A.ld_lag = ld_lag;
+    long long NN = (long long)m.nt * m.nt;
+    int threads = 128;
+    ghc_assemble_kernel<<<(unsigned)((NN + threads - 1) / threads), threads, 0, s>>>(A);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_tab);
+    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("numerical-inner assembly: ") + cudaGetErrorString(e));
+    return EBEM_OK;
+}
+
+}  // namespace ebem

@@ -1,0 +1,317 @@
+// Right-hand side, time marching and post-processing on the device.
+//
+// Reference (paths relative to the reference project root;
+// "CORE/" = functions/BEMenerg_indir/BEMenerg_core/):
+//   right-hand side   CORE/BEMenerg_core_calcTn/BEMenerg_core_calcTnBlock.m:28-58,
+//                     CORE/BEMenerg_core_calcTn/BEMenerg_core_calcNucleoTn.m:196-244
+//   time marching     CORE/BEMenerg_coreGPU/BEMenerg_coreGPU_timeMarching.m:151-169
+//                     (LU of E_0 once; phi_n = E_0^{-1}(b_n - sum_l E_l phi_{n-l}))
+//   post-processing   functions/BEMenerg_indir/BEMenerg_postProc/BEMenerg_postProcA/
+//                     BEMenerg_postProcA_singlePoint.m:21-61, _calcMatrix.m, _calcMatrixBlock.m
+#include "ebem_internal.h"
+#include "sa_pair.cuh"
+
+#include <cusolverDn.h>
+
+namespace ebem {
+
+// ---------------------------------------------------------------------------
+// Dirichlet data g(x, t).  Ids 2..7 are the reference's cases
+// (BEMenerg_core_calcNucleoTn.m:199-237); 0 and 1 are the data of the screen
+// and sphere benchmark problems.
+__device__ void datum_value(int id, double velP, double Tfin, const double x[3], double t, double g[3]) {
+    g[0] = g[1] = g[2] = 0.0;
+    switch (id) {
+    case 0: g[2] = t * t * t * t * exp(-2 * t); break;
+    case 1: {
+        double s = (t > 0) ? sin(2 * kPi * t) : 0.0;
+        g[0] = x[0] * s; g[1] = x[1] * s; g[2] = x[2] * s;
+    } break;
+    case 2: g[2] = 0.5 * t; break;
+    case 3: {
+        double f = 1.0;
+        if (t < kPi / 2) { double s = sin(t); f = s * s * s * s * s; }
+        g[2] = f * (x[0] * x[0]);
+    } break;
+    case 4: case 5: {
+        double h = (id == 4) ? 1.0 : 3.0;
+        int hat_k = (int)ceil((velP * Tfin) / (2 * h)) - 1;
+        double s = 0.0;
+        for (int k = 0; k <= hat_k; k++) {
+            double a1 = velP * t - 2 * h * k - (h - x[2]);
+            double a2 = velP * t - 2 * h * (k + 1) + (h - x[2]);
+            double term = a1 * (a1 > 0) - a2 * (a2 > 0);
+            s += ((k & 1) ? -1.0 : 1.0) * term;
+        }
+        g[2] = s;
+    } break;
+    case 6: { double u = x[0] - 2 + velP * t - 0.475; g[0] = -exp(-20 * u * u); } break;
+    case 7: { double u = x[2] + 1 - velP * t; g[2] = -exp(-20 * u * u); } break;
+    default: break;
+    }
+}
+
+__global__ void rhs_kernel(const NodeW* __restrict__ nodes, int N, int n_gh, int datum, double dt, int nT,
+                           double velP, double Tfin, double* __restrict__ rhs) {
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)N * nT) return;
+    int t = (int)(idx % N), n = (int)(idx / N);
+    double t0 = dt * n, t1 = dt * (n + 1);
+    double ris[3] = {0, 0, 0};
+    for (int g = 0; g < n_gh; g++) {
+        NodeW p = nodes[(size_t)t * n_gh + g];
+        double x[3] = {p.x, p.y, p.z}, g1[3], g0[3];
+        datum_value(datum, velP, Tfin, x, t1, g1);
+        datum_value(datum, velP, Tfin, x, t0, g0);
+        for (int c = 0; c < 3; c++) ris[c] = ris[c] + (g1[c] - g0[c]) * p.w;
+    }
+    for (int c = 0; c < 3; c++) rhs[(size_t)n * 3 * N + 3 * t + c] = (fabs(ris[c]) < 1.0e-14) ? 0.0 : ris[c];
+}
+
+int launch_rhs(const MeshData& m, const PhysParams& P, int n_gh, int datum, double* d_rhs, cudaStream_t s) {
+    long long total = (long long)m.nt * P.nT;
+    int threads = 128;
+    rhs_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, s>>>(m.d_nodes, m.nt, n_gh, datum, P.dt,
+                                                                              P.nT, P.velP, P.dt * P.nT, d_rhs);
+    EBEM_CUDA_TRY(cudaGetLastError());
+    return EBEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// History product y -= A x, A column-major n3 x K (the concatenated blocks
+// [E_1 E_2 ... E_M]), x contiguous (phi_{n-1}, phi_{n-2}, ... thanks to the
+// reversed storage of the density).  HBM-bound: each block streams a chunk
+// of columns for a tile of rows, keeps per-thread partial sums of
+// EBEM_GEMV_RPT rows and adds them to y with one atomic per row.
+#define EBEM_GEMV_THREADS 256
+#define EBEM_GEMV_RPT 8
+
+__global__ void __launch_bounds__(EBEM_GEMV_THREADS)
+hist_gemv_kernel(const double* __restrict__ A, int n3, long long K, long long cols_per_block,
+                 const double* __restrict__ x, double* __restrict__ y) {
+    const int tile_rows = EBEM_GEMV_THREADS * EBEM_GEMV_RPT;
+    const int row0 = blockIdx.y * tile_rows + threadIdx.x;
+    const long long k0 = (long long)blockIdx.x * cols_per_block;
+    long long k1 = k0 + cols_per_block;
+    if (k1 > K) k1 = K;
+    double acc[EBEM_GEMV_RPT];
+#pragma unroll
+    for (int i = 0; i < EBEM_GEMV_RPT; i++) acc[i] = 0.0;
+    long long k = k0;
+    for (; k + 1 < k1; k += 2) {
+        const double xa = x[k], xb = x[k + 1];
+        const double* ca = A + k * (long long)n3;
+        const double* cb = ca + n3;
+#pragma unroll
+        for (int i = 0; i < EBEM_GEMV_RPT; i++) {
+            int r = row0 + i * EBEM_GEMV_THREADS;
+            if (r < n3) acc[i] += __ldg(ca + r) * xa + __ldg(cb + r) * xb;
+        }
+    }
+    if (k < k1) {
+        const double xa = x[k];
+        const double* ca = A + k * (long long)n3;
+#pragma unroll
+        for (int i = 0; i < EBEM_GEMV_RPT; i++) {
+            int r = row0 + i * EBEM_GEMV_THREADS;
+            if (r < n3) acc[i] += __ldg(ca + r) * xa;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < EBEM_GEMV_RPT; i++) {
+        int r = row0 + i * EBEM_GEMV_THREADS;
+        if (r < n3 && acc[i] != 0.0) atomicAdd(y + r, -acc[i]);
+    }
+}
+
+int launch_hist_gemv(const double* A, int n3, long long K, const double* x, double* y, int sm_count, cudaStream_t s) {
+    if (K <= 0) return EBEM_OK;
+    const int tile_rows = EBEM_GEMV_THREADS * EBEM_GEMV_RPT;
+    int row_tiles = (n3 + tile_rows - 1) / tile_rows;
+    // about four resident blocks per SM in total, at least 64 columns each
+    long long want = (long long)sm_count * 4 / row_tiles;
+    if (want < 1) want = 1;
+    long long cpb = (K + want - 1) / want;
+    if (cpb < 64) cpb = 64;
+    long long nblk = (K + cpb - 1) / cpb;
+    dim3 grid((unsigned)nblk, (unsigned)row_tiles);
+    hist_gemv_kernel<<<grid, EBEM_GEMV_THREADS, 0, s>>>(A, n3, K, cpb, x, y);
+    EBEM_CUDA_TRY(cudaGetLastError());
+    return EBEM_OK;
+}
+
+__global__ void copy_reverse_kernel(const double* __restrict__ src, double* __restrict__ dst, int n3, int nT, int to_rev) {
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n3 * nT) return;
+    int r = (int)(idx % n3), n = (int)(idx / n3);
+    if (to_rev) dst[(size_t)(nT - 1 - n) * n3 + r] = src[idx];
+    else dst[idx] = src[(size_t)(nT - 1 - n) * n3 + r];
+}
+
+#define CUSOLVER_TRY(expr)                                                                        \
+    do {                                                                                          \
+        cusolverStatus_t _st = (expr);                                                            \
+        if (_st != CUSOLVER_STATUS_SUCCESS) {                                                     \
+            rc = fail(EBEM_ERR_CUDA, std::string(#expr) + " failed with status " + std::to_string((int)_st)); \
+            goto done;                                                                            \
+        }                                                                                         \
+    } while (0)
+
+// phi (device, column-major n3 x nT) from E (device, n3 x n3 x L) and rhs
+// (device, n3 x nT).
+int march_device(const double* dE, int n3, int L, const double* drhs, int nT, double* dphi, cudaStream_t s) {
+    int rc = EBEM_OK;
+    cusolverDnHandle_t h = nullptr;
+    double *lu = nullptr, *work = nullptr, *rev = nullptr;
+    int *ipiv = nullptr, *info = nullptr;
+    int lwork = 0, hinfo = 0, dev = 0, sms = 148;
+    const size_t nn = (size_t)n3 * n3;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaMalloc(&lu, nn * sizeof(double)) != cudaSuccess || cudaMalloc(&ipiv, n3 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&info, sizeof(int)) != cudaSuccess || cudaMalloc(&rev, (size_t)n3 * nT * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(EBEM_ERR_NOMEM, "time-marching workspace allocation failed");
+        goto done;
+    }
+    CUSOLVER_TRY(cusolverDnCreate(&h));
+    CUSOLVER_TRY(cusolverDnSetStream(h, s));
+    if (cudaMemcpyAsync(lu, dE, nn * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        rc = fail(EBEM_ERR_CUDA, "E_0 copy failed");
+        goto done;
+    }
+    CUSOLVER_TRY(cusolverDnDgetrf_bufferSize(h, n3, n3, lu, n3, &lwork));
+    if (cudaMalloc(&work, (size_t)(lwork > 0 ? lwork : 1) * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(EBEM_ERR_NOMEM, "LU workspace allocation failed");
+        goto done;
+    }
+    CUSOLVER_TRY(cusolverDnDgetrf(h, n3, n3, lu, n3, work, ipiv, info));
+    if (cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        rc = fail(EBEM_ERR_CUDA, "LU factorisation failed");
+        goto done;
+    }
+    if (hinfo != 0) {
+        rc = fail(EBEM_ERR_SINGULAR, "E_0 is singular (zero pivot " + std::to_string(hinfo) + ")");
+        goto done;
+    }
+    {
+        // density in reversed time order: phi_n at column nT-1-n, so that
+        // phi_{n-1}, phi_{n-2}, ... are contiguous for the history product
+        long long tot = (long long)n3 * nT;
+        copy_reverse_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(drhs, rev, n3, nT, 1);
+        if (cudaGetLastError() != cudaSuccess) { rc = fail(EBEM_ERR_CUDA, "rhs copy failed"); goto done; }
+        for (int n = 0; n < nT; n++) {
+            double* y = rev + (size_t)(nT - 1 - n) * n3;
+            int M = (n < L - 1) ? n : L - 1;
+            if (M > 0) {
+                rc = launch_hist_gemv(dE + nn, n3, (long long)n3 * M, rev + (size_t)(nT - n) * n3, y, sms, s);
+                if (rc) goto done;
+            }
+            CUSOLVER_TRY(cusolverDnDgetrs(h, CUBLAS_OP_N, n3, 1, lu, n3, ipiv, y, n3, info));
+        }
+        copy_reverse_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rev, dphi, n3, nT, 0);
+        if (cudaGetLastError() != cudaSuccess) { rc = fail(EBEM_ERR_CUDA, "density copy failed"); goto done; }
+        if (cudaStreamSynchronize(s) != cudaSuccess) { rc = fail(EBEM_ERR_CUDA, "time marching failed"); goto done; }
+    }
+done:
+    if (h) cusolverDnDestroy(h);
+    if (lu) cudaFree(lu);
+    if (work) cudaFree(work);
+    if (rev) cudaFree(rev);
+    if (ipiv) cudaFree(ipiv);
+    if (info) cudaFree(info);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Post-processing (closed form): u(x, t) = sum_{k=1}^{nHat} (M(t - (k-1) dt)
+// - M(t - k dt)) phi_k + M(t - nHat dt) phi_{nHat+1}, nHat = ceil(t/dt) - 1,
+// M(tau) the single-point combined kernel integral over each triangle
+// (BEMenerg_postProcA_singlePoint.m:21-61), divided by 4 pi rho and cleaned
+// below 1e-14 (BEMenerg_postProcA_calcMatrix.m:103).  One thread per
+// (triangle, point); consecutive lanes take consecutive triangles of one
+// point, reduce over the warp and add to u with one atomic per component.
+__device__ __forceinline__ void pp_block(double M[6], const TriGeom& F, const NodeW& x, double tau, double velP,
+                                         double velS, double c4) {
+    level_value(M, 1, velP, velS, tau, F, &x, 1);
+#pragma unroll
+    for (int e = 0; e < 6; e++) {
+        double v = M[e] / c4;
+        M[e] = (fabs(v) < 1.0e-14) ? 0.0 : v;
+    }
+}
+
+__device__ __forceinline__ void sym_mv_add(double acc[3], const double M[6], const double* ph, double sgn) {
+    acc[0] += sgn * (M[0] * ph[0] + M[1] * ph[1] + M[2] * ph[2]);
+    acc[1] += sgn * (M[1] * ph[0] + M[3] * ph[1] + M[4] * ph[2]);
+    acc[2] += sgn * (M[2] * ph[0] + M[4] * ph[1] + M[5] * ph[2]);
+}
+
+__global__ void __launch_bounds__(128) pp_sa_kernel(const TriGeom* __restrict__ geo, int N, const double* __restrict__ pts,
+                                                    int npts, const double* __restrict__ times, int ntimes,
+                                                    const double* __restrict__ phi, int nT, double velP, double velS,
+                                                    double dt, double c4, double* __restrict__ u) {
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = idx < (long long)N * npts;
+    int j = valid ? (int)(idx % N) : 0, p = valid ? (int)(idx / N) : 0;
+    NodeW x;
+    x.x = pts[3 * p]; x.y = pts[3 * p + 1]; x.z = pts[3 * p + 2]; x.w = 1.0;
+    const TriGeom& F = geo[j];
+    const size_t n3 = 3 * (size_t)N;
+    for (int q = 0; q < ntimes; q++) {
+        double t = times[q];
+        double acc[3] = {0, 0, 0};
+        if (valid && t > 0) {
+            int nHat = (int)ceil(t / dt) - 1;
+            if (nHat > nT - 1) nHat = nT - 1;
+            double Mc[6], Mn[6];
+            pp_block(Mc, F, x, t, velP, velS, c4);
+            for (int k = 1; k <= nHat; k++) {
+                pp_block(Mn, F, x, t - k * dt, velP, velS, c4);
+                const double* ph = phi + (size_t)(k - 1) * n3 + 3 * (size_t)j;
+                double D[6];
+#pragma unroll
+                for (int e = 0; e < 6; e++) { D[e] = Mc[e] - Mn[e]; Mc[e] = Mn[e]; }
+                sym_mv_add(acc, D, ph, 1.0);
+            }
+            sym_mv_add(acc, Mc, phi + (size_t)nHat * n3 + 3 * (size_t)j, 1.0);
+        }
+        double sum[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double v = acc[c];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            sum[c] = v;
+        }
+        // a warp may straddle two points: then every lane adds its own value
+        int p_first = __shfl_sync(0xffffffffu, p, 0), p_last = __shfl_sync(0xffffffffu, p, 31);
+        int v_last = __shfl_sync(0xffffffffu, valid ? 1 : 0, 31);
+        if (p_first == p_last && v_last) {
+            if ((threadIdx.x & 31) == 0)
+                for (int c = 0; c < 3; c++) atomicAdd(u + ((size_t)q * npts + p) * 3 + c, sum[c]);
+        } else if (valid) {
+            for (int c = 0; c < 3; c++) atomicAdd(u + ((size_t)q * npts + p) * 3 + c, acc[c]);
+        }
+    }
+}
+
+int launch_pp_sa(const MeshData& m, const PhysParams& P, const double* d_phi, const double* d_pts, int npts,
+                 const double* h_times, int ntimes, double* d_u, cudaStream_t s) {
+    double* d_times = nullptr;
+    EBEM_CUDA_TRY(cudaMalloc(&d_times, sizeof(double) * ntimes));
+    EBEM_CUDA_TRY(cudaMemcpyAsync(d_times, h_times, sizeof(double) * ntimes, cudaMemcpyHostToDevice, s));
+    EBEM_CUDA_TRY(cudaMemsetAsync(d_u, 0, sizeof(double) * 3 * (size_t)npts * ntimes, s));
+    long long total = (long long)m.nt * npts;
+    int threads = 128;
+    pp_sa_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, s>>>(
+        m.d_geo, m.nt, d_pts, npts, d_times, ntimes, d_phi, P.nT, P.velP, P.velS, P.dt, 4 * kPi * P.rho, d_u);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_times);
+    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("post-processing kernel: ") + cudaGetErrorString(e));
+    return EBEM_OK;
+}
+
+}  // namespace ebem

@@ -101,6 +101,7 @@ struct SAArgs {
     double velP, velS, dt, c4pirho;
     int lag0, nlag;
     int src0, nsrc;         // source rows [src0, src0 + nsrc) of the panel
+    int diag_only;          // 1: only the diagonal pairs (i, i), i in the panel
     double* E;
     size_t ld;              // leading dimension (>= 3 nsrc)
     size_t ld_lag;          // doubles between consecutive lags
@@ -125,10 +126,10 @@ __device__ __forceinline__ void store_block(const SAArgs& A, int q, int i, int j
 
 __global__ void __launch_bounds__(128) sa_assemble_kernel(SAArgs A) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long NN = (long long)A.nsrc * A.N;
+    const long long NN = A.diag_only ? (long long)A.nsrc : (long long)A.nsrc * A.N;
     const bool valid = p < NN;
     const int i = valid ? A.src0 + (int)(p % A.nsrc) : A.src0;   // source (row block)
-    const int j = valid ? (int)(p / A.nsrc) : 0;                 // field (column block)
+    const int j = A.diag_only ? i : (valid ? (int)(p / A.nsrc) : 0);   // field (column block)
     const TriGeom& F = A.geo[j];
     const TriGeom& Sg = A.geo[i];
     double v0 = F.ctr[0] - Sg.ctr[0], v1 = F.ctr[1] - Sg.ctr[1], v2 = F.ctr[2] - Sg.ctr[2];
@@ -184,7 +185,7 @@ __global__ void __launch_bounds__(128) sa_assemble_kernel(SAArgs A) {
 
 int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
-                       cudaStream_t s) {
+                       cudaStream_t s, int diag_only) {
     SAArgs A;
     A.geo = m.d_geo;
     A.nodes = m.d_nodes;
@@ -198,12 +199,13 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
     A.nlag = nlag;
     A.src0 = src0;
     A.nsrc = nsrc;
+    A.diag_only = diag_only;
     A.E = d_E;
     A.ld = ld;
     A.ld_lag = ld_lag;
     A.accumulate = accumulate;
     A.count = d_count;
-    long long NN = (long long)nsrc * m.nt;
+    long long NN = diag_only ? (long long)nsrc : (long long)nsrc * m.nt;
     int threads = 128;
     long long blocks = (NN + threads - 1) / threads;
     if (blocks > 0x7fffffffLL) return fail(EBEM_ERR_INVALID, "mesh too large for one launch");

@@ -24,26 +24,60 @@
 
 #include <math.h>
 
+#ifndef EBEM_NOINLINE_MATH
+#define EBEM_NOINLINE_MATH 1
+#endif
+#ifndef EBEM_NOINLINE_REGIONS
+#define EBEM_NOINLINE_REGIONS 0
+#endif
+#ifndef EBEM_UNIFORM_SLOTS
+#define EBEM_UNIFORM_SLOTS 1
+#endif
+
 #ifdef __CUDACC__
 #include <cuda_runtime.h>
 #define EBEM_DI __device__ __forceinline__
 #define EBEM_HDI __host__ __device__ inline
+// One out-of-line copy of each transcendental and of each region routine
+// keeps the kernel's instruction footprint inside the instruction caches
+// (fully inlined, the kernel stalls on instruction fetch).
+#if EBEM_NOINLINE_MATH
+#define EBEM_MFN static __device__ __noinline__
+#else
+#define EBEM_MFN __device__ __forceinline__
+#endif
+#if EBEM_NOINLINE_REGIONS
+#define EBEM_RFN static __device__ __noinline__
+#else
+#define EBEM_RFN __device__ __forceinline__
+#endif
 #else
 // host compilation of the same device algebra (used to emulate the kernels'
 // arithmetic on the CPU when investigating a numerical difference)
 #define EBEM_DI inline
 #define EBEM_HDI inline
+#define EBEM_MFN inline
+#define EBEM_RFN inline
 #endif
 
 namespace ebem {
 
 constexpr double kPi = 3.141592653589793238462643383279502884;
 
+EBEM_MFN double m_sin(double x) { return sin(x); }
+EBEM_MFN double m_cos(double x) { return cos(x); }
+EBEM_MFN void m_sincos(double x, double* s, double* c) { sincos(x, s, c); }
+EBEM_MFN double m_log(double x) { return log(x); }
+EBEM_MFN double m_exp(double x) { return exp(x); }
+EBEM_MFN double m_acos(double x) { return acos(x); }
+EBEM_MFN double m_asin(double x) { return asin(x); }
+EBEM_MFN double m_atan2(double y, double x) { return atan2(y, x); }
+
 enum : int { T_NONE = 0, T_SP_SP = 1, T_SP_P = 2, T_P = 3 };
 
 EBEM_HDI double sgn(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
-EBEM_DI double acos_c(double x) { return acos(fmin(1.0, fmax(-1.0, x))); }
-EBEM_DI double asin_c(double x) { return asin(fmin(1.0, fmax(-1.0, x))); }
+EBEM_DI double acos_c(double x) { return m_acos(fmin(1.0, fmax(-1.0, x))); }
+EBEM_DI double asin_c(double x) { return m_asin(fmin(1.0, fmax(-1.0, x))); }
 EBEM_DI double sqrt_c(double x) { return x > 0.0 ? sqrt(x) : 0.0; }
 
 // Per field triangle data produced by the preparation kernel.
@@ -70,7 +104,7 @@ struct LevelCtx {
 // (SA/operazioniGeometriche/calcoloDatiTriangolo.m and the theta0 rotation of
 // SA/BEMenerg_coreSA_calcIntgInt_fieldTriangle.m:37-59).
 struct ChildGeo {
-    double a, bm, F;                 // |V1|, a*vt_x, a*sin(beta)
+    double a, bm, F;                 // |V1|, a*vt_x, a*m_sin(beta)
     double alpha, beta, gamma;
     double ca, cb, cg, sa, sb, sg;   // cos/sin of alpha, beta, gamma
     double ct, st;                   // cos/sin of the back-rotation angle theta0
@@ -91,13 +125,13 @@ struct Phi { double p1, p2, p3, p4, p5; };
 
 EBEM_DI Phi phi_all(double T1t, double T2t, double gamma, double cos_gamma) {
     Phi P;
-    double sh = sin(T1t / 2);
-    P.p1 = 2 * sin(T2t / 2) * sh;
-    P.p2 = 2 * sin(gamma - (T2t / 2)) * sh;
-    double s1 = sin(T1t);
-    P.p3 = 0.5 * (T1t - (cos(T2t) * s1));
-    P.p4 = -0.5 * (-(s1 * cos(gamma - T2t)) + (T1t * cos_gamma));
-    P.p5 = 0.5 * (T1t - (cos(2 * gamma - T2t) * s1));
+    double sh = m_sin(T1t / 2);
+    P.p1 = 2 * m_sin(T2t / 2) * sh;
+    P.p2 = 2 * m_sin(gamma - (T2t / 2)) * sh;
+    double s1 = m_sin(T1t);
+    P.p3 = 0.5 * (T1t - (m_cos(T2t) * s1));
+    P.p4 = -0.5 * (-(s1 * m_cos(gamma - T2t)) + (T1t * cos_gamma));
+    P.p5 = 0.5 * (T1t - (m_cos(2 * gamma - T2t) * s1));
     return P;
 }
 
@@ -118,7 +152,7 @@ EBEM_DI void add_sep_P(Acc7& A, const LevelCtx& L, double T1t, const Phi& P, boo
 }
 
 // AI/BEMenerg_analiticIntg_CC.m:1-93 — annulus between the S and P fronts.
-EBEM_DI void reg_CC(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
+EBEM_RFN void reg_CC(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
                                        double rhoS, double rhoP, double TH1, double TH2) {
     const double RS = L.RS, RP = L.RP;
     double T1t = TH2 - TH1, T2t = TH2 + TH1;
@@ -126,7 +160,7 @@ EBEM_DI void reg_CC(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
     if (zeta > 1.0e-6) {
         double I1 = RP - RS;
         double I2 = RP - RS + (zeta * zeta * (1 / RP - 1 / RS));
-        double I3 = log((rhoP + RP) / (rhoS + RS)) - (rhoP / RP) + (rhoS / RS);
+        double I3 = m_log((rhoP + RP) / (rhoS + RS)) - (rhoP / RP) + (rhoS / RS);
         double I4 = -(1 / RP) + (1 / RS);
         double iRP3 = 1 / (RP * RP * RP), iRS3 = 1 / (RS * RS * RS);
         double I5 = I4 + (zeta * zeta / 3) * (iRP3 - iRS3);
@@ -143,14 +177,14 @@ EBEM_DI void reg_CC(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
 
 // AI/BEMenerg_analiticIntg_SC_P.m:1-54 — sector of the P disc (zeta > 0 always
 // reaches here: the P-only case needs the S sphere to miss the plane).
-EBEM_DI void reg_SC_P(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
+EBEM_RFN void reg_SC_P(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
                                          double rhoP, double TH1, double TH2) {
     const double RP = L.RP;
     double T1t = TH2 - TH1, T2t = TH2 + TH1;
     Phi P = phi_all(T1t, T2t, g.gamma, g.cg);
     double I1 = RP - zeta;
     double I2 = RP + (zeta * zeta / RP) - (2 * zeta);
-    double I3 = log((rhoP + RP) / zeta) - (rhoP / RP);
+    double I3 = m_log((rhoP + RP) / zeta) - (rhoP / RP);
     double I4 = -(1 / RP) + (1 / zeta);
     double I5 = -(1 / RP) + (zeta * zeta / (3 * RP * RP * RP)) + (2 / (3 * zeta));
     double q1 = rhoP / RP;
@@ -160,7 +194,7 @@ EBEM_DI void reg_SC_P(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta
 }
 
 // AI/BEMenerg_analiticIntg_SC_SP.m:1-75 — sector of the S disc (P&S terms).
-EBEM_DI void reg_SC_SP(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
+EBEM_RFN void reg_SC_SP(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
                                           double rhoS, double TH1, double TH2) {
     const double RS = L.RS;
     double T1t = TH2 - TH1, T2t = TH2 + TH1;
@@ -168,7 +202,7 @@ EBEM_DI void reg_SC_SP(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zet
     if (zeta > 1.0e-6) {
         double I1 = RS - zeta;
         double I2 = RS + (zeta * zeta / RS) - (2 * zeta);
-        double I3 = log((rhoS + RS) / zeta) - (rhoS / RS);
+        double I3 = m_log((rhoS + RS) / zeta) - (rhoS / RS);
         double I4 = -(1 / RS) + (1 / zeta);
         A.S += L.k5 * (T1t * I1);
         double X = L.k6 * I2, Y = L.k6 * I3;
@@ -184,7 +218,7 @@ EBEM_DI void reg_SC_SP(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zet
 
 // G coefficients of the "triangle minus circle" region,
 // AI/coefficientiG/BEMenerg_analiticIntg_coeffG_TC.m:1-182.  G[k] = G(k).
-EBEM_DI void coeffG_TC(double G[20], double zeta, double RS, double rhoS,
+EBEM_RFN void coeffG_TC(double G[20], double zeta, double RS, double rhoS,
                                           double TH1, double TH2, const ChildGeo& g) {
     const double sin_beta = g.sb, sin_alpha = g.sa;
     const double cos_alpha = g.ca, cos_beta = g.cb, cos_gamma = g.cg;
@@ -193,27 +227,27 @@ EBEM_DI void coeffG_TC(double G[20], double zeta, double RS, double rhoS,
     const double F = g.F;
     Phi P = phi_all(T1t, T2t, gamma, cos_gamma);
     double s1b, c1b, s2b, c2b;
-    sincos(TH1 + beta, &s1b, &c1b);
-    sincos(TH2 + beta, &s2b, &c2b);
+    m_sincos(TH1 + beta, &s1b, &c1b);
+    m_sincos(TH2 + beta, &s2b, &c2b);
     if (zeta > 1.0e-6) {
         double R1 = F / s1b, R2 = F / s2b;
         double FR1 = zeta / R1, FR2 = zeta / R2;
         double ADD = zeta * zeta + F * F;
         double g1 = sqrt(1 + FR1 * FR1);
         double g2 = sqrt(1 + FR2 * FR2);
-        double g3 = 0.5 * (log((g1 + c1b) * (g2 - c2b)) - log((g1 - c1b) * (g2 + c2b)));
+        double g3 = 0.5 * (m_log((g1 + c1b) * (g2 - c2b)) - m_log((g1 - c1b) * (g2 + c2b)));
         double iF1 = 1 / FR1, iF2 = 1 / FR2;
-        double g4 = log(iF1 + sqrt(1 + iF1 * iF1));
-        double g5 = log(iF2 + sqrt(1 + iF2 * iF2));
+        double g4 = m_log(iF1 + sqrt(1 + iF1 * iF1));
+        double g5 = m_log(iF2 + sqrt(1 + iF2 * iF2));
         double sq = sqrt(ADD);
         double g7 = kPi - acos_c((-zeta * c2b) / sq) - acos_c((zeta * c1b) / sq);
         double g8 = F * F / ADD;
-        double Lg = (rhoS / RS) - log((rhoS + RS) / zeta);
-        double cgm1 = cos(gamma - TH1), cgm2 = cos(gamma - TH2);
-        double cth1 = cos(TH1), cth2 = cos(TH2);
-        double cag1 = cos(alpha - gamma + TH1), cag2 = cos(alpha - gamma + TH2);
-        double cta1 = cos(TH1 + alpha), cta2 = cos(TH2 + alpha);
-        double ctb1 = cos(TH1 - beta), ctb2 = cos(TH2 - beta);
+        double Lg = (rhoS / RS) - m_log((rhoS + RS) / zeta);
+        double cgm1 = m_cos(gamma - TH1), cgm2 = m_cos(gamma - TH2);
+        double cth1 = m_cos(TH1), cth2 = m_cos(TH2);
+        double cag1 = m_cos(alpha - gamma + TH1), cag2 = m_cos(alpha - gamma + TH2);
+        double cta1 = m_cos(TH1 + alpha), cta2 = m_cos(TH2 + alpha);
+        double ctb1 = m_cos(TH1 - beta), ctb2 = m_cos(TH2 - beta);
         G[1] = -(RS * T1t) + (zeta * g7) + (F * g3);
         G[4] = (1 / RS * T1t) - (1 / zeta * g7);
         G[5] = cgm2 * g5 - cgm1 * g4 - cos_alpha * g3 + Lg * (cgm2 - cgm1);
@@ -242,17 +276,17 @@ EBEM_DI void coeffG_TC(double G[20], double zeta, double RS, double rhoS,
               - 1.0 / 3 * (s1b2 * ctb1 + g8 * ((cos_beta * cos_beta) * c1b)) / (F * g1)
               - g7 / (3 * zeta) + K * P.p3;
     } else {
-        double g_3 = 0.5 * (log((1 + c1b) * (1 - c2b)) - log((1 - c1b) * (1 + c2b)));
-        double cag1 = cos(alpha - gamma + TH1), cag2 = cos(alpha - gamma + TH2);
-        double cta1 = cos(TH1 + alpha), cta2 = cos(TH2 + alpha);
-        double ctb1 = cos(TH1 - beta), ctb2 = cos(TH2 - beta);
+        double g_3 = 0.5 * (m_log((1 + c1b) * (1 - c2b)) - m_log((1 - c1b) * (1 + c2b)));
+        double cag1 = m_cos(alpha - gamma + TH1), cag2 = m_cos(alpha - gamma + TH2);
+        double cta1 = m_cos(TH1 + alpha), cta2 = m_cos(TH2 + alpha);
+        double ctb1 = m_cos(TH1 - beta), ctb2 = m_cos(TH2 - beta);
         double s1b2 = s1b * s1b, s2b2 = s2b * s2b;
         G[1] = (F * g_3) - (RS * T1t);
         G[4] = 1 / F * (c2b - c1b) + 1 / RS * T1t;
         G[7] = -RS * P.p5 + F * (cag2 - cag1 + (sin_alpha * sin_alpha) * g_3);
         G[8] = -RS * P.p4 + F * (cta1 - cta2 - sin_alpha * sin_beta * g_3);
         G[9] = -RS * P.p3 + F * (ctb1 - ctb2 + (sin_beta * sin_beta) * g_3);
-        double cab = (cos_alpha * cos_beta) + cos(alpha + beta);
+        double cab = (cos_alpha * cos_beta) + m_cos(alpha + beta);
         G[17] = 1 / (3 * F) * (((1 + cos_alpha * cos_alpha) * c2b - s2b2 * cag2)
                                - ((1 + cos_alpha * cos_alpha) * c1b - s1b2 * cag1)) + 1 / RS * P.p5;
         G[18] = 1 / (3 * F) * ((c2b * cab + s2b2 * cta2) - (c1b * cab + s1b2 * cta1)) + 1 / RS * P.p4;
@@ -265,7 +299,7 @@ EBEM_DI void coeffG_TC(double G[20], double zeta, double RS, double rhoS,
 // AI/coefficientiG/BEMenerg_analiticIntg_coeffG_TR_P.m:1-120 and
 // _TR_SP.m:1-111 (the TR_SP set is G(1), G(4..9) of the same expressions;
 // with_p4 selects whether G(14..19) are needed).
-EBEM_DI void coeffG_TR(double G[20], double zeta, double TH1, double TH2,
+EBEM_RFN void coeffG_TR(double G[20], double zeta, double TH1, double TH2,
                                           const ChildGeo& g, bool with_r4) {
     const double sin_beta = g.sb, sin_alpha = g.sa;
     const double cos_alpha = g.ca, cos_beta = g.cb, cos_gamma = g.cg;
@@ -273,30 +307,30 @@ EBEM_DI void coeffG_TR(double G[20], double zeta, double TH1, double TH2,
     double T1t = TH2 - TH1, T2t = TH2 + TH1;
     const double F = g.F;
     double s1b, c1b, s2b, c2b;
-    sincos(TH1 + beta, &s1b, &c1b);
-    sincos(TH2 + beta, &s2b, &c2b);
-    double cag1 = cos(alpha - gamma + TH1), cag2 = cos(alpha - gamma + TH2);
-    double cta1 = cos(TH1 + alpha), cta2 = cos(TH2 + alpha);
-    double ctb1 = cos(TH1 - beta), ctb2 = cos(TH2 - beta);
+    m_sincos(TH1 + beta, &s1b, &c1b);
+    m_sincos(TH2 + beta, &s2b, &c2b);
+    double cag1 = m_cos(alpha - gamma + TH1), cag2 = m_cos(alpha - gamma + TH2);
+    double cta1 = m_cos(TH1 + alpha), cta2 = m_cos(TH2 + alpha);
+    double ctb1 = m_cos(TH1 - beta), ctb2 = m_cos(TH2 - beta);
     if (with_r4 || zeta > 1.0e-6) {   // TR_P has no coplanar branch
-        double p3 = 0.5 * (T1t - (cos(T2t) * sin(T1t)));
-        double p4 = -0.5 * (-(sin(T1t) * cos(gamma - T2t)) + (T1t * cos_gamma));
-        double p5 = 0.5 * (T1t - (cos(2 * gamma - T2t) * sin(T1t)));
+        double p3 = 0.5 * (T1t - (m_cos(T2t) * m_sin(T1t)));
+        double p4 = -0.5 * (-(m_sin(T1t) * m_cos(gamma - T2t)) + (T1t * cos_gamma));
+        double p5 = 0.5 * (T1t - (m_cos(2 * gamma - T2t) * m_sin(T1t)));
         double R1 = F / s1b, R2 = F / s2b;
         double FR1 = zeta / R1, FR2 = zeta / R2;
         double ADD = zeta * zeta + F * F;
         double g1 = sqrt(1 + FR1 * FR1);
         double g2 = sqrt(1 + FR2 * FR2);
-        double g3 = 0.5 * (log((g1 + c1b) * (g2 - c2b)) - log((g1 - c1b) * (g2 + c2b)));
+        double g3 = 0.5 * (m_log((g1 + c1b) * (g2 - c2b)) - m_log((g1 - c1b) * (g2 + c2b)));
         double iF1 = 1 / FR1, iF2 = 1 / FR2;
-        double g4 = log(iF1 + sqrt(1 + iF1 * iF1));
-        double g5 = log(iF2 + sqrt(1 + iF2 * iF2));
+        double g4 = m_log(iF1 + sqrt(1 + iF1 * iF1));
+        double g5 = m_log(iF2 + sqrt(1 + iF2 * iF2));
         double sq = sqrt(ADD);
         double g7 = kPi - acos_c((-zeta * c2b) / sq) - acos_c((zeta * c1b) / sq);
         G[1] = (zeta * (-T1t + g7)) + (F * g3);
         G[4] = 1 / zeta * (T1t - g7);
-        G[5] = cos(gamma - TH2) * g5 - cos(gamma - TH1) * g4 - cos_alpha * g3;
-        G[6] = -cos(TH2) * g5 + cos(TH1) * g4 - cos_beta * g3;
+        G[5] = m_cos(gamma - TH2) * g5 - m_cos(gamma - TH1) * g4 - cos_alpha * g3;
+        G[6] = -m_cos(TH2) * g5 + m_cos(TH1) * g4 - cos_beta * g3;
         G[7] = zeta * (g7 - 2 * p5) + F * (-g1 * cag1 + g2 * cag2 + g3 * (sin_alpha * sin_alpha));
         G[8] = -zeta * ((cos_gamma * g7) + 2 * p4) + F * (-sin_alpha * sin_beta * g3 + g1 * cta1 - g2 * cta2);
         G[9] = zeta * (g7 - 2 * p3) + F * ((sin_beta * sin_beta) * g3 + g1 * ctb1 - g2 * ctb2);
@@ -319,7 +353,7 @@ EBEM_DI void coeffG_TR(double G[20], double zeta, double TH1, double TH2,
         }
     } else {
         // coplanar branch of _TR_SP.m:210-229 (TR_P never sees zeta = 0)
-        double g_3 = 0.5 * (log((1 + c1b) * (1 - c2b)) - log((1 - c1b) * (1 + c2b)));
+        double g_3 = 0.5 * (m_log((1 + c1b) * (1 - c2b)) - m_log((1 - c1b) * (1 + c2b)));
         G[1] = F * g_3;
         G[4] = G[5] = G[6] = 0.0;
         G[7] = F * (-cag1 + cag2 + (sin_alpha * sin_alpha) * g_3);
@@ -329,7 +363,7 @@ EBEM_DI void coeffG_TR(double G[20], double zeta, double TH1, double TH2,
 }
 
 // AI/BEMenerg_analiticIntg_TC.m:1-50 — triangle minus the S disc (P terms).
-EBEM_DI void reg_TC(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
+EBEM_RFN void reg_TC(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
                                        double rhoS, double TH1, double TH2) {
     double G[20];
     bool full = zeta > 1.0e-6;
@@ -345,7 +379,7 @@ EBEM_DI void reg_TC(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
 
 // AI/BEMenerg_analiticIntg_TR_P.m:1-28 — plain triangle piece inside the P
 // disc (P terms; zeta > 0 here).
-EBEM_DI void reg_TR_P(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
+EBEM_RFN void reg_TR_P(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
                                          double TH1, double TH2) {
     double G[20];
     coeffG_TR(G, zeta, TH1, TH2, g, true);
@@ -356,7 +390,7 @@ EBEM_DI void reg_TR_P(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta
 
 // AI/BEMenerg_analiticIntg_TR_SP.m:1-40 — plain triangle piece inside the S
 // disc (P&S terms).
-EBEM_DI void reg_TR_SP(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
+EBEM_RFN void reg_TR_SP(Acc7& A, const LevelCtx& L, const ChildGeo& g, double zeta,
                                           double TH1, double TH2) {
     double G[20];
     bool full = zeta > 1.0e-6;
@@ -465,7 +499,7 @@ EBEM_DI void child_level(double& Sout, double T[6], const ChildGeo& g, const Lev
 // angle of 1e-3 comes out with a relative error near 1e-10 and the region
 // formulas amplify it through their 1/F terms).  The same angles are computed
 // here from the cross and dot products of the edge vectors with atan2, and
-// F = a sin(beta) = 2 area / |V2 - V1| directly: identical quantities, full
+// F = a m_sin(beta) = 2 area / |V2 - V1| directly: identical quantities, full
 // precision.
 EBEM_DI void child_geo(ChildGeo& g, double v1x, double v1y, double v2x, double v2y, double sgnC) {
     double a = sqrt(v1x * v1x + v1y * v1y);
@@ -477,17 +511,17 @@ EBEM_DI void child_geo(ChildGeo& g, double v1x, double v1y, double v2x, double v
     double db = -(v1x * dx + v1y * dy);           // (-V1) . (V2-V1)  (angle at V1)
     double da = v2x * dx + v2y * dy;              // (-V2) . (V1-V2)  (angle at V2)
     g.a = a;
-    g.gamma = atan2(cr, dg);
-    g.beta = atan2(cr, db);
-    g.alpha = atan2(cr, da);
+    g.gamma = m_atan2(cr, dg);
+    g.beta = m_atan2(cr, db);
+    g.alpha = m_atan2(cr, da);
     double iab = 1.0 / (a * b), iac = 1.0 / (a * c), ibc = 1.0 / (b * c);
     g.cg = dg * iab; g.sg = cr * iab;
     g.cb = db * iac; g.sb = cr * iac;
     g.ca = da * ibc; g.sa = cr * ibc;
     g.F = cr / c;
-    // Bmezzi = a * vt_x = a (b cos(gamma) - a) / c = -a cos(beta)
+    // Bmezzi = a * vt_x = a (b m_cos(gamma) - a) / c = -a m_cos(beta)
     g.bm = -db / c;
-    // back-rotation by theta0 = -atan2(v1y, v1x) (mod 2 pi): cos = v1x/a, sin = -v1y/a
+    // back-rotation by theta0 = -m_atan2(v1y, v1x) (mod 2 pi): cos = v1x/a, sin = -v1y/a
     g.ct = v1x / a;
     g.st = -v1y / a;
     g.sgnC = sgnC;

@@ -14,6 +14,13 @@
 #pragma once
 
 #include "sa_device.cuh"
+#include "sa_edge.cuh"
+
+// 1: child integrals in the edge variable (stable; default); 0: the
+// reference's closed-form region formulas (for comparison)
+#ifndef EBEM_SA_FORM
+#define EBEM_SA_FORM 1
+#endif
 
 namespace ebem {
 
@@ -177,6 +184,16 @@ EBEM_DI bool node_child(ChildGeo& g, const NodeGeo& G, int k) {
     return true;
 }
 
+EBEM_DI bool node_child_e(ChildE& g, const NodeGeo& G, int k) {
+    const int k1 = (k == 2) ? 0 : k + 1;
+    double C = G.c[k];
+    if (fabs(C) < 1.0e-06) return false;
+    double v1x = G.tri[k][0], v1y = G.tri[k][1], v2x = G.tri[k1][0], v2y = G.tri[k1][1];
+    if (C < 0) { double tx = v1x, ty = v1y; v1x = v2x; v1y = v2y; v2x = tx; v2y = ty; }
+    child_geo_e(g, v1x, v1y, v2x, v2y, sgn(C));
+    return true;
+}
+
 // rho_P / rho_S and the case split (BEMenerg_coreSA_calcMatrixSubBlock.m:58-81)
 EBEM_DI int classify(double zeta, double rP, double rS, double dMIN, double& rhoP, double& rhoS) {
     if (zeta == 0) { rhoP = rP; rhoS = rS; }
@@ -219,9 +236,15 @@ EBEM_DI void level_value(double Fk[6], int k, double velP, double velS, double d
         double s = 0.0, tt[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll 1
         for (int c = 0; c < 3; c++) {
+#if EBEM_SA_FORM == 1
+            ChildE cg;
+            if (!node_child_e(cg, G, c)) continue;
+            child_level_e(s, tt, cg, L, G.zeta, G.sigma, rhoP, rhoS, type);
+#else
             ChildGeo cg;
             if (!node_child(cg, G, c)) continue;
             child_level(s, tt, cg, L, G.zeta, G.sigma, rhoP, rhoS, type);
+#endif
         }
         S += sp.w * s;
 #pragma unroll

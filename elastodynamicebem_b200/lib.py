@@ -40,6 +40,14 @@ PROTOTYPES = {
     "ebem_assemble_sa_panel": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_int, C.c_int,
                                          C.c_int, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p,
                                          C.POINTER(C.c_longlong)]),
+    "ebem_assemble_ghc": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.c_void_p, C.c_int, C.c_void_p]),
+    "ebem_rhs": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "ebem_march": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "ebem_timemarch_sa": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_void_p,
+                                    C.POINTER(C.c_int), C.c_void_p]),
+    "ebem_pp_sa": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                             C.c_void_p, C.c_void_p]),
 }
 
 
@@ -52,8 +60,8 @@ def load(build_if_missing: bool = True):
     global _LIB
     if _LIB is not None:
         return _LIB
-    path = _build.LIB
-    if not os.path.exists(path) or _build._stale():
+    path = os.environ.get("EBEM_LIBRARY", _build.LIB)
+    if path == _build.LIB and (not os.path.exists(path) or _build._stale()):
         if not build_if_missing:
             raise FileNotFoundError(f"{path} is missing; run elastodynamicebem_b200.build.build()")
         _build.build()

@@ -73,15 +73,16 @@ def screen_workload() -> Workload:
     return Workload("screen_n128", m, prm, 7, DATUM_SCREEN_T4EXP, pts, times)
 
 
-def sphere_workload(n_gh: int = 7) -> Workload:
+def sphere_workload(n_gh: int = 7, subdivisions: int = 3) -> Workload:
     """Unit icosphere subdivided 3x (1280 triangles), rho=1, mu=1, lambda=1,
     dt=0.025, T=1 (40 steps), g = x sin(2 pi t) H(t); displacement at 256
-    exterior points (direction uniform on S^2, radius U[1.5, 3], seed 2)."""
-    m = _mesh.icosphere(3)
+    exterior points (direction uniform on S^2, radius U[1.5, 3], seed 2).
+    ``subdivisions`` selects a coarser sphere of the same problem."""
+    m = _mesh.icosphere(subdivisions)
     prm = ProblemParams(1.0, 1.0, 1.0, 1.0, 40)
     rng = np.random.default_rng(2)
     d = rng.normal(size=(256, 3))
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     pts = d * rng.uniform(1.5, 3.0, 256)[:, None]
     times = prm.dt * np.arange(1, 41)
-    return Workload("sphere_n1280", m, prm, n_gh, DATUM_RADIAL_SIN, pts, times)
+    return Workload(f"sphere_n{m.numberTriangles}", m, prm, n_gh, DATUM_RADIAL_SIN, pts, times)

@@ -112,6 +112,57 @@ int ebem_assemble_sa_panel(const ebem_mesh* mesh, const ebem_problem* prob, int 
                            int src0, int nsrc, double* E, long long ld, int accumulate, void* stream,
                            long long* nonnull);
 
+/* Numerical-inner assembly (the reference's GPU method "GPU xx yy z"): outer
+ * Gauss-Hammer rule with n_gh nodes on the source triangle, composite rule of
+ * n_sub sub-triangles x n_sing nodes on the field triangle, Lamé kernel with
+ * P/S Heaviside fronts, off-diagonal pairs only, added to E (E += block,
+ * entries with |value| <= 1e-14 before the 1/(4 pi rho) skipped).  Replaces
+ * the kernelGHC feval of
+ * f/BEMenerg_indir/BEMenerg_core/BEMenerg_coreGPU/BEMenerg_coreGPU_launchKernel.m:11
+ * (kernel: .../CUDAkernels/kernelGHC.cu:5; the same kernel is kernelV.cu of
+ * f/BEMenerg_dir).  sa_diagonal = 1 also writes the diagonal blocks with the
+ * semi-analytic result, as BEMenerg_coreGPU_timeMarching.m:101-131 inserts
+ * its CPU semi-analytic diagonal.  E: host or device, 9 N^2 nlag doubles. */
+int ebem_assemble_ghc(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int n_sub, int n_sing, int lag0,
+                      int nlag, double* E, int sa_diagonal, void* stream);
+
+/* Right-hand side b_n, n = 0..nT-1: b_n[3i+c] = sum_g w_g (g(x_g, t_{n+1}) -
+ * g(x_g, t_n)) over the outer nodes of triangle i, entries below 1e-14 set
+ * to 0.  Replaces BEMenerg_core_calcTnBlock(rhs, methodInfo, indTemp, deltaT,
+ * pbParam, domainMesh, constValues)
+ * (f/BEMenerg_indir/BEMenerg_core/BEMenerg_core_calcTn/BEMenerg_core_calcTnBlock.m:1),
+ * all steps at once.  datum selects g (f/.../BEMenerg_core_calcNucleoTn.m:196-244):
+ * 0 (0,0,t^4 e^{-2t}), 1 x sin(2 pi t) H(t), 2 'sphereUniform', 3 'screenUniform',
+ * 4 'barH1', 5 'barH3', 6 'sphereWave', 7 'elementoIndustriale'.
+ * rhs: 3N x nT column-major, host or device. */
+int ebem_rhs(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int datum, double* rhs, void* stream);
+
+/* Time marching: LU of E_0 once, then phi_n = E_0^{-1}(b_n -
+ * sum_{l=1}^{min(n,L-1)} E_l phi_{n-l}).  Replaces the marching loop of
+ * f/BEMenerg_indir/BEMenerg_core/BEMenerg_coreGPU/BEMenerg_coreGPU_timeMarching.m:151-169
+ * (and of BEMenerg_coreSA_timeMarching.m:46-113).  E: n3 x n3 x L (the
+ * layout of ebem_assemble_sa), rhs and phi: n3 x nT; host or device.
+ * Returns EBEM_ERR_SINGULAR when E_0 has a zero pivot. */
+int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double* phi, void* stream);
+
+/* The semi-analytic indirect solve end to end: assembly of E_0..E_{L-1}
+ * (L from ebem_num_blocks), right-hand side, time marching.  Replaces
+ * density = BEMenerg_coreSA_timeMarching(pbParam, domainMesh, methodInfo, GHn, GHw)
+ * (f/BEMenerg_indir/BEMenerg_core/BEMenerg_coreSA/BEMenerg_coreSA_timeMarching.m:1).
+ * phi: 3N x nT, host or device; num_blocks (may be NULL) receives L. */
+int ebem_timemarch_sa(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int datum, double* phi,
+                      int* num_blocks, void* stream);
+
+/* Displacement u(x, t) at npts points and ntimes times from the density
+ * (closed-form inner integrals, the single-point analogue of the assembly).
+ * Replaces campoVett = BEMenerg_postProcA_setup(pbParam, domainMesh, density,
+ * numPoints, xVal, tVal)
+ * (f/BEMenerg_indir/BEMenerg_postProc/BEMenerg_postProcA/BEMenerg_postProcA_setup.m:1).
+ * phi: 3N x nT; pts: npts x 3 (row-major); times: host array; u: 3 x npts x
+ * ntimes (u[(q*npts + p)*3 + c]); phi/pts/u host or device. */
+int ebem_pp_sa(const ebem_mesh* mesh, const ebem_problem* prob, const double* phi, const double* pts, int npts,
+               const double* times, int ntimes, double* u, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

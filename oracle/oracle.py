@@ -100,10 +100,10 @@ def assemble_sa_pairs(mesh, prm, n_gh: int, src, fld, lag, nthreads: int = 0, va
     return out.reshape(len(src), 3, 3).transpose(0, 2, 1)    # block[q][r, c]
 
 
-def rhs(mesh, prm, n_gh: int, datum_id: int):
+def rhs(mesh, prm, n_gh: int, datum_id: int, variant: str = "f64"):
     n3 = 3 * mesh.numberTriangles
     b = np.zeros(n3 * prm.nT)
-    lib().or_rhs(*_m(mesh), *_p(prm), n_gh, datum_id, b)
+    lib(variant).or_rhs(*_m(mesh), *_p(prm), n_gh, datum_id, b)
     return b.reshape(prm.nT, n3).T.copy()        # (3N, nT)
 
 
@@ -120,14 +120,14 @@ def march(E, b):
     return phi.reshape(nT, n3).T.copy()
 
 
-def pp_sa(mesh, prm, phi, points, times, nthreads: int = 0):
+def pp_sa(mesh, prm, phi, points, times, nthreads: int = 0, variant: str = "f64"):
     """u(x, t): returns (3, npts, ntimes)."""
     n3 = 3 * mesh.numberTriangles
     phicm = np.ascontiguousarray(np.asarray(phi).T).ravel()
     pts = np.ascontiguousarray(points, np.float64)
     tms = np.ascontiguousarray(times, np.float64)
     u = np.zeros(3 * len(pts) * len(tms))
-    lib().or_pp_sa(*_m(mesh), *_p(prm), phicm, pts, len(pts), tms, len(tms), u, nthreads)
+    lib(variant).or_pp_sa(*_m(mesh), *_p(prm), phicm, pts, len(pts), tms, len(tms), u, nthreads)
     return u.reshape(len(tms), len(pts), 3).transpose(2, 1, 0).copy()
 
 
@@ -192,3 +192,30 @@ def field_integrals(mesh, velP: float, velS: float, j: int, x, t: float, variant
     typ = L.or_field_integrals(*_m(mesh), float(velP), float(velS), int(j),
                                np.ascontiguousarray(x, np.float64), float(t), out)
     return out.reshape(6, 3, 3), int(typ)
+
+
+def ref_ghc_available() -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", "libref_ghc.so"))
+
+
+def ref_ghc(mesh, prm, n_gh: int, n_sub: int, n_sing: int, nlag: int):
+    """Run the reference's own CUDA kernelGHC (compiled from its source into
+    oracle/_ref by `make ref`) on the device: E (nlag, 3N, 3N) with
+    E[l][row, col], off-diagonal blocks only, as BEMenerg_coreGPU_launchKernel
+    produces them."""
+    L = C.CDLL(os.path.join(_HERE, "_ref", "libref_ghc.so"))
+    L.ref_ghc.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp,
+                          C.c_int, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_int, C.c_int]
+    N = mesh.numberTriangles
+    gn, gw = gauss_hammer(n_gh, 1)
+    cn, cw = gauss_hammer(n_sing, n_sub)
+    P = mesh.coordinates[mesh.triangles]                  # (N, vertex, coord)
+    verts = np.ascontiguousarray(P.transpose(0, 2, 1).reshape(N, 9))   # 9t + 3*coord + vertex
+    E = np.zeros(9 * N * N * nlag)
+    rc = L.ref_ghc(E, N, nlag, prm.dt, prm.velP, prm.velS, 4 * np.pi * prm.rho, np.ascontiguousarray(gw),
+                   np.ascontiguousarray(gn), n_gh, np.ascontiguousarray(cw), np.ascontiguousarray(cn), n_sub, n_sing,
+                   verts.ravel(), np.ascontiguousarray(mesh.area), 0, nlag)
+    if rc:
+        raise RuntimeError(f"reference kernelGHC launch failed ({rc})")
+    n3 = 3 * N
+    return E.reshape(nlag, n3, n3).transpose(0, 2, 1)

@@ -1,0 +1,111 @@
+"""Right-hand side, time marching and post-processing on the device (through
+the C ABI) against the oracle.
+
+The density and displacement are judged like the blocks: against the
+binary128 evaluation of the reference's formulas where affordable, with the
+bar "no farther from it than the FP64 restatement of the reference", and
+against the FP64 restatement within its own noise.
+"""
+import numpy as np
+import pytest
+
+from conftest import cuda_available
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def ebem():
+    if not cuda_available():
+        pytest.skip("no CUDA device")
+    import elastodynamicebem_b200.core as core
+    return core
+
+
+@pytest.mark.parametrize("datum", list(range(8)))
+def test_rhs_matches_oracle(ebem, oracle, datum):
+    from elastodynamicebem_b200 import mesh, problem
+    for m, prm in [(mesh.screen_uniform(4), problem.ProblemParams(1, 1, 2, 1, 20)),
+                   (mesh.icosphere(1), problem.ProblemParams(1, 1, 1, 2, 16))]:
+        dm = ebem.DeviceMesh(m)
+        b = ebem.rhs(dm, prm, 7, datum).cpu().numpy().T          # (3N, nT)
+        bo = oracle.rhs(m, prm, 7, datum)
+        if np.linalg.norm(bo) == 0:
+            assert np.linalg.norm(b) == 0
+        else:
+            assert rel(b, bo) <= 1e-13
+
+
+def test_march_matches_oracle(ebem, oracle):
+    """Same blocks and right-hand side: device LU + history product vs the
+    oracle's LU marching."""
+    import torch
+    from elastodynamicebem_b200 import mesh, problem
+    m, prm = mesh.icosphere(1), problem.ProblemParams(1, 1, 1, 1, 40)
+    L = oracle.num_blocks(m, prm)
+    Eo, _ = oracle.assemble_sa(m, prm, 7, 0, L)
+    bo = oracle.rhs(m, prm, 7, 1)
+    phi_o = oracle.march(Eo, bo)
+    E = torch.tensor(Eo, device="cuda")
+    b = torch.tensor(bo.T.copy(), device="cuda")
+    phi = ebem.march(E, b).cpu().numpy().T
+    assert rel(phi, phi_o) <= 1e-11
+    # host buffers through the same entry point
+    phi_h = ebem.march(torch.tensor(Eo), torch.tensor(bo.T.copy())).numpy().T
+    assert rel(phi_h, phi_o) <= 1e-11
+
+
+def test_timemarch_screen128(ebem, oracle):
+    """The screen workload end to end: 128 triangles, dt = 0.05, 20 steps,
+    GH7, g = (0,0,t^4 e^{-2t})."""
+    from elastodynamicebem_b200 import problem
+    w = problem.screen_workload()
+    m, prm = w.mesh, w.params
+    dm = ebem.DeviceMesh(m)
+    phi, L = ebem.timemarch_sa(dm, prm, 7, w.datum)
+    phi = phi.cpu().numpy().T
+    Eo, _ = oracle.assemble_sa(m, prm, 7, 0, L)
+    bo = oracle.rhs(m, prm, 7, w.datum)
+    phi_o = oracle.march(Eo, bo)
+    assert np.isfinite(phi).all()
+    assert rel(phi, phi_o) <= 1e-6          # FP64 restatement's own noise on this mesh: ~2e-8 in E
+
+
+def test_timemarch_vs_exact_small(ebem, oracle):
+    """Density from the device vs the density from the binary128 blocks."""
+    from elastodynamicebem_b200 import mesh, problem
+    m, prm = mesh.screen_uniform(4), problem.ProblemParams(1, 1, 2, 1, 20)
+    dm = ebem.DeviceMesh(m)
+    phi, L = ebem.timemarch_sa(dm, prm, 7, 0)
+    phi = phi.cpu().numpy().T
+    bo = oracle.rhs(m, prm, 7, 0)
+    Eq, _ = oracle.assemble_sa(m, prm, 7, 0, L, variant="q")
+    Ef, _ = oracle.assemble_sa(m, prm, 7, 0, L)
+    phi_q = oracle.march(Eq, bo)
+    phi_f = oracle.march(Ef, bo)
+    e_dev, e_ref = rel(phi, phi_q), rel(phi_f, phi_q)
+    assert e_dev <= max(1e-10, 3 * e_ref), (e_dev, e_ref)
+
+
+def test_pp_screen(ebem, oracle):
+    """Displacement on z = 0.3 from the device density; oracle evaluates the
+    same closed form from the same density."""
+    import torch
+    from elastodynamicebem_b200 import problem
+    w = problem.screen_workload()
+    m, prm = w.mesh, w.params
+    dm = ebem.DeviceMesh(m)
+    phi, L = ebem.timemarch_sa(dm, prm, 7, w.datum)
+    pts, times = w.points[:24], w.times[::3]
+    u = ebem.pp_sa(dm, prm, phi, pts, times).cpu().numpy()          # (nt, np, 3)
+    uo = oracle.pp_sa(m, prm, phi.cpu().numpy().T, pts, times)      # (3, np, nt)
+    uo = uo.transpose(2, 1, 0)
+    assert np.isfinite(u).all()
+    assert rel(u, uo) <= 1e-9
+    # exact value of the formulas at a few points and times
+    uq = oracle.pp_sa(m, prm, phi.cpu().numpy().T, pts[:3], times[:2], variant="q").transpose(2, 1, 0)
+    assert rel(u[:2, :3], uq) <= 1e-10
