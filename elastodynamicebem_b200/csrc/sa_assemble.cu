@@ -23,6 +23,11 @@
 // times, once per lag that uses it).
 #include "ebem_internal.h"
 #include "sa_pair.cuh"
+#include "sa_warp.cuh"
+
+#ifndef EBEM_SA_KERNEL
+#define EBEM_SA_KERNEL 0    // 0: warp per pair when 3 n_gh <= 32, 1: always thread per pair
+#endif
 
 namespace ebem {
 
@@ -183,6 +188,230 @@ __global__ void __launch_bounds__(128) sa_assemble_kernel(SAArgs A) {
     }
 }
 
+__device__ __forceinline__ void store_entry(const SAArgs& A, int q, int i, int j, int e, double v) {
+    // entry e = 3 c + r of the column-major 3x3 block at (3(i - src0), 3j)
+    const int c = e / 3, r = e - 3 * c;
+    double* dst = A.E + (size_t)q * A.ld_lag + (3 * (size_t)j + c) * A.ld + 3 * (size_t)(i - A.src0) + r;
+    if (A.accumulate) *dst += v;
+    else *dst = v;
+}
+
+// One warp per pair (schedule described in sa_warp.cuh); requires 3 n_gh <= 32.
+#define EBEM_WARPS_PER_BLOCK 4
+__global__ void __launch_bounds__(32 * EBEM_WARPS_PER_BLOCK) sa_assemble_warp_kernel(SAArgs A) {
+    __shared__ WarpShared Wsh[EBEM_WARPS_PER_BLOCK];
+    __shared__ double glx[10], glw[10];
+    __shared__ unsigned long long blk_count;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    WarpShared& W = Wsh[wib];
+    if (threadIdx.x < 10) {
+        const int k = threadIdx.x < 5 ? threadIdx.x : threadIdx.x - 5;
+        glx[threadIdx.x] = (threadIdx.x < 5 ? -1.0 : 1.0) * gl_x(k);
+        glw[threadIdx.x] = gl_w(k);
+    }
+    if (threadIdx.x == 0) blk_count = 0;
+    __syncthreads();
+    const long long NP = A.diag_only ? (long long)A.nsrc : (long long)A.nsrc * A.N;
+    const long long nwarps = (long long)gridDim.x * EBEM_WARPS_PER_BLOCK;
+    const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    unsigned long long my_count = 0;
+    for (long long p = (long long)blockIdx.x * EBEM_WARPS_PER_BLOCK + wib; p < NP; p += nwarps) {
+        const int i = A.src0 + (int)(p % A.nsrc);
+        const int j = A.diag_only ? i : (int)(p / A.nsrc);
+        const TriGeom& F = A.geo[j];
+        const TriGeom& Sg = A.geo[i];
+        double v0 = F.ctr[0] - Sg.ctr[0], v1 = F.ctr[1] - Sg.ctr[1], v2 = F.ctr[2] - Sg.ctr[2];
+        double d = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        double distMin = d - F.maxL - Sg.maxL;
+        double distMax = d + F.maxL + Sg.maxL;
+        int llo = -1, lhi = -2;
+        for (int q = 0; q < A.nlag; q++) {
+            int l = A.lag0 + q;
+            if (lag_nonnull(l, A.velP, A.velS, A.dt, distMin, distMax)) {
+                if (llo < 0) llo = l;
+                lhi = l;
+            }
+        }
+        if (lane == 0 && llo >= 0) my_count += (unsigned long long)(lhi - llo + 1);
+        if (!A.accumulate) {
+            for (int idx = lane; idx < A.nlag * 9; idx += 32) {
+                const int q = idx / 9, e = idx - 9 * q, l = A.lag0 + q;
+                if (llo < 0 || l < llo || l > lhi) store_entry(A, q, i, j, e, 0.0);
+            }
+        }
+        if (llo < 0) continue;
+        // lane = child c of outer node g
+        LaneChild C;
+        C.live = false;
+        C.zeta = 0.0; C.sigma = 0.0; C.dMIN = 0.0; C.w = 0.0;
+        {
+            const int g = lane / 3, c = lane - 3 * (lane / 3);
+            if (g < A.n_gh) {
+                NodeW sp = A.nodes[(size_t)i * A.n_gh + g];
+                NodeGeo G;
+                node_geo(G, sp, F);
+                C.zeta = G.zeta;
+                C.sigma = G.sigma;
+                C.dMIN = G.dMIN;
+                C.w = sp.w;
+                if (node_child_e(C.g, G, c)) {
+                    C.live = true;
+                    m_sincos(C.g.gamma, &C.sg, &C.cg);
+                }
+            }
+        }
+        if (C.live) {
+            const ChildE& g = C.g;
+            W.F[lane] = g.F;
+            W.cbp[lane] = g.cb * g.ct + g.sb * g.st;     // cos(beta - theta_V1)
+            W.sbp[lane] = g.sb * g.ct - g.cb * g.st;     // sin(beta - theta_V1)
+            W.zeta[lane] = C.zeta;
+            W.zs[lane] = C.zeta * C.sigma;
+            W.scale[lane] = C.w * g.sgnC;
+        }
+        bool hasmom = false;
+        __syncwarp();
+        const int klo = max(1, llo - 1), khi = lhi + 1;
+        double Fm2[6] = {0, 0, 0, 0, 0, 0}, Fm1[6] = {0, 0, 0, 0, 0, 0}, Fk[6];
+        const double vp2 = A.velP * A.velP, vs2 = A.velS * A.velS, den = vp2 * vs2;
+        for (int k = klo; k <= khi; k++) {
+            const double t = k * A.dt;
+            LevelCtx L;
+            L.t2 = t * t;
+            L.RP = A.velP * t;
+            L.RS = A.velS * t;
+            L.k1 = 1.0 / vp2;
+            L.k5 = (vp2 + vs2) / den;
+            L.k6 = (vp2 - vs2) / den;
+            // decision phase (per child)
+            int type = T_NONE;
+            double rhoP = -1.0, rhoS = -1.0;
+            if (C.live) type = classify(C.zeta, L.RP, L.RS, C.dMIN, rhoP, rhoS);
+            AccE Ac = {0, 0, 0, 0, 0, 0, 0};
+            Piece pc[3];
+            int np = 0, full = 0;
+            if (type != T_NONE) child_decide(Ac, pc, np, full, C, L, rhoP, rhoS, type);
+            // whole-range moments, computed by the whole warp once per child
+            const bool need = full && !hasmom;
+            unsigned mm = __ballot_sync(0xffffffffu, need);
+            while (mm) {
+                const int b = __ffs(mm) - 1;
+                mm &= mm - 1;
+                const double Fb = __shfl_sync(0xffffffffu, C.g.F, b), cbb = __shfl_sync(0xffffffffu, C.g.cb, b);
+                const double sbb = __shfl_sync(0xffffffffu, C.g.sb, b), zb = __shfl_sync(0xffffffffu, C.zeta, b);
+                const double s1b = __shfl_sync(0xffffffffu, C.g.s1, b), s0b = __shfl_sync(0xffffffffu, C.g.s0, b);
+                double m[14];
+                moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx, glw);
+#pragma unroll
+                for (int e = 0; e < 14; e++) m[e] = warp_sum(m[e]);
+                if (lane == b) {
+#pragma unroll
+                    for (int e = 0; e < 14; e++) W.mom[e][lane] = m[e];
+                }
+            }
+            if (need) hasmom = true;
+            const double zs = C.zeta * C.sigma;
+            if (full & 1) apply_moments(Ac, W, lane, true, L, zs);
+            if (full & 2) apply_moments(Ac, W, lane, false, L, zs);
+            double S = 0.0, T[6] = {0, 0, 0, 0, 0, 0};
+            if (type != T_NONE) child_to_plane(S, T, Ac, C.g, C.w * C.g.sgnC);
+            // partial edge pieces -> per-warp list
+            int nsubs[3];
+            double hs[3];
+            int nn = 0;
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                if (u < np) {
+                    double len = pc[u].shi - pc[u].slo;
+                    int ns = (int)ceil(len * (1.0 / EBEM_EDGE_H));
+                    ns = max(1, min(ns, 4096));
+                    nsubs[u] = ns;
+                    hs[u] = len / ns;
+                    nn += 10 * ns;
+                }
+            }
+            int totp, totn;
+            const int pb = warp_excl_scan(np, lane, totp);
+            int o = warp_excl_scan(nn, lane, totn);
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                if (u < np) {
+                    W.slo[pb + u] = pc[u].slo;
+                    W.h[pb + u] = hs[u];
+                    W.off[pb + u] = o;
+                    W.who[pb + u] = lane | (pc[u].pterm ? 32 : 0);
+                    o += 10 * nsubs[u];
+                }
+            }
+            if (lane == 31) W.off[totp] = totn;
+            __syncwarp();
+            // all lanes: Gauss-Legendre nodes of the list, plane frame
+            int pp = 0;
+            for (int idx = lane; idx < totn; idx += 32) {
+                while (idx >= W.off[pp + 1]) pp++;
+                const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
+                const double h = W.h[pp];
+                const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
+                const int who = W.who[pp], cl = who & 31;
+                double ch, sech, th;
+                hyp(s, ch, sech, th);
+                const double cbq = W.cbp[cl], sbq = W.sbp[cl];
+                const double cq = th * cbq + sech * sbq, sq = sech * cbq - th * sbq;
+                Rad v = radial_edge(W.F[cl] * ch, W.zeta[cl]);
+                W4 w = weigh(v, (who & 32) != 0, L);
+                const double f = 0.5 * h * glw[q] * sech * W.scale[cl];
+                const double fin = f * w.in, fmx = -W.zs[cl] * f * w.mx;
+                S += f * w.sc;
+                T[0] += fin * cq * cq;
+                T[1] += fin * sq * cq;
+                T[2] += fin * sq * sq;
+                T[3] += fmx * cq;
+                T[4] += fmx * sq;
+                T[5] += f * w.zz;
+            }
+            __syncwarp();
+            S = warp_sum(S);
+#pragma unroll
+            for (int e = 0; e < 6; e++) T[e] = warp_sum(T[e]);
+            // F(t_k) = (S I + C^T M C) / 2 in global axes
+            {
+                double M[3][3] = {{T[0], T[1], T[3]}, {T[1], T[2], T[4]}, {T[3], T[4], T[5]}};
+                const double* Cm = F.C;
+                double MC[3][3];
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++) MC[r][c] = M[r][0] * Cm[c] + M[r][1] * Cm[3 + c] + M[r][2] * Cm[6 + c];
+                double R[3][3];
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+#pragma unroll
+                    for (int c = r; c < 3; c++) R[r][c] = Cm[r] * MC[0][c] + Cm[3 + r] * MC[1][c] + Cm[6 + r] * MC[2][c];
+                Fk[0] = 0.5 * (S + R[0][0]);
+                Fk[1] = 0.5 * R[0][1];
+                Fk[2] = 0.5 * R[0][2];
+                Fk[3] = 0.5 * (S + R[1][1]);
+                Fk[4] = 0.5 * R[1][2];
+                Fk[5] = 0.5 * (S + R[2][2]);
+            }
+            const int l = k - 1;
+            if (l >= llo && l <= lhi && lane < 9) {
+                const int e = map[lane];
+                double prev = (l - 1 >= 1) ? Fm2[e] : 0.0;
+                double v = ((Fk[e] + (-2.0) * Fm1[e]) + prev) / A.c4pirho;
+                store_entry(A, l - A.lag0, i, j, lane, (fabs(v) < 1.0e-14) ? 0.0 : v);
+            }
+#pragma unroll
+            for (int e = 0; e < 6; e++) { Fm2[e] = Fm1[e]; Fm1[e] = Fk[e]; }
+        }
+    }
+    if (A.count) {
+        if (lane == 0 && my_count) atomicAdd(&blk_count, my_count);
+        __syncthreads();
+        if (threadIdx.x == 0 && blk_count) atomicAdd(A.count, blk_count);
+    }
+}
+
 int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
                        cudaStream_t s, int diag_only) {
@@ -206,6 +435,17 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
     A.accumulate = accumulate;
     A.count = d_count;
     long long NN = diag_only ? (long long)nsrc : (long long)nsrc * m.nt;
+    if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 32) {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
+        long long want = (NN + EBEM_WARPS_PER_BLOCK - 1) / EBEM_WARPS_PER_BLOCK;
+        long long cap = (long long)sms * 16;
+        unsigned blocks = (unsigned)(want < cap ? want : cap);
+        if (blocks == 0) blocks = 1;
+        sa_assemble_warp_kernel<<<blocks, 32 * EBEM_WARPS_PER_BLOCK, 0, s>>>(A);
+        EBEM_CUDA_TRY(cudaGetLastError());
+        return EBEM_OK;
+    }
     int threads = 128;
     long long blocks = (NN + threads - 1) / threads;
     if (blocks > 0x7fffffffLL) return fail(EBEM_ERR_INVALID, "mesh too large for one launch");

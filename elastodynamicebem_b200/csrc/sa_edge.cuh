@@ -23,7 +23,7 @@
 //   closed-form angular integrals; pieces limited by the edge are integrated
 //   by Gauss-Legendre in s on sub-pieces of length <= EBEM_EDGE_H.  In s the
 //   integrands are analytic in the strip |Im s| < pi/2, so the rule converges
-//   geometrically (10 nodes on 0.6-long sub-pieces: ~1e-13 relative).
+//   geometrically (10 nodes on sub-pieces of length <= 1: ~1e-14 relative).
 // * Radial antiderivatives in r = sqrt(rho^2 + zeta^2):
 //     A1 = r, A3 = -1/r                       (1/r, 1/r^3 times rho d rho)
 //     B2 = r + zeta^2/r, C2 = ln(rho + r) - rho/r, D2 = -zeta^2/r
@@ -40,7 +40,7 @@
 #include "sa_device.cuh"
 
 #ifndef EBEM_EDGE_H
-#define EBEM_EDGE_H 0.6
+#define EBEM_EDGE_H 1.0
 #endif
 #ifndef EBEM_EDGE_NOINLINE
 #define EBEM_EDGE_NOINLINE 1

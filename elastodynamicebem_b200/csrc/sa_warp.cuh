@@ -1,0 +1,260 @@
+// Warp-cooperative semi-analytic assembly: one warp per (source, field) pair.
+//
+// The value computed is the one of sa_assemble_kernel (thread per pair, the
+// same closed-form child integrals of sa_edge.cuh); only the schedule differs:
+//
+// * Lane = child.  Lane 3 g + c owns child c of the projection of outer node g
+//   of the source triangle onto the field plane (3 n_gh <= 32 lanes).  Its
+//   geometry (ChildE, the node's zeta, sigma, distance to the triangle and
+//   weight) is level-independent and computed once per pair, not once per
+//   level.
+// * Per level a lane decides its pieces (BEMenerg_coreSA_calcIntgInt_childTriangle.m:
+//   front crossings with the reference's DeltaP/DeltaS <= 1e-6 thresholds)
+//   and evaluates the circle-bounded pieces in closed form.  An edge-bounded
+//   piece int_{slo}^{shi} w(theta) [V(F cosh s) - V_lo] sech(s) ds is split
+//   into int w V(F cosh s) sech ds (quadrature) minus V_lo int w dtheta over
+//   the same angular interval (closed form, the circle formula).
+// * Whole-range pieces (the piece spans the child's entire edge: the edge
+//   lies between the fronts, or inside the S front) use per-child moments
+//   int w V_f(F cosh s) sech ds of the eight radial functions, computed once
+//   per child by the whole warp the first time they are needed: no quadrature
+//   at later levels.
+// * The remaining (partial) edge pieces of all lanes are put in a per-warp
+//   list and their Gauss-Legendre nodes are evaluated by all 32 lanes, each
+//   node weighted by its child's node weight and orientation sign and taken
+//   in the plane frame, so every lane sums into the same pair value.
+// * The per-level pair value is a warp reduction; every lane forms F(t_k)
+//   and the sliding window, lanes 0..8 store the 3x3 block.
+//
+// Grid-stride over pairs (pair p = field j * nsrc + source i - src0, or the
+// diagonal pairs), one warp at a time per pair.
+#pragma once
+
+#include "sa_pair.cuh"
+
+namespace ebem {
+
+#define EBEM_WARP_PIECES 96   // <= 3 edge pieces per lane and level
+
+struct WarpShared {
+    double slo[EBEM_WARP_PIECES], h[EBEM_WARP_PIECES];
+    int off[EBEM_WARP_PIECES + 1];
+    int who[EBEM_WARP_PIECES];                  // child lane | (P terms ? 32 : 0)
+    double F[32], cbp[32], sbp[32], zeta[32], zs[32], scale[32];
+    double mom[14][32];                         // per-child moments (child frame)
+};
+
+struct Piece { double slo, shi; int pterm; };
+
+// Radial antiderivatives at the edge point R = F cosh s (one reciprocal for
+// both 1/r and 1/(r + R)).
+EBEM_DI Rad radial_edge(double R, double zeta) {
+    Rad v;
+    double z2 = zeta * zeta;
+    double r = sqrt(R * R + z2);
+    double q = 1.0 / (r * (r + R));
+    double ir = (r + R) * q, ir3 = ir * ir * ir;
+    v.A1 = r;
+    v.A3 = -ir;
+    v.B2 = r + z2 * ir;
+    v.D2 = -z2 * ir;
+    v.B4 = -ir + z2 * ir3 * (1.0 / 3.0);
+    v.D4 = -z2 * ir3 * (1.0 / 3.0);
+    if (zeta > 0) {
+        v.C2 = m_log(R + r) - R * ir;
+        v.C4 = -(r * r + r * R + R * R) * ir3 * (r * q) * (1.0 / 3.0);
+    } else {
+        v.C2 = 0.0;
+        v.C4 = 0.0;
+    }
+    return v;
+}
+
+// cosh(s), sech(s), tanh(s) from one exponential.
+EBEM_DI void hyp(double s, double& ch, double& sech, double& th) {
+    double e = m_exp(s), ie = 1.0 / e;
+    ch = 0.5 * (e + ie);
+    sech = 1.0 / ch;
+    th = 0.5 * (e - ie) * sech;
+}
+
+// Moments of one child (child frame), this lane's share of the nodes
+// n = lane, lane + 32, ... of the whole-range rule.
+EBEM_DI void moment_share(double m[14], double F, double cb, double sb, double zeta, double s1, double s0, int lane,
+                          const double* glx, const double* glw) {
+#pragma unroll
+    for (int e = 0; e < 14; e++) m[e] = 0.0;
+    double len = s0 - s1;
+    if (!(len > 0)) return;
+    int nsub = (int)ceil(len * (1.0 / EBEM_EDGE_H));
+    nsub = max(1, min(nsub, 4096));
+    double h = len / nsub;
+    for (int idx = lane; idx < nsub * 10; idx += 32) {
+        int sub = idx / 10, q = idx - 10 * sub;
+        double s = s1 + (sub + 0.5) * h + 0.5 * h * glx[q];
+        double ch, sech, th;
+        hyp(s, ch, sech, th);
+        double c = th * cb + sech * sb, sn = sech * cb - th * sb;
+        Rad v = radial_edge(F * ch, zeta);
+        double f = 0.5 * h * glw[q] * sech;
+        double cc = c * c, sc = sn * c, ss = sn * sn;
+        m[0] += f * v.A1;
+        m[1] += f * v.A3;
+        m[2] += f * v.B2 * cc; m[3] += f * v.B2 * sc; m[4] += f * v.B2 * ss;
+        m[5] += f * v.B4 * cc; m[6] += f * v.B4 * sc; m[7] += f * v.B4 * ss;
+        m[8] += f * v.C2 * c;  m[9] += f * v.C2 * sn;
+        m[10] += f * v.C4 * c; m[11] += f * v.C4 * sn;
+        m[12] += f * v.D2;     m[13] += f * v.D4;
+    }
+}
+
+// Whole-range piece from the moments with the level's weights (child frame).
+EBEM_DI void apply_moments(AccE& A, const WarpShared& W, int lane, bool pterm, const LevelCtx& L, double zs) {
+    double m[14];
+#pragma unroll
+    for (int e = 0; e < 14; e++) m[e] = W.mom[e][lane];
+    double sc, i0, i1, i2, x0, x1, zz;
+    if (pterm) {
+        sc = L.k1 * m[0] - L.t2 * m[1];
+        i0 = -L.k1 * m[2] + 3 * L.t2 * m[5];
+        i1 = -L.k1 * m[3] + 3 * L.t2 * m[6];
+        i2 = -L.k1 * m[4] + 3 * L.t2 * m[7];
+        x0 = -L.k1 * m[8] + 3 * L.t2 * m[10];
+        x1 = -L.k1 * m[9] + 3 * L.t2 * m[11];
+        zz = -L.k1 * m[12] + 3 * L.t2 * m[13];
+    } else {
+        sc = L.k5 * m[0];
+        i0 = L.k6 * m[2];
+        i1 = L.k6 * m[3];
+        i2 = L.k6 * m[4];
+        x0 = L.k6 * m[8];
+        x1 = L.k6 * m[9];
+        zz = L.k6 * m[12];
+    }
+    A.S += sc;
+    A.t11 += i0; A.t12 += i1; A.t22 += i2;
+    A.t13 += -zs * x0; A.t23 += -zs * x1;
+    A.t33 += zz;
+}
+
+EBEM_DI W4 neg(W4 w) { w.sc = -w.sc; w.in = -w.in; w.mx = -w.mx; w.zz = -w.zz; return w; }
+
+// Per-lane child state, level-independent.
+struct LaneChild {
+    ChildE g;
+    double cg, sg;          // cos/sin of gamma
+    double zeta, sigma, dMIN, w;
+    bool live;
+};
+
+// Decision phase of one child at one level: closed-form circle pieces and
+// lo-subtractions into A (child frame), whole-range pieces from the moments
+// (or flagged in need_mom when they are not computed yet), partial edge
+// pieces returned in pc[0..np).  Mirrors child_level_e piece by piece.
+EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const LaneChild& C, const LevelCtx& L,
+                          double rhoP, double rhoS, int type) {
+    const ChildE& g = C.g;
+    const bool isP = (type == T_P), spsp = (type == T_SP_SP);
+    const double zeta = C.zeta, zs = C.zeta * C.sigma;
+    np = 0;
+    full_mask = 0;                          // bit 0: full P piece, bit 1: full S piece
+    double DeltaP = g.bm * g.bm - (g.a * g.a - rhoP * rhoP);
+    double DeltaS = isP ? 0.0 : g.bm * g.bm - (g.a * g.a - rhoS * rhoS);
+    const bool xP = DeltaP > 1.0e-6, xS = xP && DeltaS > 1.0e-6;
+    double rhoSe = isP ? 0.0 : rhoS;
+    Rad VSe = radial_at(rhoSe, isP ? zeta : L.RS, zeta);
+    Rad VP = radial_at(rhoP, L.RP, zeta);
+    W4 wPc = weigh(rad_sub(VP, VSe), true, L);
+    W4 wPlo = neg(weigh(VSe, true, L));
+    const double smax = g.s0, smin = g.s1;
+    const double th0 = 0.0, c0 = 1.0, sn0 = 0.0;
+    const double thg = g.gamma, cg = C.cg, sgm = C.sg;
+    // S crossing data (used by the P pieces when the S front crosses, and by the S terms)
+    double sS = 0.0, thAS = 0.0, cAS = 1.0, sAS = 0.0, thBS = 0.0, cBS = 1.0, sBS = 0.0;
+    if (xS && !isP) {
+        sS = m_log((rhoS + sqrt_c((rhoS - g.F) * (rhoS + g.F))) / g.F);
+        clipped_theta(g, rhoS, sS, true, smin, thg, cg, sgm, thAS, cAS, sAS);
+        clipped_theta(g, rhoS, -sS, false, smin, thg, cg, sgm, thBS, cBS, sBS);
+    }
+    if (!xP) {
+        add_circle(A, wPc, th0, c0, sn0, thg, cg, sgm, zs);
+    } else {
+        double sP = m_log((rhoP + sqrt_c((rhoP - g.F) * (rhoP + g.F))) / g.F);
+        double thA, cA, sA, thB, cB, sB;
+        clipped_theta(g, rhoP, sP, true, smin, thg, cg, sgm, thA, cA, sA);
+        clipped_theta(g, rhoP, -sP, false, smin, thg, cg, sgm, thB, cB, sB);
+        if (smax > sP) add_circle(A, wPc, th0, c0, sn0, thA, cA, sA, zs);
+        if (-sP > smin) add_circle(A, wPc, thB, cB, sB, thg, cg, sgm, zs);
+        if (xS && !isP) {
+            // [sS, sP] <-> theta in [thA, thAS];  [-sP, -sS] <-> [thBS, thB]
+            double lo1 = fmax(sS, smin), hi1 = fmin(sP, smax);
+            if (hi1 - lo1 > 0) {
+                add_circle(A, wPlo, thA, cA, sA, thAS, cAS, sAS, zs);
+                pc[np++] = {lo1, hi1, 1};
+            }
+            double lo2 = fmax(-sP, smin), hi2 = fmin(-sS, smax);
+            if (hi2 - lo2 > 0) {
+                add_circle(A, wPlo, thBS, cBS, sBS, thB, cB, sB, zs);
+                pc[np++] = {lo2, hi2, 1};
+            }
+        } else {
+            double lo = fmax(-sP, smin), hi = fmin(sP, smax);
+            if (hi - lo > 0) {
+                add_circle(A, wPlo, thA, cA, sA, thB, cB, sB, zs);
+                if (-sP <= smin && sP >= smax) full_mask |= 1;
+                else pc[np++] = {lo, hi, 1};
+            }
+        }
+    }
+    if (spsp) {
+        Rad V0 = radial_at(0.0, zeta, zeta);
+        if (!(zeta > 0)) { V0.A1 = 0.0; V0.B2 = 0.0; V0.D2 = 0.0; }
+        Rad VS = radial_at(rhoS, L.RS, zeta);
+        W4 wSc = weigh(rad_sub(VS, V0), false, L);
+        if (!xS) {
+            add_circle(A, wSc, th0, c0, sn0, thg, cg, sgm, zs);
+        } else {
+            if (smax > sS) add_circle(A, wSc, th0, c0, sn0, thAS, cAS, sAS, zs);
+            if (-sS > smin) add_circle(A, wSc, thBS, cBS, sBS, thg, cg, sgm, zs);
+            double lo = fmax(-sS, smin), hi = fmin(sS, smax);
+            if (hi - lo > 0) {
+                add_circle(A, neg(weigh(V0, false, L)), thAS, cAS, sAS, thBS, cBS, sBS, zs);
+                if (-sS <= smin && sS >= smax) full_mask |= 2;
+                else pc[np++] = {lo, hi, 0};
+            }
+        }
+    }
+}
+
+// Child frame -> plane frame (rotation by the direction of V1), times the
+// node weight and the orientation sign, added to (S, T[6]).
+EBEM_DI void child_to_plane(double& S, double T[6], const AccE& A, const ChildE& g, double wsc) {
+    const double c = g.ct, s = g.st;
+    const double cc = c * c, ss = s * s, cs = c * s;
+    S += wsc * A.S;
+    T[0] += wsc * (cc * A.t11 - 2 * cs * A.t12 + ss * A.t22);
+    T[1] += wsc * (cs * A.t11 + (cc - ss) * A.t12 - cs * A.t22);
+    T[2] += wsc * (ss * A.t11 + 2 * cs * A.t12 + cc * A.t22);
+    T[3] += wsc * (c * A.t13 - s * A.t23);
+    T[4] += wsc * (s * A.t13 + c * A.t23);
+    T[5] += wsc * A.t33;
+}
+
+EBEM_DI double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+EBEM_DI int warp_excl_scan(int v, int lane, int& total) {
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    total = __shfl_sync(0xffffffffu, x, 31);
+    return x - v;
+}
+
+}  // namespace ebem
