@@ -196,3 +196,105 @@ def assemble_ghc(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, n_sub: int, n
                                              int(nlag), _ptr(out), int(bool(sa_diagonal)),
                                              _stream_ptr(stream) if out.is_cuda else None))
     return out.view(nlag, n3, n3).transpose(1, 2)
+
+
+# ---------------------------------------------------------------------------
+# direct formulation
+
+FIX_REFERENCE_DEFECTS = 1
+
+
+def num_blocks_dir(dmesh: DeviceMesh, prm: ProblemParams):
+    """(L_V, L_K) of the direct formulation."""
+    lv, lk = C.c_int(), C.c_int()
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_num_blocks_dir(dmesh.handle, C.byref(p), C.byref(lv), C.byref(lk)))
+    return int(lv.value), int(lk.value)
+
+
+def assemble_k(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, n_sub: int, n_sing: int, n_diag: int,
+               lag0: int = 0, nlag: int | None = None, fix: bool = False, out: torch.Tensor | None = None, stream=None):
+    """Double-layer blocks K[l][row, col], shape (nlag, 3N, 3Nv) (a transposed
+    view of the column-major storage of the C ABI)."""
+    if nlag is None:
+        nlag = num_blocks_dir(dmesh, prm)[1] - lag0
+    N, Nv = dmesh.N, dmesh.mesh.number_nodes
+    if out is None:
+        out = torch.empty((nlag, 3 * Nv, 3 * N), dtype=torch.float64, device="cuda")
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_assemble_k(dmesh.handle, C.byref(p), int(n_gh), int(n_sub), int(n_sing), int(n_diag),
+                                           int(lag0), int(nlag), FIX_REFERENCE_DEFECTS if fix else 0, _ptr(out), 0,
+                                           _stream_ptr(stream) if out.is_cuda else None))
+    return out.transpose(1, 2)
+
+
+def assemble_v(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, n_sub: int, n_sing: int, n_diag: int,
+               lag0: int = 0, nlag: int | None = None, out: torch.Tensor | None = None, stream=None):
+    """Single-layer blocks of the direct formulation V[l][row, col], (nlag, 3N, 3N)."""
+    if nlag is None:
+        nlag = num_blocks_dir(dmesh, prm)[0] - lag0
+    n3 = 3 * dmesh.N
+    if out is None:
+        out = torch.empty((nlag, n3, n3), dtype=torch.float64, device="cuda")
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_assemble_v(dmesh.handle, C.byref(p), int(n_gh), int(n_sub), int(n_sing), int(n_diag),
+                                           int(lag0), int(nlag), _ptr(out),
+                                           _stream_ptr(stream) if out.is_cuda else None))
+    return out.transpose(1, 2)
+
+
+def _raw(blocks: torch.Tensor) -> torch.Tensor:
+    """Column-major per-lag storage of blocks given as [l][row, col]."""
+    return blocks.transpose(1, 2).contiguous()
+
+
+def march_dn(dmesh: DeviceMesh, prm: ProblemParams, V: torch.Tensor, K: torch.Tensor, gV: torch.Tensor, stream=None):
+    """DN time marching: displacement u (nT, 3Nv) from V (LV, 3N, 3N), K (LK, 3N, 3Nv)
+    and the Neumann datum gV (nT, 3N)."""
+    Vr, Kr = _raw(V), _raw(K)
+    u = torch.empty((prm.nT, 3 * dmesh.mesh.number_nodes), dtype=torch.float64, device=Vr.device)
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_march_dn(dmesh.handle, C.byref(p), _ptr(Vr), int(Vr.shape[0]), _ptr(Kr),
+                                         int(Kr.shape[0]), _ptr(gV.contiguous()), _ptr(u), _stream_ptr(stream)))
+    return u
+
+
+def march_dd(dmesh: DeviceMesh, prm: ProblemParams, V: torch.Tensor, K: torch.Tensor, rhs_: torch.Tensor,
+             gK: torch.Tensor, stream=None):
+    """DD time marching: traction phi (nT, 3N) from V, K, the right-hand side
+    (nT, 3N) and the Dirichlet datum gK (nT, 3Nv)."""
+    Vr, Kr = _raw(V), _raw(K)
+    phi = torch.empty((prm.nT, 3 * dmesh.N), dtype=torch.float64, device=Vr.device)
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_march_dd(dmesh.handle, C.byref(p), _ptr(Vr), int(Vr.shape[0]), _ptr(Kr),
+                                         int(Kr.shape[0]), _ptr(rhs_.contiguous()), _ptr(gK.contiguous()), _ptr(phi),
+                                         _stream_ptr(stream)))
+    return phi
+
+
+def pp_dir(dmesh: DeviceMesh, prm: ProblemParams, n_sub: int, n_sing: int, a: torch.Tensor, b: torch.Tensor, points,
+           times, fix: bool = False, stream=None):
+    """Direct post-processing u (ntimes, npts, 3) = sum_n G_n a_n - P_n b_n with
+    a (nT, 3N) and b (nT, 3Nv)."""
+    pts = torch.as_tensor(np.ascontiguousarray(points, np.float64)).to(a.device)
+    tms = np.ascontiguousarray(times, np.float64)
+    u = torch.empty((len(tms), pts.shape[0], 3), dtype=torch.float64, device=a.device)
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_pp_dir(dmesh.handle, C.byref(p), int(n_sub), int(n_sing),
+                                       FIX_REFERENCE_DEFECTS if fix else 0, _ptr(a.contiguous()), _ptr(b.contiguous()),
+                                       _ptr(pts), int(pts.shape[0]), tms.ctypes.data, len(tms), _ptr(u),
+                                       _stream_ptr(stream)))
+    return u
+
+
+def pp_dir_matrices(dmesh: DeviceMesh, prm: ProblemParams, n_sub: int, n_sing: int, x, t: float, fix: bool = False):
+    """The reference's per-(x, t) matrices G (3 nHat, 3N) and P (3 nHat, 3Nv), on the host."""
+    N, Nv = dmesh.N, dmesh.mesh.number_nodes
+    nhat = int(np.ceil(t / prm.dt)) if t > 0 else 0
+    G = np.zeros(9 * nhat * N); P = np.zeros(9 * nhat * Nv)
+    xs = np.ascontiguousarray(x, np.float64)
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_pp_dir_matrices(dmesh.handle, C.byref(p), int(n_sub), int(n_sing),
+                                                FIX_REFERENCE_DEFECTS if fix else 0, xs.ctypes.data, float(t),
+                                                G.ctypes.data, P.ctypes.data))
+    return G.reshape(3 * N, 3 * nhat).T, P.reshape(3 * Nv, 3 * nhat).T

@@ -31,6 +31,8 @@ PhysParams phys_from(const ebem_problem* p) {
     P.velS = std::sqrt(p->mu / p->rho);
     P.dt = p->tfin / p->nt;
     P.nT = p->nt;
+    P.lam = p->lambda;
+    P.mu = p->mu;
     return P;
 }
 
@@ -201,6 +203,7 @@ int ebem_mesh_destroy(ebem_mesh* m) {
     if (m->d.d_tris) cudaFree(m->d.d_tris);
     if (m->d.d_geo) cudaFree(m->d.d_geo);
     if (m->d.d_nodes) cudaFree(m->d.d_nodes);
+    free_direct(m->d);
     delete m;
     return EBEM_OK;
 }
@@ -426,6 +429,165 @@ int ebem_pp_sa(const ebem_mesh* m, const ebem_problem* p, const double* phi, con
 int ebem_assemble_sa_panel(const ebem_mesh* m, const ebem_problem* p, int n_gh, int lag0, int nlag, int src0,
                            int nsrc, double* E, long long ld, int accumulate, void* stream, long long* nonnull) {
     return assemble_impl(m, p, n_gh, lag0, nlag, src0, nsrc, E, ld, accumulate, stream, nonnull);
+}
+
+// ---------------------------------------------------------------------------
+// direct formulation
+
+static int check_rules(int n_gh, int n_sub, int n_sing, int n_diag) {
+    if (n_gh != 3 && n_gh != 7 && n_gh != 12 && n_gh != 19) return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+    if ((n_sub != 1 && n_sub != 4 && n_sub != 16 && n_sub != 64) ||
+        (n_sing != 1 && n_sing != 3 && n_sing != 7 && n_sing != 12 && n_sing != 19))
+        return fail(EBEM_ERR_INVALID, "inner rule: n_sub in {1,4,16,64}, n_sing in {1,3,7,12,19}");
+    if (n_diag != 0 && n_diag != 16 && n_diag != 64 && n_diag != 256 && n_diag != 1024)
+        return fail(EBEM_ERR_INVALID, "DIAG rule: n_diag in {16,64,256,1024} (0: none)");
+    return EBEM_OK;
+}
+
+int ebem_num_blocks_dir(const ebem_mesh* m, const ebem_problem* p, int* lv, int* lk) {
+    int L = 0;
+    if (int rc = ebem_num_blocks(m, p, &L)) return rc;
+    if (lv) *lv = L;
+    if (lk) *lk = std::min(L + 1, p->nt);
+    return EBEM_OK;
+}
+
+int ebem_assemble_k(const ebem_mesh* m, const ebem_problem* p, int n_gh, int n_sub, int n_sing, int n_diag, int lag0,
+                    int nlag, int flags, double* K, int accumulate, void* stream) {
+    if (!m || !K) return fail(EBEM_ERR_INVALID, "NULL mesh or output");
+    if (int rc = check_problem(p)) return rc;
+    if (int rc = check_rules(n_gh, n_sub, n_sing, n_diag)) return rc;
+    if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
+    int LK = 0;
+    if (int rc = ebem_num_blocks_dir(m, p, nullptr, &LK)) return rc;
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MeshData& md = const_cast<MeshData&>(m->d);
+    if (int rc = prep_direct(md, s)) return rc;
+    PhysParams P = phys_from(p);
+    const size_t n = 9 * (size_t)md.nt * md.nv * nlag;
+    DevOut out;
+    if (int rc = out.init(K, n)) return rc;
+    if (accumulate) {
+        if (out.host) EBEM_CUDA_TRY(cudaMemcpyAsync(out.d, K, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    } else {
+        EBEM_CUDA_TRY(cudaMemsetAsync(out.d, 0, n * sizeof(double), s));
+    }
+    if (int rc = launch_k_assemble(md, P, n_gh, n_sub, n_sing, n_diag, lag0, nlag, LK, flags & EBEM_FIX_REFERENCE_DEFECTS,
+                                   out.d, s))
+        return rc;
+    return out.finish(s);
+}
+
+int ebem_assemble_v(const ebem_mesh* m, const ebem_problem* p, int n_gh, int n_sub, int n_sing, int n_diag, int lag0,
+                    int nlag, double* V, void* stream) {
+    if (!m || !V) return fail(EBEM_ERR_INVALID, "NULL mesh or output");
+    if (int rc = check_problem(p)) return rc;
+    if (int rc = check_rules(n_gh, n_sub, n_sing, n_diag)) return rc;
+    if (n_diag == 0) return fail(EBEM_ERR_INVALID, "the direct V operator needs a DIAG rule for its diagonal blocks");
+    if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MeshData& md = const_cast<MeshData&>(m->d);
+    if (int rc = prep_direct(md, s)) return rc;
+    PhysParams P = phys_from(p);
+    const size_t n3 = 3 * (size_t)md.nt;
+    DevOut out;
+    if (int rc = out.init(V, n3 * n3 * nlag)) return rc;
+    EBEM_CUDA_TRY(cudaMemsetAsync(out.d, 0, n3 * n3 * nlag * sizeof(double), s));
+    if (int rc = launch_ghc_assemble(md, P, n_gh, n_sub, n_sing, lag0, nlag, out.d, n3, n3 * n3, s)) return rc;
+    if (int rc = launch_v_diag(md, P, n_gh, n_diag, lag0, nlag, out.d, s)) return rc;
+    return out.finish(s);
+}
+
+int ebem_march_dn(const ebem_mesh* m, const ebem_problem* p, const double* V, int LV, const double* K, int LK,
+                  const double* gV, double* u, void* stream) {
+    if (!m || !V || !K || !gV || !u || LV < 1 || LK < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
+    if (int rc = check_problem(p)) return rc;
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MeshData& md = const_cast<MeshData&>(m->d);
+    if (int rc = prep_direct(md, s)) return rc;
+    const size_t R = 3 * (size_t)md.nt, Cn = 3 * (size_t)md.nv;
+    DevIn dV, dK, dgv;
+    if (int rc = dV.init(V, R * R * LV, s)) return rc;
+    if (int rc = dK.init(K, R * Cn * LK, s)) return rc;
+    if (int rc = dgv.init(gV, R * p->nt, s)) return rc;
+    DevOut out;
+    if (int rc = out.init(u, Cn * p->nt)) return rc;
+    if (int rc = march_dn_device(md, dV.d, LV, dK.d, LK, dgv.d, p->nt, out.d, s)) return rc;
+    return out.finish(s);
+}
+
+int ebem_march_dd(const ebem_mesh* m, const ebem_problem* p, const double* V, int LV, const double* K, int LK,
+                  const double* rhs, const double* gK, double* phi, void* stream) {
+    if (!m || !V || !K || !rhs || !gK || !phi || LV < 1 || LK < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
+    if (int rc = check_problem(p)) return rc;
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MeshData& md = const_cast<MeshData&>(m->d);
+    if (int rc = prep_direct(md, s)) return rc;
+    const size_t R = 3 * (size_t)md.nt, Cn = 3 * (size_t)md.nv;
+    DevIn dV, dK, dr, dgk;
+    if (int rc = dV.init(V, R * R * LV, s)) return rc;
+    if (int rc = dK.init(K, R * Cn * LK, s)) return rc;
+    if (int rc = dr.init(rhs, R * p->nt, s)) return rc;
+    if (int rc = dgk.init(gK, Cn * p->nt, s)) return rc;
+    DevOut out;
+    if (int rc = out.init(phi, R * p->nt)) return rc;
+    if (int rc = march_dd_device(md, dV.d, LV, dK.d, LK, dr.d, dgk.d, p->nt, out.d, s)) return rc;
+    return out.finish(s);
+}
+
+int ebem_pp_dir(const ebem_mesh* m, const ebem_problem* p, int n_sub, int n_sing, int flags, const double* a,
+                const double* b, const double* pts, int npts, const double* times, int ntimes, double* u, void* stream) {
+    if (!m || !a || !b || !pts || !times || !u || npts < 1 || ntimes < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
+    if (int rc = check_problem(p)) return rc;
+    if (int rc = check_rules(3, n_sub, n_sing, 0)) return rc;
+    if (is_device_ptr(times)) return fail(EBEM_ERR_INVALID, "times must be a host array");
+    for (int q = 0; q < ntimes; q++)
+        if (!(times[q] <= p->tfin * (1 + 1e-12))) return fail(EBEM_ERR_INVALID, "evaluation time beyond tfin");
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MeshData& md = const_cast<MeshData&>(m->d);
+    if (int rc = prep_direct(md, s)) return rc;
+    PhysParams P = phys_from(p);
+    DevIn da, db, dp;
+    if (int rc = da.init(a, 3 * (size_t)md.nt * P.nT, s)) return rc;
+    if (int rc = db.init(b, 3 * (size_t)md.nv * P.nT, s)) return rc;
+    if (int rc = dp.init(pts, 3 * (size_t)npts, s)) return rc;
+    DevOut out;
+    if (int rc = out.init(u, 3 * (size_t)npts * ntimes)) return rc;
+    if (int rc = launch_pp_dir(md, P, n_sub, n_sing, flags & EBEM_FIX_REFERENCE_DEFECTS, dp.d, npts, times, ntimes, da.d,
+                               db.d, out.d, nullptr, nullptr, 0, s))
+        return rc;
+    return out.finish(s);
+}
+
+int ebem_pp_dir_matrices(const ebem_mesh* m, const ebem_problem* p, int n_sub, int n_sing, int flags, const double* x,
+                         double t, double* G, double* Pm) {
+    if (!m || !x || !G || !Pm) return fail(EBEM_ERR_INVALID, "bad arguments");
+    if (int rc = check_problem(p)) return rc;
+    if (int rc = check_rules(3, n_sub, n_sing, 0)) return rc;
+    if (!(t > 0)) return EBEM_OK;
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = 0;
+    MeshData& md = const_cast<MeshData&>(m->d);
+    if (int rc = prep_direct(md, s)) return rc;
+    PhysParams P = phys_from(p);
+    const int nhat = (int)std::ceil(t / P.dt);
+    DevIn dx;
+    if (int rc = dx.init(x, 3, s)) return rc;
+    DevOut oG, oP;
+    if (int rc = oG.init(G, 9 * (size_t)nhat * md.nt)) return rc;
+    if (int rc = oP.init(Pm, 9 * (size_t)nhat * md.nv)) return rc;
+    EBEM_CUDA_TRY(cudaMemsetAsync(oG.d, 0, 9 * (size_t)nhat * md.nt * sizeof(double), s));
+    EBEM_CUDA_TRY(cudaMemsetAsync(oP.d, 0, 9 * (size_t)nhat * md.nv * sizeof(double), s));
+    if (int rc = launch_pp_dir(md, P, n_sub, n_sing, flags & EBEM_FIX_REFERENCE_DEFECTS, dx.d, 1, &t, 1, nullptr,
+                               nullptr, nullptr, oG.d, oP.d, 1, s))
+        return rc;
+    if (int rc = oG.finish(s)) return rc;
+    return oP.finish(s);
 }
 
 }  // extern "C"

@@ -34,6 +34,12 @@ struct MeshData {
     // mapped outer nodes cached per rule: (x, y, z, weight) per (triangle, node)
     int nodes_rule = 0;
     NodeW* d_nodes = nullptr;     // nt x nodes_rule
+    // direct formulation (built on first use): per-triangle P1 data and the
+    // vertex -> triangles adjacency (CSR)
+    struct DirTri* d_dir = nullptr;
+    int32_t* d_vt_off = nullptr;  // nv + 1
+    int32_t* d_vt_tri = nullptr;  // 3 nt
+    double max_len = 0.0;         // largest triangle edge
 };
 
 // Gauss-Hammer base rules (barycentric nodes, weights summing to 1/2).
@@ -48,6 +54,7 @@ int map_nodes(MeshData& m, int n_gh, cudaStream_t s);
 struct PhysParams {
     double rho, velP, velS, dt;
     int nT;
+    double lam = 0.0, mu = 0.0;
 };
 PhysParams phys_from(const ebem_problem* p);
 
@@ -63,5 +70,43 @@ int launch_rhs(const MeshData& m, const PhysParams& P, int n_gh, int datum, doub
 int march_device(const double* dE, int n3, int L, const double* drhs, int nT, double* dphi, cudaStream_t s);
 int launch_pp_sa(const MeshData& m, const PhysParams& P, const double* d_phi, const double* d_pts, int npts,
                  const double* h_times, int ntimes, double* d_u, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// direct formulation (direct.cu)
+
+// Per-triangle data of the direct formulation: vertices, unit normal and area
+// (readSpaceMesh.m:114-121), P1 basis phi_k(y) = v[k] + M[3k..3k+2] . y, longest edge.
+struct DirTri {
+    double V[3][3];
+    double n[3];
+    double area;
+    double M[9];
+    double v[3];
+    double maxL;
+};
+
+int prep_direct(MeshData& m, cudaStream_t s);
+void free_direct(MeshData& m);
+// K_l (3N x 3Nv per lag, column-major, ld = 3N): off-singular part with the
+// outer GH rule n_gh and composite inner rule (n_sub, n_sing), then, when
+// n_diag > 0, the same-triangle parts on the DIAG rule.  Accumulates (+=).
+int launch_k_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_sub, int n_sing, int n_diag, int lag0,
+                      int nlag, int nblocks, int fix, double* d_K, cudaStream_t s);
+// Diagonal blocks of V_l on the DIAG rule, written into a 3N x 3N per lag buffer.
+int launch_v_diag(const MeshData& m, const PhysParams& P, int n_gh, int n_diag, int lag0, int nlag, double* d_V,
+                  cudaStream_t s);
+// Direct post-processing.  mode 0: u(t_q, x_p) = sum_n G_n a_n - P_n b_n into
+// d_u (ntimes x npts x 3); mode 1: the matrices G (3 nHat x 3N) and P
+// (3 nHat x 3Nv) of one (x, t) into d_G, d_P.
+int launch_pp_dir(const MeshData& m, const PhysParams& P, int n_sub, int n_sing, int fix, const double* d_pts, int npts,
+                  const double* h_times, int ntimes, const double* d_a, const double* d_b, double* d_u, double* d_G,
+                  double* d_P, int mode, cudaStream_t s);
+// Direct time marching.  DN: least squares (K_0 + I) u_n = beta_V,n + I u_{n-1}
+// - sum K_l u_{n-l}; DD: V_0 phi_n = rhs_n / 2 + beta_K,n - sum V_l phi_{n-l}.
+int march_dn_device(const MeshData& m, const double* dV, int LV, const double* dK, int LK, const double* d_gV, int nT,
+                    double* d_u, cudaStream_t s);
+int march_dd_device(const MeshData& m, const double* dV, int LV, const double* dK, int LK, const double* d_rhs,
+                    const double* d_gK, int nT, double* d_phi, cudaStream_t s);
+int launch_hist_gemv(const double* A, int n3, long long K, const double* x, double* y, int sm_count, cudaStream_t s);
 
 }  // namespace ebem

@@ -198,7 +198,10 @@ __device__ __forceinline__ void store_entry(const SAArgs& A, int q, int i, int j
 
 // One warp per pair (schedule described in sa_warp.cuh); requires 3 n_gh <= 32.
 #define EBEM_WARPS_PER_BLOCK 4
-__global__ void __launch_bounds__(32 * EBEM_WARPS_PER_BLOCK) sa_assemble_warp_kernel(SAArgs A) {
+#ifndef EBEM_WARP_MINB
+#define EBEM_WARP_MINB 4   // 128 registers: 4 blocks (16 warps) per SM
+#endif
+__global__ void __launch_bounds__(32 * EBEM_WARPS_PER_BLOCK, EBEM_WARP_MINB) sa_assemble_warp_kernel(SAArgs A) {
     __shared__ WarpShared Wsh[EBEM_WARPS_PER_BLOCK];
     __shared__ double glx[10], glw[10];
     __shared__ unsigned long long blk_count;

@@ -86,3 +86,60 @@ def sphere_workload(n_gh: int = 7, subdivisions: int = 3) -> Workload:
     pts = d * rng.uniform(1.5, 3.0, 256)[:, None]
     times = prm.dt * np.arange(1, 41)
     return Workload(f"sphere_n{m.numberTriangles}", m, prm, n_gh, DATUM_RADIAL_SIN, pts, times)
+
+
+# ---------------------------------------------------------------------------
+# direct formulation: the 1-D bar data of the reference and the bar workload
+
+def _bar_terms(prm: ProblemParams, h: float):
+    khat = int(np.ceil(prm.velP * prm.Tfin / (2 * h))) - 1
+    return np.arange(0, khat + 1)
+
+
+def bar_neumann(mesh: _mesh.Mesh, prm: ProblemParams, h: float) -> np.ndarray:
+    """Neumann datum gV (nT, 3N) of the bar of height h at the triangle
+    centres, t_n = n dt, n = 1..nT (BEMenerg_dir_calcBoundDataNeumann.m:6-24):
+    g = (0, 0, 2 mu P(x, t) n_3), P = sum_k (-1)^k [H(c_P t - 2hk - (h - x_3))
+    + H(c_P t - 2h(k+1) + (h - x_3))]."""
+    k = _bar_terms(prm, h)
+    sgn = (-1.0) ** k
+    x3 = mesh.center[:, 2]
+    out = np.zeros((prm.nT, 3 * mesh.numberTriangles))
+    for n in range(1, prm.nT + 1):
+        ct = prm.velP * (n * prm.dt)
+        a = ((ct - 2 * h * k[None, :] - (h - x3[:, None])) > 0).astype(float)
+        b = ((ct - 2 * h * (k[None, :] + 1) + (h - x3[:, None])) > 0).astype(float)
+        P = (sgn[None, :] * (a + b)).sum(1)
+        out[n - 1, 2::3] = 2 * prm.mu * P * mesh.normal[:, 2]
+    return out
+
+
+def bar_dirichlet(mesh: _mesh.Mesh, prm: ProblemParams, h: float) -> np.ndarray:
+    """Dirichlet datum gK (nT, 3Nv) of the bar at the vertices
+    (BEMenerg_dir_calcBoundDataDirichlet.m:6-16): g = (0, 0, u(x, t)),
+    u = sum_k (-1)^k [(c_P t - 2hk - (h - x_3))_+ - (c_P t - 2h(k+1) + (h - x_3))_+]."""
+    k = _bar_terms(prm, h)
+    sgn = (-1.0) ** k
+    x3 = mesh.coordinates[:, 2]
+    out = np.zeros((prm.nT, 3 * mesh.number_nodes))
+    for n in range(1, prm.nT + 1):
+        ct = prm.velP * (n * prm.dt)
+        a = ct - 2 * h * k[None, :] - (h - x3[:, None])
+        b = ct - 2 * h * (k[None, :] + 1) + (h - x3[:, None])
+        u = (sgn[None, :] * (a * (a > 0) - b * (b > 0))).sum(1)
+        out[n - 1, 2::3] = u
+    return out
+
+
+def bar_workload(h: float = 0.1) -> Workload:
+    """Prism [0,1] x [0,1] x [0,3] triangulated with squares of side h (h=0.1:
+    2800 triangles, 1402 vertices), rho=1, mu=1, lambda=2, dt=0.02, T=2 (100
+    steps); Neumann datum of the bar of height 3 (DN formulation);
+    displacement at 512 interior points (uniform in the open prism, seed 3) at
+    t_n = n dt."""
+    m = _mesh.prism_bar(1.0, 1.0, 3.0, h)
+    prm = ProblemParams(1.0, 1.0, 2.0, 2.0, 100)
+    rng = np.random.default_rng(3)
+    pts = np.column_stack([rng.uniform(0, 1, 512), rng.uniform(0, 1, 512), rng.uniform(0, 3, 512)])
+    times = prm.dt * np.arange(1, prm.nT + 1)
+    return Workload(f"bar_n{m.numberTriangles}", m, prm, 7, DATUM_BAR_H3, pts, times)

@@ -163,6 +163,69 @@ int ebem_timemarch_sa(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh,
 int ebem_pp_sa(const ebem_mesh* mesh, const ebem_problem* prob, const double* phi, const double* pts, int npts,
                const double* times, int ntimes, double* u, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Direct formulation (f/BEMenerg_dir, f/BEMenerg_dirPP).
+ * Rules: outer Gauss-Hammer n_gh in {3,7,12,19}; inner composite rule
+ * (n_sub in {1,4,16,64}, n_sing in {1,3,7,12,19}); DIAG rule n_diag in
+ * {16,64,256,1024} (doppioGauss1D).  "FN n_gh n_sub n_sing n_diag" of
+ * BEMenerg_setupCore.m:86-110.
+ *
+ * flags: EBEM_FIX_REFERENCE_DEFECTS evaluates H(t - r/c_P) in the lambda-mu
+ * term of kernelK (the reference has H(r - r/c_P), kernelK.cu:414-449),
+ * starts the null test's minimum distance at +inf (kernelK.cu:242: 100) and
+ * reads kernelG's nodes with stride n_sing (kernelG.cu:51: 3).  Default 0
+ * reproduces the reference. */
+#define EBEM_FIX_REFERENCE_DEFECTS 1
+
+/* L_V and L_K = min(L_V + 1, nT) (BEMenerg_dir_timeMarchingN.m:10,172). */
+int ebem_num_blocks_dir(const ebem_mesh* mesh, const ebem_problem* prob, int* lv, int* lk);
+
+/* Double-layer operator K_lag0..K_{lag0+nlag-1}: nlag x (3N x 3Nv), column
+ * major per lag (entry (3t+i, 3s+j): triangle t, vertex s), host or device.
+ * The off-singular part of kernelK.cu:14-212 (launched by
+ * BEMenerg_dir_timeMarchingN.m:186-206, clamp |x| <= 1e-14, / 4 pi dt) plus,
+ * when n_diag > 0, the same-triangle parts of BEMenerg_dir_calcSubBlockSingK.m
+ * (BEMenerg_dir_timeMarchingN.m:208-264).  Lags >= L_K stay zero.
+ * accumulate = 0 zeroes the output first. */
+int ebem_assemble_k(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int n_sub, int n_sing, int n_diag,
+                    int lag0, int nlag, int flags, double* K, int accumulate, void* stream);
+
+/* Single-layer operator of the direct formulation, V_lag0..: nlag x (3N x 3N):
+ * kernelV.cu off the diagonal (BEMenerg_dir_launchKernelV.m) and the DIAG-rule
+ * diagonal blocks of BEMenerg_dir_calcSubBlockDiagV.m
+ * (BEMenerg_dir_timeMarchingN.m:94-160).  n_diag > 0 is required. */
+int ebem_assemble_v(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int n_sub, int n_sing, int n_diag,
+                    int lag0, int nlag, double* V, void* stream);
+
+/* DN time marching (BEMenerg_dir_timeMarchingN.m:268-299): beta_V,n =
+ * sum_j V_{n-j} gV_j (BEMenerg_dir_calcBetaVgpu.m), then per step the least
+ * squares solution of (K_0 + I_Gamma) u_n = beta_V,n + I_Gamma u_{n-1} -
+ * sum_{l=1}^{min(n,LK)-1} K_l u_{n-l} (the reference's mldivide of a 3N x 3Nv
+ * system), I_Gamma = kron((vertex in triangle) area / 6, eye(3)).
+ * V: LV x 3N x 3N; K: LK x 3N x 3Nv; gV: 3N x nT; u: 3Nv x nT. */
+int ebem_march_dn(const ebem_mesh* mesh, const ebem_problem* prob, const double* V, int LV, const double* K, int LK,
+                  const double* gV, double* u, void* stream);
+
+/* DD time marching (BEMenerg_dir_timeMarchingD.m:272-296): V_0 phi_n =
+ * rhs_n / 2 + beta_K,n - sum_l V_l phi_{n-l}, beta_K,n = sum_j K_{n-j} gK_j.
+ * rhs: 3N x nT; gK: 3Nv x nT; phi: 3N x nT. */
+int ebem_march_dd(const ebem_mesh* mesh, const ebem_problem* prob, const double* V, int LV, const double* K, int LK,
+                  const double* rhs, const double* gK, double* phi, void* stream);
+
+/* Direct post-processing u(x, t) = sum_{n=1}^{nHat} G_n a_n - P_n b_n at npts
+ * points and ntimes times (BEMenerg_ppN_calc.m:115-124 with a = gV, b = u;
+ * BEMenerg_ppD_calc.m:91-99 with a = phi, b = gK), G of kernelG.cu and P of
+ * kernelP.cu on the composite rule (n_sub, n_sing), contracted on the device.
+ * a: 3N x nT; b: 3Nv x nT; u: ntimes x npts x 3; times host, <= tfin. */
+int ebem_pp_dir(const ebem_mesh* mesh, const ebem_problem* prob, int n_sub, int n_sing, int flags, const double* a,
+                const double* b, const double* pts, int npts, const double* times, int ntimes, double* u,
+                void* stream);
+
+/* The matrices of one (x, t) as the reference builds them (BEMenerg_ppN_calc.m:
+ * 80-109): G (3 nHat x 3N) and P (3 nHat x 3Nv) column major, nHat = ceil(t/dt). */
+int ebem_pp_dir_matrices(const ebem_mesh* mesh, const ebem_problem* prob, int n_sub, int n_sing, int flags,
+                         const double* x, double t, double* G, double* P);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,15 @@ def lib(variant: str = "f64"):
         L.or_field_integrals.argtypes = [_dp, C.c_int, _ip, C.c_int, C.c_double, C.c_double, C.c_int, _dp,
                                          C.c_double, _dp]
         L.or_field_integrals.restype = C.c_int
+        if variant == "f64":
+            mat = [C.c_double, C.c_double, C.c_double, C.c_double]    # rho, mu, lambda, dt
+            L.or_p1_coeffs.argtypes = mesh_args + [C.c_int, _dp, _dp]
+            L.or_doppio_gauss.argtypes = [C.c_int, _dp, _dp]
+            L.or_assemble_k.argtypes = mesh_args + mat + [C.c_int] * 7 + [_dp, C.c_int]
+            L.or_k_sing.argtypes = mesh_args + mat + [C.c_int] * 4 + [_dp, C.c_int]
+            L.or_v_diag.argtypes = mesh_args + mat + [C.c_int] * 4 + [_dp, C.c_int]
+            L.or_pp_dir_g.argtypes = mesh_args + mat + [C.c_int, C.c_int, _dp, C.c_double, C.c_int, _dp]
+            L.or_pp_dir_p.argtypes = mesh_args + mat + [C.c_int, C.c_int, _dp, C.c_double, _dp]
         _LIBS[variant] = L
     return _LIBS[variant]
 
@@ -219,3 +228,146 @@ def ref_ghc(mesh, prm, n_gh: int, n_sub: int, n_sing: int, nlag: int):
         raise RuntimeError(f"reference kernelGHC launch failed ({rc})")
     n3 = 3 * N
     return E.reshape(nlag, n3, n3).transpose(0, 2, 1)
+
+
+# ---------------------------------------------------------------------------
+# direct formulation (dir_oracle.cpp)
+
+def _mat(prm):
+    return (float(prm.rho), float(prm.mu), float(prm.lam), float(prm.dt))
+
+
+def p1_coeffs(mesh, unit_normal: bool = False):
+    """P1 basis of every triangle: phi_k(y) = v[t, k] + M[t, k, :] . y."""
+    N = mesh.numberTriangles
+    M = np.zeros((N, 3, 3)); v = np.zeros((N, 3))
+    lib().or_p1_coeffs(*_m(mesh), int(unit_normal), M.reshape(-1), v.reshape(-1))
+    return M, v
+
+
+def doppio_gauss(n: int):
+    nodes = np.zeros((n, 3)); w = np.zeros(n)
+    if lib().or_doppio_gauss(n, nodes.reshape(-1), w):
+        raise ValueError(f"invalid DIAG rule size {n}")
+    return nodes, w
+
+
+def num_blocks_dir(mesh, prm):
+    """(L_V, L_K) of BEMenerg_dir_timeMarchingN.m:10,172."""
+    LV = num_blocks(mesh, prm)
+    return LV, min(LV + 1, prm.nT)
+
+
+def assemble_k(mesh, prm, n_gh, n_sub, n_sing, lag0, nlag, nblocks=None, fix=False, nthreads=0):
+    """K_l off-singular part (kernelK.cu), returned as K[l][row, col] with
+    shape (nlag, 3N, 3Nv)."""
+    N, Nv = mesh.numberTriangles, mesh.number_nodes
+    if nblocks is None:
+        nblocks = num_blocks_dir(mesh, prm)[1]
+    K = np.zeros(nlag * 9 * N * Nv)
+    rc = lib().or_assemble_k(*_m(mesh), *_mat(prm), n_gh, n_sub, n_sing, lag0, nlag, nblocks, int(fix), K, nthreads)
+    if rc:
+        raise ValueError("invalid rule")
+    return K.reshape(nlag, 3 * Nv, 3 * N).transpose(0, 2, 1)
+
+
+def k_sing(mesh, prm, n_gh, n_diag, lag0, nlag, nthreads=0):
+    """Same-triangle parts of K_l (calcSubBlockSingK.m), shape (nlag, 3N, 3Nv)."""
+    N, Nv = mesh.numberTriangles, mesh.number_nodes
+    K = np.zeros(nlag * 9 * N * Nv)
+    if lib().or_k_sing(*_m(mesh), *_mat(prm), n_gh, n_diag, lag0, nlag, K, nthreads):
+        raise ValueError("invalid rule")
+    return K.reshape(nlag, 3 * Nv, 3 * N).transpose(0, 2, 1)
+
+
+def v_diag(mesh, prm, n_gh, n_diag, lag0, nlag, nthreads=0):
+    """Diagonal blocks of V_l on the DIAG rule (calcSubBlockDiagV.m), as a
+    (nlag, 3N, 3N) array that is zero off the diagonal blocks."""
+    N = mesh.numberTriangles
+    V = np.zeros(nlag * 9 * N * N)
+    if lib().or_v_diag(*_m(mesh), *_mat(prm), n_gh, n_diag, lag0, nlag, V, nthreads):
+        raise ValueError("invalid rule")
+    return V.reshape(nlag, 3 * N, 3 * N).transpose(0, 2, 1)
+
+
+def pp_dir_matrices(mesh, prm, n_sub, n_sing, x, t, fix=False):
+    """(G, P) of kernelG.cu / kernelP.cu at one point and time: G (3 nHat, 3N),
+    P (3 nHat, 3 Nv)."""
+    N, Nv = mesh.numberTriangles, mesh.number_nodes
+    nhat = int(np.ceil(t / prm.dt)) if t > 0 else 0
+    G = np.zeros(9 * nhat * N); Pm = np.zeros(9 * nhat * Nv)
+    xs = np.ascontiguousarray(x, np.float64)
+    if lib().or_pp_dir_g(*_m(mesh), *_mat(prm), n_sub, n_sing, xs, float(t), int(fix), G):
+        raise ValueError("invalid rule for kernelG")
+    if lib().or_pp_dir_p(*_m(mesh), *_mat(prm), n_sub, n_sing, xs, float(t), Pm):
+        raise ValueError("invalid rule")
+    return G.reshape(3 * N, 3 * nhat).T, Pm.reshape(3 * Nv, 3 * nhat).T
+
+
+def ref_dir_available() -> bool:
+    return all(os.path.exists(os.path.join(_HERE, "_ref", f)) for f in ("libref_k.so", "libref_g.so", "libref_p.so"))
+
+
+def _ref_mesh_arrays(mesh, unit_normal):
+    N, Nv = mesh.numberTriangles, mesh.number_nodes
+    P = mesh.coordinates[mesh.triangles]
+    verts = np.ascontiguousarray(P.transpose(0, 2, 1).reshape(-1))          # 9t + 3*coord + vertex
+    normT = np.ascontiguousarray(mesh.normal.reshape(-1))
+    ism = np.zeros((Nv, N), np.int32)                                         # s*N + m
+    for m_, tri in enumerate(mesh.triangles):
+        for k, s in enumerate(tri):
+            ism[s, m_] = k + 1
+    M, v = p1_coeffs(mesh, unit_normal)
+    matc = np.ascontiguousarray(M.transpose(0, 2, 1).reshape(-1))            # 9m + 3j + i = M(i, j)
+    return verts, normT, np.ascontiguousarray(ism.reshape(-1)), matc, np.ascontiguousarray(v.reshape(-1))
+
+
+def ref_k(mesh, prm, n_gh, n_sub, n_sing, nlag, nblocks=None):
+    """The reference's own kernelK (compiled into oracle/_ref): (nlag, 3N, 3Nv)."""
+    L = C.CDLL(os.path.join(_HERE, "_ref", "libref_k.so"))
+    _ip_ = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    L.ref_k.argtypes = [_dp, C.c_int, C.c_int, C.c_int] + [C.c_double] * 6 + [_dp, _dp, C.c_int, _dp, _dp, C.c_int,
+                        C.c_int, _dp, _dp, _dp, _ip_, _dp, _dp, C.c_int, C.c_int, _dp, C.c_double]
+    N, Nv = mesh.numberTriangles, mesh.number_nodes
+    if nblocks is None:
+        nblocks = num_blocks_dir(mesh, prm)[1]
+    gn, gw = gauss_hammer(n_gh, 1)
+    cn, cw = gauss_hammer(n_sing, n_sub)
+    verts, normT, ism, matc, vetc = _ref_mesh_arrays(mesh, False)
+    K = np.zeros(9 * N * Nv * nlag)
+    rc = L.ref_k(K, N, Nv, nlag, prm.dt, prm.velP, prm.velS, prm.lam, prm.mu, prm.rho, np.ascontiguousarray(gw),
+                 np.ascontiguousarray(gn), n_gh, np.ascontiguousarray(cw), np.ascontiguousarray(cn), n_sub, n_sing,
+                 verts, np.ascontiguousarray(mesh.area), normT, ism, matc, vetc, 0, nblocks,
+                 np.ascontiguousarray(mesh.coordinates.reshape(-1)), float(mesh.maxL.max()))
+    if rc:
+        raise RuntimeError(f"reference kernelK launch failed ({rc})")
+    return K.reshape(nlag, 3 * Nv, 3 * N).transpose(0, 2, 1)
+
+
+def ref_pp_dir(mesh, prm, n_sub, n_sing, x, t):
+    """The reference's own kernelG / kernelP at one (x, t): (G, P)."""
+    Lg = C.CDLL(os.path.join(_HERE, "_ref", "libref_g.so"))
+    Lp = C.CDLL(os.path.join(_HERE, "_ref", "libref_p.so"))
+    _ip_ = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    Lg.ref_g.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp, C.c_int,
+                         C.c_int, _dp, _dp, _dp, _dp]
+    Lp.ref_p.argtypes = [_dp, C.c_int, C.c_int, C.c_int] + [C.c_double] * 6 + [_dp, _dp, _dp, _dp, C.c_int, C.c_int,
+                                                                               _dp, _dp, _dp, _ip_, _dp, _dp]
+    N, Nv = mesh.numberTriangles, mesh.number_nodes
+    nhat = int(np.ceil(t / prm.dt))
+    diff = np.ascontiguousarray(t - np.arange(nhat + 2) * prm.dt)
+    pn, pw = gauss_hammer(n_sing, n_sub)
+    verts, normT, ism, matc, vetc = _ref_mesh_arrays(mesh, True)
+    xs = np.ascontiguousarray(x, np.float64)
+    G = np.zeros(9 * nhat * N); P = np.zeros(9 * nhat * Nv)
+    rc = Lg.ref_g(G, N, nhat, prm.velP, prm.velS, prm.rho, xs, diff, np.ascontiguousarray(pw), np.ascontiguousarray(pn),
+                  n_sub, n_sing, verts, np.ascontiguousarray(mesh.area), np.ascontiguousarray(mesh.center.reshape(-1)),
+                  np.ascontiguousarray(mesh.maxL))
+    if rc:
+        raise RuntimeError(f"reference kernelG launch failed ({rc})")
+    rc = Lp.ref_p(P, N, Nv, nhat, prm.velP, prm.velS, prm.lam, prm.mu, prm.rho, prm.dt, xs, diff,
+                  np.ascontiguousarray(pw), np.ascontiguousarray(pn), n_sub, n_sing, verts,
+                  np.ascontiguousarray(mesh.area), normT, ism, matc, vetc)
+    if rc:
+        raise RuntimeError(f"reference kernelP launch failed ({rc})")
+    return G.reshape(3 * N, 3 * nhat).T, P.reshape(3 * Nv, 3 * nhat).T

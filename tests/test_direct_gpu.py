@@ -1,0 +1,186 @@
+"""Direct formulation on the device (BEMenerg_dir / BEMenerg_dirPP): the
+double-layer operator K_l with its singular parts, the single-layer V_l with
+its DIAG-rule diagonal, the post-processing matrices and their contraction,
+and the DN / DD time marching, against the oracle's restatement
+(oracle/dir_oracle.cpp) and, where the reference's own CUDA kernels were
+compiled from its sources into oracle/_ref, against those kernels."""
+import numpy as np
+import pytest
+
+from conftest import cuda_available
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10           # device vs the FP64 restatement (different summation order)
+TOL_REF = 1e-12       # restatement vs the reference's own kernel
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def ebem():
+    if not cuda_available():
+        pytest.skip("no CUDA device")
+    import elastodynamicebem_b200.core as core
+    return core
+
+
+@pytest.fixture(scope="module")
+def bar():
+    from elastodynamicebem_b200 import mesh, problem
+    return mesh.prism_bar(1.0, 1.0, 3.0, 0.5), problem.ProblemParams(1.0, 1.0, 2.0, 2.0, 20)
+
+
+@pytest.mark.parametrize("fix", [False, True])
+def test_k_matches_oracle(ebem, oracle, bar, fix):
+    m, prm = bar
+    dm = ebem.DeviceMesh(m)
+    LV, LK = ebem.num_blocks_dir(dm, prm)
+    assert (LV, LK) == oracle.num_blocks_dir(m, prm)
+    nl = 8
+    K = ebem.assemble_k(dm, prm, 7, 4, 3, 16, 0, nl, fix=fix).cpu().numpy()
+    Ko = oracle.assemble_k(m, prm, 7, 4, 3, 0, nl, nblocks=LK, fix=fix) + oracle.k_sing(m, prm, 7, 16, 0, nl)
+    assert np.isfinite(K).all()
+    assert rel(K, Ko) <= TOL
+    for l in range(nl):
+        if np.linalg.norm(Ko[l]) > 1e-8:
+            assert rel(K[l], Ko[l]) <= 1e-9, l
+
+
+def test_k_lag_window(ebem, bar):
+    """A lag panel equals the same lags of the full assembly."""
+    m, prm = bar
+    dm = ebem.DeviceMesh(m)
+    full = ebem.assemble_k(dm, prm, 3, 1, 3, 16, 0, 10).cpu().numpy()
+    part = ebem.assemble_k(dm, prm, 3, 1, 3, 16, 4, 5).cpu().numpy()
+    assert rel(part, full[4:9]) <= 1e-13
+
+
+def test_v_matches_oracle(ebem, oracle, bar):
+    m, prm = bar
+    dm = ebem.DeviceMesh(m)
+    nl = 8
+    V = ebem.assemble_v(dm, prm, 7, 4, 3, 16, 0, nl).cpu().numpy()
+    Vo = oracle.assemble_ghc(m, prm, 7, 4, 3, 0, nl) + oracle.v_diag(m, prm, 7, 16, 0, nl)
+    assert rel(V, Vo) <= TOL
+
+
+def test_pp_matrices_match_oracle(ebem, oracle, bar):
+    m, prm = bar
+    dm = ebem.DeviceMesh(m)
+    x = np.array([0.4, 0.55, 1.7])
+    for t in (0.3, 1.0, 2.0):
+        G, P = ebem.pp_dir_matrices(dm, prm, 4, 3, x, t)
+        Go, Po = oracle.pp_dir_matrices(m, prm, 4, 3, x, t)
+        assert rel(G, Go) <= TOL and rel(P, Po) <= TOL
+
+
+def test_pp_contraction(ebem, oracle, bar):
+    """u = sum_n G_n a_n - P_n b_n contracted in the kernel equals the
+    contraction of the oracle's matrices."""
+    import torch
+    m, prm = bar
+    dm = ebem.DeviceMesh(m)
+    rng = np.random.default_rng(7)
+    a = rng.normal(size=(prm.nT, 3 * m.numberTriangles))
+    b = rng.normal(size=(prm.nT, 3 * m.number_nodes))
+    pts = np.array([[0.3, 0.6, 0.9], [0.5, 0.5, 2.5], [0.8, 0.2, 1.4]])
+    times = np.array([0.25, 1.0, 1.9])
+    u = ebem.pp_dir(dm, prm, 4, 3, torch.tensor(a, device="cuda"), torch.tensor(b, device="cuda"), pts,
+                    times).cpu().numpy()
+    for q, t in enumerate(times):
+        for ip, x in enumerate(pts):
+            G, P = oracle.pp_dir_matrices(m, prm, 4, 3, x, t)
+            nh = G.shape[0] // 3
+            ref = sum(G[3 * n:3 * n + 3] @ a[n] - P[3 * n:3 * n + 3] @ b[n] for n in range(nh))
+            assert np.linalg.norm(u[q, ip] - ref) <= TOL * max(np.linalg.norm(ref), 1e-12), (q, ip)
+
+
+def _march_dn_numpy(m, prm, V, K, gV):
+    """BEMenerg_dir_timeMarchingN.m:268-299 in numpy (least squares)."""
+    N, Nv = m.numberTriangles, m.number_nodes
+    LV, LK = V.shape[0], K.shape[0]
+    I = np.zeros((3 * N, 3 * Nv))
+    for x, tri in enumerate(m.triangles):
+        for s in tri:
+            I[3 * x:3 * x + 3, 3 * s:3 * s + 3] += np.eye(3) * m.area[x] / 6
+    beta = np.zeros((prm.nT, 3 * N))
+    for n in range(prm.nT):
+        for j in range(n + 1):
+            if n - j < LV:
+                beta[n] += V[n - j] @ gV[j]
+    A = K[0] + I
+    u = np.zeros((prm.nT, 3 * Nv))
+    for n in range(prm.nT):
+        r = beta[n].copy()
+        if n > 0:
+            r += I @ u[n - 1]
+        for l in range(1, min(n + 1, LK)):
+            r -= K[l] @ u[n - l]
+        u[n] = np.linalg.lstsq(A, r, rcond=None)[0]
+    return u
+
+
+def test_march_dn(ebem, oracle, bar):
+    import torch
+    from elastodynamicebem_b200 import problem
+    m, prm = bar
+    dm = ebem.DeviceMesh(m)
+    LV, LK = ebem.num_blocks_dir(dm, prm)
+    V = ebem.assemble_v(dm, prm, 7, 4, 3, 16, 0, LV)
+    K = ebem.assemble_k(dm, prm, 7, 4, 3, 16, 0, LK)
+    gV = torch.tensor(problem.bar_neumann(m, prm, 3.0), device="cuda")
+    u = ebem.march_dn(dm, prm, V, K, gV).cpu().numpy()
+    ref = _march_dn_numpy(m, prm, V.cpu().numpy(), K.cpu().numpy(), gV.cpu().numpy())
+    assert np.isfinite(u).all()
+    assert rel(u, ref) <= 1e-9
+
+
+def test_march_dd(ebem, bar):
+    import torch
+    from elastodynamicebem_b200 import problem
+    m, prm = bar
+    dm = ebem.DeviceMesh(m)
+    LV, LK = ebem.num_blocks_dir(dm, prm)
+    V = ebem.assemble_v(dm, prm, 7, 4, 3, 16, 0, LV)
+    K = ebem.assemble_k(dm, prm, 7, 4, 3, 16, 0, LK)
+    gK = torch.tensor(problem.bar_dirichlet(m, prm, 3.0), device="cuda")
+    b = ebem.rhs(dm, prm, 7, problem.DATUM_BAR_H3)
+    phi = ebem.march_dd(dm, prm, V, K, b, gK).cpu().numpy()
+    Vn, Kn, bn, gn = V.cpu().numpy(), K.cpu().numpy(), b.cpu().numpy(), gK.cpu().numpy()
+    ref = np.zeros_like(phi)
+    for n in range(prm.nT):
+        r = bn[n] / 2
+        for j in range(n + 1):
+            if n - j < LK:
+                r = r + Kn[n - j] @ gn[j]
+        for l in range(1, min(n + 1, LV)):
+            r = r - Vn[l] @ ref[n - l]
+        ref[n] = np.linalg.solve(Vn[0], r)
+    assert rel(phi, ref) <= 1e-9
+
+
+# ---------------------------------------------------------------------------
+# pins against the reference's own CUDA kernels (compiled from its sources)
+
+def test_oracle_k_matches_reference_kernel(oracle, bar):
+    if not cuda_available() or not oracle.ref_dir_available():
+        pytest.skip("reference kernels not built (oracle/_ref) or no device")
+    m, prm = bar
+    nl = 6
+    Kr = oracle.ref_k(m, prm, 7, 4, 3, nl)
+    Ko = oracle.assemble_k(m, prm, 7, 4, 3, 0, nl)
+    assert rel(Ko, Kr) <= TOL_REF
+
+
+def test_oracle_pp_matches_reference_kernels(oracle, bar):
+    if not cuda_available() or not oracle.ref_dir_available():
+        pytest.skip("reference kernels not built (oracle/_ref) or no device")
+    m, prm = bar
+    x = np.array([0.4, 0.55, 1.7])
+    for t in (0.3, 1.3):
+        Gr, Pr = oracle.ref_pp_dir(m, prm, 4, 3, x, t)
+        Go, Po = oracle.pp_dir_matrices(m, prm, 4, 3, x, t)
+        assert rel(Go, Gr) <= TOL_REF and rel(Po, Pr) <= TOL_REF
