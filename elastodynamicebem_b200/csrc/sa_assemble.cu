@@ -196,17 +196,18 @@ __device__ __forceinline__ void store_entry(const SAArgs& A, int q, int i, int j
     else *dst = v;
 }
 
-// One warp per pair (schedule described in sa_warp.cuh); requires 3 n_gh <= 32.
-#define EBEM_WARPS_PER_BLOCK 4
+// One warp per pair (schedule described in sa_warp.cuh); R children per lane
+// (3 n_gh <= 32 R), WPB warps per block.
 #ifndef EBEM_WARP_MINB
 #define EBEM_WARP_MINB 4   // 128 registers: 4 blocks (16 warps) per SM
 #endif
-__global__ void __launch_bounds__(32 * EBEM_WARPS_PER_BLOCK, EBEM_WARP_MINB) sa_assemble_warp_kernel(SAArgs A) {
-    __shared__ WarpShared Wsh[EBEM_WARPS_PER_BLOCK];
+template <int R, int WPB, int MINB>
+__global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs A) {
+    __shared__ WarpShared<R> Wsh[WPB];
     __shared__ double glx[10], glw[10];
     __shared__ unsigned long long blk_count;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    WarpShared& W = Wsh[wib];
+    WarpShared<R>& W = Wsh[wib];
     if (threadIdx.x < 10) {
         const int k = threadIdx.x < 5 ? threadIdx.x : threadIdx.x - 5;
         glx[threadIdx.x] = (threadIdx.x < 5 ? -1.0 : 1.0) * gl_x(k);
@@ -215,10 +216,10 @@ __global__ void __launch_bounds__(32 * EBEM_WARPS_PER_BLOCK, EBEM_WARP_MINB) sa_
     if (threadIdx.x == 0) blk_count = 0;
     __syncthreads();
     const long long NP = A.diag_only ? (long long)A.nsrc : (long long)A.nsrc * A.N;
-    const long long nwarps = (long long)gridDim.x * EBEM_WARPS_PER_BLOCK;
+    const long long nwarps = (long long)gridDim.x * WPB;
     const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
     unsigned long long my_count = 0;
-    for (long long p = (long long)blockIdx.x * EBEM_WARPS_PER_BLOCK + wib; p < NP; p += nwarps) {
+    for (long long p = (long long)blockIdx.x * WPB + wib; p < NP; p += nwarps) {
         const int i = A.src0 + (int)(p % A.nsrc);
         const int j = A.diag_only ? i : (int)(p / A.nsrc);
         const TriGeom& F = A.geo[j];
@@ -243,36 +244,40 @@ __global__ void __launch_bounds__(32 * EBEM_WARPS_PER_BLOCK, EBEM_WARP_MINB) sa_
             }
         }
         if (llo < 0) continue;
-        // lane = child c of outer node g
-        LaneChild C;
-        C.live = false;
-        C.zeta = 0.0; C.sigma = 0.0; C.dMIN = 0.0; C.w = 0.0;
-        {
-            const int g = lane / 3, c = lane - 3 * (lane / 3);
+        // slot u of this lane = child c of outer node g, slot = lane + 32 u = 3 g + c
+        LaneChild C[R];
+        bool hasmom[R];
+#pragma unroll
+        for (int u = 0; u < R; u++) {
+            const int slot = lane + 32 * u;
+            LaneChild& Cu = C[u];
+            Cu.live = false;
+            Cu.zeta = 0.0; Cu.sigma = 0.0; Cu.dMIN = 0.0; Cu.w = 0.0;
+            hasmom[u] = false;
+            const int g = slot / 3, c = slot - 3 * (slot / 3);
             if (g < A.n_gh) {
                 NodeW sp = A.nodes[(size_t)i * A.n_gh + g];
                 NodeGeo G;
                 node_geo(G, sp, F);
-                C.zeta = G.zeta;
-                C.sigma = G.sigma;
-                C.dMIN = G.dMIN;
-                C.w = sp.w;
-                if (node_child_e(C.g, G, c)) {
-                    C.live = true;
-                    m_sincos(C.g.gamma, &C.sg, &C.cg);
+                Cu.zeta = G.zeta;
+                Cu.sigma = G.sigma;
+                Cu.dMIN = G.dMIN;
+                Cu.w = sp.w;
+                if (node_child_e(Cu.g, G, c)) {
+                    Cu.live = true;
+                    m_sincos(Cu.g.gamma, &Cu.sg, &Cu.cg);
                 }
             }
+            if (Cu.live) {
+                const ChildE& gg = Cu.g;
+                W.F[slot] = gg.F;
+                W.cbp[slot] = gg.cb * gg.ct + gg.sb * gg.st;     // cos(beta - theta_V1)
+                W.sbp[slot] = gg.sb * gg.ct - gg.cb * gg.st;     // sin(beta - theta_V1)
+                W.zeta[slot] = Cu.zeta;
+                W.zs[slot] = Cu.zeta * Cu.sigma;
+                W.scale[slot] = Cu.w * gg.sgnC;
+            }
         }
-        if (C.live) {
-            const ChildE& g = C.g;
-            W.F[lane] = g.F;
-            W.cbp[lane] = g.cb * g.ct + g.sb * g.st;     // cos(beta - theta_V1)
-            W.sbp[lane] = g.sb * g.ct - g.cb * g.st;     // sin(beta - theta_V1)
-            W.zeta[lane] = C.zeta;
-            W.zs[lane] = C.zeta * C.sigma;
-            W.scale[lane] = C.w * g.sgnC;
-        }
-        bool hasmom = false;
         __syncwarp();
         const int klo = max(1, llo - 1), khi = lhi + 1;
         double Fm2[6] = {0, 0, 0, 0, 0, 0}, Fm1[6] = {0, 0, 0, 0, 0, 0}, Fk[6];
@@ -286,64 +291,75 @@ __global__ void __launch_bounds__(32 * EBEM_WARPS_PER_BLOCK, EBEM_WARP_MINB) sa_
             L.k1 = 1.0 / vp2;
             L.k5 = (vp2 + vs2) / den;
             L.k6 = (vp2 - vs2) / den;
-            // decision phase (per child)
-            int type = T_NONE;
-            double rhoP = -1.0, rhoS = -1.0;
-            if (C.live) type = classify(C.zeta, L.RP, L.RS, C.dMIN, rhoP, rhoS);
-            AccE Ac = {0, 0, 0, 0, 0, 0, 0};
-            Piece pc[3];
-            int np = 0, full = 0;
-            if (type != T_NONE) child_decide(Ac, pc, np, full, C, L, rhoP, rhoS, type);
-            // whole-range moments, computed by the whole warp once per child
-            const bool need = full && !hasmom;
-            unsigned mm = __ballot_sync(0xffffffffu, need);
-            while (mm) {
-                const int b = __ffs(mm) - 1;
-                mm &= mm - 1;
-                const double Fb = __shfl_sync(0xffffffffu, C.g.F, b), cbb = __shfl_sync(0xffffffffu, C.g.cb, b);
-                const double sbb = __shfl_sync(0xffffffffu, C.g.sb, b), zb = __shfl_sync(0xffffffffu, C.zeta, b);
-                const double s1b = __shfl_sync(0xffffffffu, C.g.s1, b), s0b = __shfl_sync(0xffffffffu, C.g.s0, b);
-                double m[14];
-                moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx, glw);
-#pragma unroll
-                for (int e = 0; e < 14; e++) m[e] = warp_sum(m[e]);
-                if (lane == b) {
-#pragma unroll
-                    for (int e = 0; e < 14; e++) W.mom[e][lane] = m[e];
-                }
-            }
-            if (need) hasmom = true;
-            const double zs = C.zeta * C.sigma;
-            if (full & 1) apply_moments(Ac, W, lane, true, L, zs);
-            if (full & 2) apply_moments(Ac, W, lane, false, L, zs);
             double S = 0.0, T[6] = {0, 0, 0, 0, 0, 0};
-            if (type != T_NONE) child_to_plane(S, T, Ac, C.g, C.w * C.g.sgnC);
-            // partial edge pieces -> per-warp list
-            int nsubs[3];
-            double hs[3];
-            int nn = 0;
+            Piece pc[R][3];
+            int np[R], nsubs[R][3];
+            double hs[R][3];
+            int nn = 0, npl = 0;
 #pragma unroll
-            for (int u = 0; u < 3; u++) {
-                if (u < np) {
-                    double len = pc[u].shi - pc[u].slo;
-                    int ns = (int)ceil(len * (1.0 / EBEM_EDGE_H));
-                    ns = max(1, min(ns, 4096));
-                    nsubs[u] = ns;
-                    hs[u] = len / ns;
-                    nn += 10 * ns;
+            for (int u = 0; u < R; u++) {
+                const int slot = lane + 32 * u;
+                const LaneChild& Cu = C[u];
+                // decision phase (per child)
+                int type = T_NONE;
+                double rhoP = -1.0, rhoS = -1.0;
+                if (Cu.live) type = classify(Cu.zeta, L.RP, L.RS, Cu.dMIN, rhoP, rhoS);
+                AccE Ac = {0, 0, 0, 0, 0, 0, 0};
+                int full = 0;
+                np[u] = 0;
+                if (type != T_NONE) child_decide(Ac, pc[u], np[u], full, Cu, L, rhoP, rhoS, type);
+                // whole-range moments, computed by the whole warp once per child
+                const bool need = full && !hasmom[u];
+                unsigned mm = __ballot_sync(0xffffffffu, need);
+                while (mm) {
+                    const int b = __ffs(mm) - 1;
+                    mm &= mm - 1;
+                    const double Fb = __shfl_sync(0xffffffffu, Cu.g.F, b), cbb = __shfl_sync(0xffffffffu, Cu.g.cb, b);
+                    const double sbb = __shfl_sync(0xffffffffu, Cu.g.sb, b), zb = __shfl_sync(0xffffffffu, Cu.zeta, b);
+                    const double s1b = __shfl_sync(0xffffffffu, Cu.g.s1, b), s0b = __shfl_sync(0xffffffffu, Cu.g.s0, b);
+                    double m[14];
+                    moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx, glw);
+#pragma unroll
+                    for (int e = 0; e < 14; e++) m[e] = warp_sum(m[e]);
+                    if (lane == b) {
+#pragma unroll
+                        for (int e = 0; e < 14; e++) W.mom[e][slot] = m[e];
+                    }
                 }
+                if (need) hasmom[u] = true;
+                const double zs = Cu.zeta * Cu.sigma;
+                if (full & 1) apply_moments(Ac, W, slot, true, L, zs);
+                if (full & 2) apply_moments(Ac, W, slot, false, L, zs);
+                if (type != T_NONE) child_to_plane(S, T, Ac, Cu.g, Cu.w * Cu.g.sgnC);
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    if (q < np[u]) {
+                        double len = pc[u][q].shi - pc[u][q].slo;
+                        int ns = (int)ceil(len * (1.0 / EBEM_EDGE_H));
+                        ns = max(1, min(ns, 4096));
+                        nsubs[u][q] = ns;
+                        hs[u][q] = len / ns;
+                        nn += 10 * ns;
+                    }
+                }
+                npl += np[u];
             }
+            // partial edge pieces of all children -> per-warp list
             int totp, totn;
-            const int pb = warp_excl_scan(np, lane, totp);
+            int pb = warp_excl_scan(npl, lane, totp);
             int o = warp_excl_scan(nn, lane, totn);
 #pragma unroll
-            for (int u = 0; u < 3; u++) {
-                if (u < np) {
-                    W.slo[pb + u] = pc[u].slo;
-                    W.h[pb + u] = hs[u];
-                    W.off[pb + u] = o;
-                    W.who[pb + u] = lane | (pc[u].pterm ? 32 : 0);
-                    o += 10 * nsubs[u];
+            for (int u = 0; u < R; u++) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    if (q < np[u]) {
+                        W.slo[pb] = pc[u][q].slo;
+                        W.h[pb] = hs[u][q];
+                        W.off[pb] = o;
+                        W.who[pb] = (lane + 32 * u) | (pc[u][q].pterm ? 64 : 0);
+                        o += 10 * nsubs[u][q];
+                        pb++;
+                    }
                 }
             }
             if (lane == 31) W.off[totp] = totn;
@@ -355,13 +371,13 @@ __global__ void __launch_bounds__(32 * EBEM_WARPS_PER_BLOCK, EBEM_WARP_MINB) sa_
                 const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
                 const double h = W.h[pp];
                 const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
-                const int who = W.who[pp], cl = who & 31;
+                const int who = W.who[pp], cl = who & 63;
                 double ch, sech, th;
                 hyp(s, ch, sech, th);
                 const double cbq = W.cbp[cl], sbq = W.sbp[cl];
                 const double cq = th * cbq + sech * sbq, sq = sech * cbq - th * sbq;
                 Rad v = radial_edge(W.F[cl] * ch, W.zeta[cl]);
-                W4 w = weigh(v, (who & 32) != 0, L);
+                W4 w = weigh(v, (who & 64) != 0, L);
                 const double f = 0.5 * h * glw[q] * sech * W.scale[cl];
                 const double fin = f * w.in, fmx = -W.zs[cl] * f * w.mx;
                 S += f * w.sc;
@@ -385,17 +401,17 @@ __global__ void __launch_bounds__(32 * EBEM_WARPS_PER_BLOCK, EBEM_WARP_MINB) sa_
                 for (int r = 0; r < 3; r++)
 #pragma unroll
                     for (int c = 0; c < 3; c++) MC[r][c] = M[r][0] * Cm[c] + M[r][1] * Cm[3 + c] + M[r][2] * Cm[6 + c];
-                double R[3][3];
+                double Rm[3][3];
 #pragma unroll
                 for (int r = 0; r < 3; r++)
 #pragma unroll
-                    for (int c = r; c < 3; c++) R[r][c] = Cm[r] * MC[0][c] + Cm[3 + r] * MC[1][c] + Cm[6 + r] * MC[2][c];
-                Fk[0] = 0.5 * (S + R[0][0]);
-                Fk[1] = 0.5 * R[0][1];
-                Fk[2] = 0.5 * R[0][2];
-                Fk[3] = 0.5 * (S + R[1][1]);
-                Fk[4] = 0.5 * R[1][2];
-                Fk[5] = 0.5 * (S + R[2][2]);
+                    for (int c = r; c < 3; c++) Rm[r][c] = Cm[r] * MC[0][c] + Cm[3 + r] * MC[1][c] + Cm[6 + r] * MC[2][c];
+                Fk[0] = 0.5 * (S + Rm[0][0]);
+                Fk[1] = 0.5 * Rm[0][1];
+                Fk[2] = 0.5 * Rm[0][2];
+                Fk[3] = 0.5 * (S + Rm[1][1]);
+                Fk[4] = 0.5 * Rm[1][2];
+                Fk[5] = 0.5 * (S + Rm[2][2]);
             }
             const int l = k - 1;
             if (l >= llo && l <= lhi && lane < 9) {
@@ -413,6 +429,19 @@ __global__ void __launch_bounds__(32 * EBEM_WARPS_PER_BLOCK, EBEM_WARP_MINB) sa_
         __syncthreads();
         if (threadIdx.x == 0 && blk_count) atomicAdd(A.count, blk_count);
     }
+}
+
+template <int R, int WPB, int MINB>
+static int launch_warp(const SAArgs& A, long long NN, int device, cudaStream_t s) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    long long want = (NN + WPB - 1) / WPB;
+    long long cap = (long long)sms * 16 * 4 / WPB;
+    unsigned blocks = (unsigned)(want < cap ? want : cap);
+    if (blocks == 0) blocks = 1;
+    sa_assemble_warp_kernel<R, WPB, MINB><<<blocks, 32 * WPB, 0, s>>>(A);
+    EBEM_CUDA_TRY(cudaGetLastError());
+    return EBEM_OK;
 }
 
 int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
@@ -438,17 +467,8 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
     A.accumulate = accumulate;
     A.count = d_count;
     long long NN = diag_only ? (long long)nsrc : (long long)nsrc * m.nt;
-    if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 32) {
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
-        long long want = (NN + EBEM_WARPS_PER_BLOCK - 1) / EBEM_WARPS_PER_BLOCK;
-        long long cap = (long long)sms * 16;
-        unsigned blocks = (unsigned)(want < cap ? want : cap);
-        if (blocks == 0) blocks = 1;
-        sa_assemble_warp_kernel<<<blocks, 32 * EBEM_WARPS_PER_BLOCK, 0, s>>>(A);
-        EBEM_CUDA_TRY(cudaGetLastError());
-        return EBEM_OK;
-    }
+    if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 32) return launch_warp<1, 4, EBEM_WARP_MINB>(A, NN, m.device, s);
+    if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 64) return launch_warp<2, 2, 4>(A, NN, m.device, s);
     int threads = 128;
     long long blocks = (NN + threads - 1) / threads;
     if (blocks > 0x7fffffffLL) return fail(EBEM_ERR_INVALID, "mesh too large for one launch");

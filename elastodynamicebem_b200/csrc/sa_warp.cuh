@@ -4,7 +4,7 @@
 // same closed-form child integrals of sa_edge.cuh); only the schedule differs:
 //
 // * Lane = child.  Lane 3 g + c owns child c of the projection of outer node g
-//   of the source triangle onto the field plane (3 n_gh <= 32 lanes).  Its
+//   of the source triangle onto the field plane.  Its
 //   geometry (ChildE, the node's zeta, sigma, distance to the triangle and
 //   weight) is level-independent and computed once per pair, not once per
 //   level.
@@ -27,21 +27,23 @@
 //   and the sliding window, lanes 0..8 store the 3x3 block.
 //
 // Grid-stride over pairs (pair p = field j * nsrc + source i - src0, or the
-// diagonal pairs), one warp at a time per pair.
+// diagonal pairs), one warp at a time per pair.  Rules with more than 32
+// children (12 and 19 outer nodes) give each lane two children (R = 2).
 #pragma once
 
 #include "sa_pair.cuh"
 
 namespace ebem {
 
-#define EBEM_WARP_PIECES 96   // <= 3 edge pieces per lane and level
-
+// Per-warp shared state for R children per lane (32 R child slots, at most
+// 3 edge pieces per child and level).
+template <int R>
 struct WarpShared {
-    double slo[EBEM_WARP_PIECES], h[EBEM_WARP_PIECES];
-    int off[EBEM_WARP_PIECES + 1];
-    int who[EBEM_WARP_PIECES];                  // child lane | (P terms ? 32 : 0)
-    double F[32], cbp[32], sbp[32], zeta[32], zs[32], scale[32];
-    double mom[14][32];                         // per-child moments (child frame)
+    double slo[96 * R], h[96 * R];
+    int off[96 * R + 1];
+    int who[96 * R];                            // child slot | (P terms ? 64 : 0)
+    double F[32 * R], cbp[32 * R], sbp[32 * R], zeta[32 * R], zs[32 * R], scale[32 * R];
+    double mom[14][32 * R];                     // per-child moments (child frame)
 };
 
 struct Piece { double slo, shi; int pterm; };
@@ -109,10 +111,11 @@ EBEM_DI void moment_share(double m[14], double F, double cb, double sb, double z
 }
 
 // Whole-range piece from the moments with the level's weights (child frame).
-EBEM_DI void apply_moments(AccE& A, const WarpShared& W, int lane, bool pterm, const LevelCtx& L, double zs) {
+template <int R>
+EBEM_DI void apply_moments(AccE& A, const WarpShared<R>& W, int slot, bool pterm, const LevelCtx& L, double zs) {
     double m[14];
 #pragma unroll
-    for (int e = 0; e < 14; e++) m[e] = W.mom[e][lane];
+    for (int e = 0; e < 14; e++) m[e] = W.mom[e][slot];
     double sc, i0, i1, i2, x0, x1, zz;
     if (pterm) {
         sc = L.k1 * m[0] - L.t2 * m[1];
