@@ -73,13 +73,19 @@ def num_blocks(dmesh: DeviceMesh, prm: ProblemParams) -> int:
     return int(L.value)
 
 
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+
 def assemble_sa(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, lag0: int = 0, nlag: int | None = None,
-                out: torch.Tensor | None = None, accumulate: bool = False, stream=None, count: bool = False):
+                out: torch.Tensor | None = None, accumulate: bool = False, stream=None, count: bool = False,
+                prec: int = PREC_FP64):
     """E_lag0..E_{lag0+nlag-1} on the device.
 
     Returns a tensor ``E`` of shape (nlag, 3N, 3N) with ``E[l][row, col]``
     (a transposed view of the column-major C-ABI buffer), and the number of
-    non-null pair-lags when ``count`` is set.
+    non-null pair-lags when ``count`` is set.  ``prec`` selects FP64 or the
+    FP32-bulk / FP64-inner mixed mode.
     """
     if nlag is None:
         nlag = num_blocks(dmesh, prm) - lag0
@@ -90,10 +96,10 @@ def assemble_sa(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, lag0: int = 0,
         raise ValueError("out must be a contiguous float64 tensor of nlag*(3N)^2 elements")
     p = _lib.problem_struct(prm)
     cnt = C.c_longlong(0)
-    _lib.check(_lib.load().ebem_assemble_sa(dmesh.handle, C.byref(p), int(n_gh), int(lag0), int(nlag),
-                                            out.data_ptr(), int(bool(accumulate)),
-                                            _stream_ptr(stream) if out.is_cuda else None,
-                                            C.byref(cnt) if count else None))
+    _lib.check(_lib.load().ebem_assemble_sa_ex(dmesh.handle, C.byref(p), int(n_gh), int(lag0), int(nlag), 0,
+                                               dmesh.N, out.data_ptr(), n3, int(bool(accumulate)), int(prec),
+                                               _stream_ptr(stream) if out.is_cuda else None,
+                                               C.byref(cnt) if count else None))
     E = out.view(nlag, n3, n3).transpose(1, 2)
     return (E, int(cnt.value)) if count else E
 
@@ -156,7 +162,7 @@ def march(E: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None, str
 
 
 def timemarch_sa(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, datum: int, out: torch.Tensor | None = None,
-                 stream=None):
+                 stream=None, prec: int = PREC_FP64):
     """BEMenerg_coreSA_timeMarching: assembly + right-hand side + marching.
     Returns (phi (nT, 3N), L)."""
     n3 = 3 * dmesh.N
@@ -164,8 +170,8 @@ def timemarch_sa(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, datum: int, o
         out = torch.empty((prm.nT, n3), dtype=torch.float64, device="cuda")
     p = _lib.problem_struct(prm)
     L = C.c_int()
-    _lib.check(_lib.load().ebem_timemarch_sa(dmesh.handle, C.byref(p), int(n_gh), int(datum), _ptr(out), C.byref(L),
-                                             _stream_ptr(stream) if out.is_cuda else None))
+    _lib.check(_lib.load().ebem_timemarch_sa_ex(dmesh.handle, C.byref(p), int(n_gh), int(datum), int(prec), _ptr(out),
+                                                C.byref(L), _stream_ptr(stream) if out.is_cuda else None))
     return out, int(L.value)
 
 

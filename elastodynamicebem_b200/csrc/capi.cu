@@ -253,7 +253,8 @@ int ebem_num_blocks(const ebem_mesh* m, const ebem_problem* p, int* num_blocks) 
 }
 
 static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, int lag0, int nlag, int src0,
-                         int nsrc, double* E, long long ld, int accumulate, void* stream, long long* nonnull) {
+                         int nsrc, double* E, long long ld, int accumulate, void* stream, long long* nonnull,
+                         int prec = EBEM_PREC_FP64) {
     if (!m || !E) return fail(EBEM_ERR_INVALID, "NULL mesh or output");
     if (int rc = check_problem(p)) return rc;
     if (n_gh != 3 && n_gh != 7 && n_gh != 12 && n_gh != 19)
@@ -261,6 +262,7 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
     if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
     if (src0 < 0 || nsrc < 1 || src0 + nsrc > m->d.nt) return fail(EBEM_ERR_INVALID, "source panel outside the mesh");
     if (ld < 3LL * nsrc) return fail(EBEM_ERR_INVALID, "leading dimension smaller than 3 nsrc");
+    if (prec != EBEM_PREC_FP64 && prec != EBEM_PREC_MIXED) return fail(EBEM_ERR_INVALID, "unknown precision mode");
     DeviceGuard dg(m->d.device);
     cudaStream_t s = (cudaStream_t)stream;
     MeshData& md = const_cast<MeshData&>(m->d);
@@ -275,7 +277,8 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
     }
     int rc = EBEM_OK;
     if (is_device_ptr(E)) {
-        rc = launch_sa_assemble(md, P, n_gh, lag0, nlag, src0, nsrc, E, (size_t)ld, lag_elems, accumulate, d_count, s);
+        rc = launch_sa_assemble(md, P, n_gh, lag0, nlag, src0, nsrc, E, (size_t)ld, lag_elems, accumulate, d_count, s, 0,
+                                prec == EBEM_PREC_MIXED);
     } else {
         if (ld != 3LL * nsrc) {
             if (d_count) cudaFree(d_count);
@@ -302,7 +305,7 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
                 break;
             }
             rc = launch_sa_assemble(md, P, n_gh, lag0 + q0, nq, src0, nsrc, d_buf, (size_t)ld, lag_elems, accumulate,
-                                    d_count, s);
+                                    d_count, s, 0, prec == EBEM_PREC_MIXED);
             if (rc) break;
             if (cudaMemcpyAsync(hE, d_buf, per_lag * nq, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
                 rc = fail(EBEM_ERR_CUDA, "download failed");
@@ -384,8 +387,21 @@ int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double
     return out.finish(s);
 }
 
+static int timemarch_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, int datum, double* phi, int* num_blocks,
+                          void* stream, int prec);
+
 int ebem_timemarch_sa(const ebem_mesh* m, const ebem_problem* p, int n_gh, int datum, double* phi, int* num_blocks,
                       void* stream) {
+    return timemarch_impl(m, p, n_gh, datum, phi, num_blocks, stream, EBEM_PREC_FP64);
+}
+
+int ebem_timemarch_sa_ex(const ebem_mesh* m, const ebem_problem* p, int n_gh, int datum, int prec, double* phi,
+                         int* num_blocks, void* stream) {
+    return timemarch_impl(m, p, n_gh, datum, phi, num_blocks, stream, prec);
+}
+
+static int timemarch_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, int datum, double* phi, int* num_blocks,
+                          void* stream, int prec) {
     if (!m || !phi) return fail(EBEM_ERR_INVALID, "NULL mesh or output");
     if (int rc = check_problem(p)) return rc;
     int L = 0;
@@ -400,7 +416,7 @@ int ebem_timemarch_sa(const ebem_mesh* m, const ebem_problem* p, int n_gh, int d
         if (dE) cudaFree(dE);
         return fail(EBEM_ERR_NOMEM, "device allocation of E or the right-hand side failed");
     }
-    int rc = ebem_assemble_sa(m, p, n_gh, 0, L, dE, 0, stream, nullptr);
+    int rc = assemble_impl(m, p, n_gh, 0, L, 0, m->d.nt, dE, 3LL * m->d.nt, 0, stream, nullptr, prec);
     if (!rc) rc = ebem_rhs(m, p, n_gh, datum, dr, stream);
     if (!rc) rc = ebem_march(dE, (int)n3, L, dr, p->nt, phi, stream);
     cudaStreamSynchronize(s);
@@ -429,6 +445,11 @@ int ebem_pp_sa(const ebem_mesh* m, const ebem_problem* p, const double* phi, con
 int ebem_assemble_sa_panel(const ebem_mesh* m, const ebem_problem* p, int n_gh, int lag0, int nlag, int src0,
                            int nsrc, double* E, long long ld, int accumulate, void* stream, long long* nonnull) {
     return assemble_impl(m, p, n_gh, lag0, nlag, src0, nsrc, E, ld, accumulate, stream, nonnull);
+}
+
+int ebem_assemble_sa_ex(const ebem_mesh* m, const ebem_problem* p, int n_gh, int lag0, int nlag, int src0, int nsrc,
+                        double* E, long long ld, int accumulate, int prec, void* stream, long long* nonnull) {
+    return assemble_impl(m, p, n_gh, lag0, nlag, src0, nsrc, E, ld, accumulate, stream, nonnull, prec);
 }
 
 // ---------------------------------------------------------------------------

@@ -62,7 +62,8 @@ PhysParams phys_from(const ebem_problem* p);
 // (column-major 3 nsrc x 3N per lag, leading dimension ld, lag stride ld_lag).
 int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
-                       cudaStream_t s, int diag_only = 0);
+                       cudaStream_t s, int diag_only = 0, int mixed = 0, const int2* pairs = nullptr,
+                       long long npairs = 0);
 int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_sub, int n_sing, int lag0, int nlag,
                         double* d_E, size_t ld, size_t ld_lag, cudaStream_t s);
 

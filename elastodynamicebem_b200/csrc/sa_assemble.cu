@@ -112,6 +112,8 @@ struct SAArgs {
     size_t ld_lag;          // doubles between consecutive lags
     int accumulate;
     unsigned long long* count;
+    const int2* pairs;      // optional explicit (source, field) list (npairs entries)
+    long long npairs;
 };
 
 __device__ __forceinline__ void store_block(const SAArgs& A, int q, int i, int j, const double b[6]) {
@@ -201,7 +203,7 @@ __device__ __forceinline__ void store_entry(const SAArgs& A, int q, int i, int j
 #ifndef EBEM_WARP_MINB
 #define EBEM_WARP_MINB 4   // 128 registers: 4 blocks (16 warps) per SM
 #endif
-template <int R, int WPB, int MINB>
+template <int R, int WPB, int MINB, bool MIXED>
 __global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs A) {
     __shared__ WarpShared<R> Wsh[WPB];
     __shared__ double glx[10], glw[10];
@@ -215,13 +217,20 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs
     }
     if (threadIdx.x == 0) blk_count = 0;
     __syncthreads();
-    const long long NP = A.diag_only ? (long long)A.nsrc : (long long)A.nsrc * A.N;
+    const long long NP = A.pairs ? A.npairs : A.diag_only ? (long long)A.nsrc : (long long)A.nsrc * A.N;
     const long long nwarps = (long long)gridDim.x * WPB;
     const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
     unsigned long long my_count = 0;
     for (long long p = (long long)blockIdx.x * WPB + wib; p < NP; p += nwarps) {
-        const int i = A.src0 + (int)(p % A.nsrc);
-        const int j = A.diag_only ? i : (int)(p / A.nsrc);
+        int i, j;
+        if (A.pairs) {
+            const int2 pj = A.pairs[p];
+            i = pj.x;
+            j = pj.y;
+        } else {
+            i = A.src0 + (int)(p % A.nsrc);
+            j = A.diag_only ? i : (int)(p / A.nsrc);
+        }
         const TriGeom& F = A.geo[j];
         const TriGeom& Sg = A.geo[i];
         double v0 = F.ctr[0] - Sg.ctr[0], v1 = F.ctr[1] - Sg.ctr[1], v2 = F.ctr[2] - Sg.ctr[2];
@@ -276,6 +285,14 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs
                 W.zeta[slot] = Cu.zeta;
                 W.zs[slot] = Cu.zeta * Cu.sigma;
                 W.scale[slot] = Cu.w * gg.sgnC;
+                if (MIXED) {
+                    W.Ff[slot] = (float)W.F[slot];
+                    W.cbpf[slot] = (float)W.cbp[slot];
+                    W.sbpf[slot] = (float)W.sbp[slot];
+                    W.zetaf[slot] = (float)W.zeta[slot];
+                    W.zsf[slot] = (float)W.zs[slot];
+                    W.scalef[slot] = (float)W.scale[slot];
+                }
             }
         }
         __syncwarp();
@@ -366,6 +383,24 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs
             __syncwarp();
             // all lanes: Gauss-Legendre nodes of the list, plane frame
             int pp = 0;
+            if (MIXED) {
+                float Sf = 0.0f, Tf[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                const float k1 = (float)L.k1, t2 = (float)L.t2, k5 = (float)L.k5, k6 = (float)L.k6;
+                for (int idx = lane; idx < totn; idx += 32) {
+                    while (idx >= W.off[pp + 1]) pp++;
+                    const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
+                    const double h = W.h[pp];
+                    const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
+                    const int who = W.who[pp], cl = who & 63;
+                    edge_node_f32(Sf, Tf, s, (float)(0.5 * h * glw[q]), W.Ff[cl], W.cbpf[cl], W.sbpf[cl], W.zetaf[cl],
+                                  W.zsf[cl], W.scalef[cl], (who & 64) != 0, k1, t2, k5, k6);
+                }
+                // per-lane FP32 partial sums join the FP64 lane sums reduced below
+                S += (double)Sf;
+#pragma unroll
+                for (int e = 0; e < 6; e++) T[e] += (double)Tf[e];
+                totn = 0;    // the FP64 loop below has nothing left to do
+            }
             for (int idx = lane; idx < totn; idx += 32) {
                 while (idx >= W.off[pp + 1]) pp++;
                 const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
@@ -431,7 +466,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs
     }
 }
 
-template <int R, int WPB, int MINB>
+template <int R, int WPB, int MINB, bool MIXED>
 static int launch_warp(const SAArgs& A, long long NN, int device, cudaStream_t s) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -439,14 +474,14 @@ static int launch_warp(const SAArgs& A, long long NN, int device, cudaStream_t s
     long long cap = (long long)sms * 16 * 4 / WPB;
     unsigned blocks = (unsigned)(want < cap ? want : cap);
     if (blocks == 0) blocks = 1;
-    sa_assemble_warp_kernel<R, WPB, MINB><<<blocks, 32 * WPB, 0, s>>>(A);
+    sa_assemble_warp_kernel<R, WPB, MINB, MIXED><<<blocks, 32 * WPB, 0, s>>>(A);
     EBEM_CUDA_TRY(cudaGetLastError());
     return EBEM_OK;
 }
 
 int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
-                       cudaStream_t s, int diag_only) {
+                       cudaStream_t s, int diag_only, int mixed, const int2* pairs, long long npairs) {
     SAArgs A;
     A.geo = m.d_geo;
     A.nodes = m.d_nodes;
@@ -466,9 +501,16 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
     A.ld_lag = ld_lag;
     A.accumulate = accumulate;
     A.count = d_count;
+    A.pairs = pairs;
+    A.npairs = npairs;
     long long NN = diag_only ? (long long)nsrc : (long long)nsrc * m.nt;
-    if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 32) return launch_warp<1, 4, EBEM_WARP_MINB>(A, NN, m.device, s);
-    if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 64) return launch_warp<2, 2, 4>(A, NN, m.device, s);
+    if (pairs) NN = npairs;
+    if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 32)
+        return mixed ? launch_warp<1, 4, EBEM_WARP_MINB, true>(A, NN, m.device, s)
+                     : launch_warp<1, 4, EBEM_WARP_MINB, false>(A, NN, m.device, s);
+    if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 64)
+        return mixed ? launch_warp<2, 2, 4, true>(A, NN, m.device, s) : launch_warp<2, 2, 4, false>(A, NN, m.device, s);
+    if (pairs || mixed) return fail(EBEM_ERR_INVALID, "pair lists and mixed precision need the warp kernel");
     int threads = 128;
     long long blocks = (NN + threads - 1) / threads;
     if (blocks > 0x7fffffffLL) return fail(EBEM_ERR_INVALID, "mesh too large for one launch");

@@ -44,7 +44,52 @@ struct WarpShared {
     int who[96 * R];                            // child slot | (P terms ? 64 : 0)
     double F[32 * R], cbp[32 * R], sbp[32 * R], zeta[32 * R], zs[32 * R], scale[32 * R];
     double mom[14][32 * R];                     // per-child moments (child frame)
+    float Ff[32 * R], cbpf[32 * R], sbpf[32 * R], zetaf[32 * R], zsf[32 * R], scalef[32 * R];   // FP32 bulk
 };
+
+// FP32 bulk evaluation of one edge node (mixed precision): s and e^s in
+// FP64 (the node position along the edge, whose relative error is |s| times
+// the unit roundoff), everything after it in FP32.  Adds the weighted,
+// plane-frame contribution to this lane's partial sums (S, T).
+EBEM_DI void edge_node_f32(float& S, float T[6], double s, float wq, float Fc, float cb, float sb, float z, float zs,
+                           float scale, bool pterm, float k1, float t2, float k5, float k6) {
+    const double ed = m_exp(s);
+    const float e = (float)ed, ie = (float)(1.0 / ed);
+    const float ch = 0.5f * (e + ie), sech = __fdividef(1.0f, ch), th = 0.5f * (e - ie) * sech;
+    const float c = th * cb + sech * sb, sn = sech * cb - th * sb;
+    const float R = Fc * ch, z2 = z * z;
+    const float r = sqrtf(R * R + z2);
+    const float q = __fdividef(1.0f, r * (r + R));
+    const float ir = (r + R) * q, ir3 = ir * ir * ir;
+    const float A1 = r, A3 = -ir, B2 = r + z2 * ir, D2 = -z2 * ir;
+    const float B4 = -ir + z2 * ir3 * (1.0f / 3.0f), D4 = -z2 * ir3 * (1.0f / 3.0f);
+    float C2 = 0.0f, C4 = 0.0f;
+    if (z > 0.0f) {
+        C2 = __logf(R + r) - R * ir;
+        C4 = -(r * r + r * R + R * R) * ir3 * (r * q) * (1.0f / 3.0f);
+    }
+    float wsc, win, wmx, wzz;
+    if (pterm) {
+        wsc = k1 * A1 - t2 * A3;
+        win = -k1 * B2 + 3.0f * t2 * B4;
+        wmx = -k1 * C2 + 3.0f * t2 * C4;
+        wzz = -k1 * D2 + 3.0f * t2 * D4;
+    } else {
+        wsc = k5 * A1;
+        win = k6 * B2;
+        wmx = k6 * C2;
+        wzz = k6 * D2;
+    }
+    const float f = wq * sech * scale;
+    const float fin = f * win, fmx = -zs * f * wmx;
+    S += f * wsc;
+    T[0] += fin * c * c;
+    T[1] += fin * sn * c;
+    T[2] += fin * sn * sn;
+    T[3] += fmx * c;
+    T[4] += fmx * sn;
+    T[5] += f * wzz;
+}
 
 struct Piece { double slo, shi; int pterm; };
 

@@ -112,6 +112,22 @@ int ebem_assemble_sa_panel(const ebem_mesh* mesh, const ebem_problem* prob, int 
                            int src0, int nsrc, double* E, long long ld, int accumulate, void* stream,
                            long long* nonnull);
 
+/* Precision of the semi-analytic assembly.  EBEM_PREC_FP64 is the reference's
+ * arithmetic.  EBEM_PREC_MIXED evaluates the bulk quadrature, the Gauss-
+ * Legendre nodes of the edge-bounded pieces (after the node position e^s,
+ * which stays FP64), in FP32 with FP32 per-lane accumulation, and keeps FP64
+ * for the closed-form pieces at the wavefronts and the singularity (crossing
+ * angles, logarithmic terms), the whole-edge moments, the level combination
+ * F_{l+1} - 2 F_l + F_{l-1}, the E_0 factorisation and the time-marching
+ * right-hand side.  No counterpart in the reference (the mixed-precision form
+ * of the assembly). */
+#define EBEM_PREC_FP64 0
+#define EBEM_PREC_MIXED 1
+
+/* ebem_assemble_sa_panel with a precision mode. */
+int ebem_assemble_sa_ex(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag, int src0,
+                        int nsrc, double* E, long long ld, int accumulate, int prec, void* stream, long long* nonnull);
+
 /* Numerical-inner assembly (the reference's GPU method "GPU xx yy z"): outer
  * Gauss-Hammer rule with n_gh nodes on the source triangle, composite rule of
  * n_sub sub-triangles x n_sing nodes on the field triangle, Lamé kernel with
@@ -152,6 +168,10 @@ int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double
  * phi: 3N x nT, host or device; num_blocks (may be NULL) receives L. */
 int ebem_timemarch_sa(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int datum, double* phi,
                       int* num_blocks, void* stream);
+
+/* ebem_timemarch_sa with the assembly in precision mode prec (EBEM_PREC_*). */
+int ebem_timemarch_sa_ex(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int datum, int prec, double* phi,
+                         int* num_blocks, void* stream);
 
 /* Displacement u(x, t) at npts points and ntimes times from the density
  * (closed-form inner integrals, the single-point analogue of the assembly).
