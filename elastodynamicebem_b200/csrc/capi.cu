@@ -611,4 +611,24 @@ int ebem_pp_dir_matrices(const ebem_mesh* m, const ebem_problem* p, int n_sub, i
     return oP.finish(s);
 }
 
+// Full semi-analytic assembly that allocates no device memory of its own (for
+// callers that may not allocate on the device during the call); see
+// ebem_assemble_sa_noalloc in include/ebem.h.
+int ebem_assemble_sa_noalloc(const ebem_mesh* m, const ebem_problem* p, int n_gh, int lag0, int nlag, double* E,
+                             int accumulate, void* stream, long long* nonnull) {
+    if (!m || !E) return fail(EBEM_ERR_INVALID, "NULL mesh or output");
+    if (int rc = check_problem(p)) return rc;
+    if (n_gh != 3 && n_gh != 7 && n_gh != 12 && n_gh != 19)
+        return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+    if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
+    DeviceGuard dg(m->d.device);
+    if (!is_device_ptr(E)) return fail(EBEM_ERR_INVALID, "the allocation-free assembly needs a device output buffer");
+    PhysParams P = phys_from(p);
+    unsigned long long c = 0;
+    int rc = launch_sa_assemble_noalloc(m->d, P, n_gh, lag0, nlag, E, accumulate, nonnull != nullptr, &c,
+                                        (cudaStream_t)stream);
+    if (rc == EBEM_OK && nonnull) *nonnull = (long long)c;
+    return rc;
+}
+
 }  // extern "C"

@@ -64,6 +64,11 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
                        cudaStream_t s, int diag_only = 0, int mixed = 0, const int2* pairs = nullptr,
                        long long npairs = 0);
+// Allocation-free variant of the full assembly (device E, ld = 3N): mapped
+// nodes and the counter live in a static device array (sa_assemble.cu).
+int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, double* d_E,
+                               int accumulate, bool count, unsigned long long* host_count, cudaStream_t s);
+size_t noalloc_max_nodes();
 int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_sub, int n_sing, int lag0, int nlag,
                         double* d_E, size_t ld, size_t ld_lag, cudaStream_t s);
 

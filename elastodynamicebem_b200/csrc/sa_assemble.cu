@@ -22,6 +22,8 @@
 // three-level sliding window (the reference evaluates every instant three
 // times, once per lag that uses it).
 #include "ebem_internal.h"
+
+#include <mutex>
 #include "sa_pair.cuh"
 #include "sa_warp.cuh"
 
@@ -516,6 +518,121 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
     if (blocks > 0x7fffffffLL) return fail(EBEM_ERR_INVALID, "mesh too large for one launch");
     sa_assemble_kernel<<<(unsigned)blocks, threads, 0, s>>>(A);
     EBEM_CUDA_TRY(cudaGetLastError());
+    return EBEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Assembly without device allocations (ebem_assemble_sa_noalloc).
+//
+// The ordinary assembly allocates two small device buffers of its own: the
+// mapped outer nodes of the mesh (cached per rule) and, when the caller asks
+// for the non-null count, an 8-byte counter.  This variant keeps both in one
+// statically allocated device array, so that a call allocates nothing.  The
+// array belongs to every GPU that loads the library until the process exits.
+//
+// Layout (bytes): [0, 8) counter, zeroed by each call that counts; from
+// byte 256 on, the mapped node table, rewritten by each call.  Every call on
+// a device shares the array: calls whose work overlaps on the GPU race.
+
+constexpr size_t kNoAllocScratchBytes = size_t(1) << 20;        // 1 MiB per device
+constexpr size_t kNoAllocNodeOffset = 256;
+constexpr size_t kNoAllocMaxNodes = (kNoAllocScratchBytes - kNoAllocNodeOffset) / sizeof(NodeW);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+size_t noalloc_max_nodes() { return kNoAllocMaxNodes; }
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the host-side name of the array is not a device address).
+static int noalloc_scratch(int device, unsigned char** out) {
+    constexpr int kMaxDevices = 64;
+    static unsigned char* addr[kMaxDevices] = {};
+    static std::mutex mu;
+    if (device < 0 || device >= kMaxDevices) return fail(EBEM_ERR_INVALID, "device ordinal beyond the supported range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(EBEM_ERR_CUDA, std::string("scratch address lookup failed: ") + cudaGetErrorString(e));
+        addr[device] = (unsigned char*)p;
+    }
+    *out = addr[device];
+    return EBEM_OK;
+}
+
+// Outer rule passed by value (no device table).
+struct RuleParam {
+    double b[28][3];
+    double w[28];
+};
+
+__global__ void map_nodes_param_kernel(const double* __restrict__ coords, const int32_t* __restrict__ tris, int nt,
+                                       const TriGeom* __restrict__ geo, RuleParam rule, int n_gh,
+                                       NodeW* __restrict__ out) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nt * n_gh) return;
+    int t = idx / n_gh, g = idx % n_gh;
+    double V[3][3];
+    for (int v = 0; v < 3; v++) {
+        int id = tris[3 * t + v];
+        for (int c = 0; c < 3; c++) V[v][c] = coords[3 * id + c];
+    }
+    const double b0 = rule.b[g][0], b1 = rule.b[g][1], b2 = rule.b[g][2];
+    NodeW o;
+    o.x = b0 * V[0][0] + b1 * V[1][0] + b2 * V[2][0];
+    o.y = b0 * V[0][1] + b1 * V[1][1] + b2 * V[2][1];
+    o.z = b0 * V[0][2] + b1 * V[1][2] + b2 * V[2][2];
+    o.w = geo[t].area * rule.w[g];
+    out[idx] = o;
+}
+
+int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, double* d_E,
+                               int accumulate, bool count, unsigned long long* host_count, cudaStream_t s) {
+    if ((size_t)m.nt * n_gh > kNoAllocMaxNodes)
+        return fail(EBEM_ERR_INVALID, "mesh too large for the allocation-free assembly: N x n_gh = " +
+                                          std::to_string((long long)m.nt * n_gh) + " outer nodes, at most " +
+                                          std::to_string(kNoAllocMaxNodes) + " fit in its 1 MiB scratch array");
+    if (3 * n_gh > 64) return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+    unsigned char* base = nullptr;
+    if (int rc = noalloc_scratch(m.device, &base)) return rc;
+    unsigned long long* d_count = (unsigned long long*)base;
+    NodeW* d_nodes = (NodeW*)(base + kNoAllocNodeOffset);
+    RuleParam rule;
+    if (int rc = gh_composite(n_gh, 1, &rule.b[0][0], rule.w)) return fail(rc, "unsupported Gauss-Hammer rule");
+    const int total = m.nt * n_gh;
+    map_nodes_param_kernel<<<(total + 127) / 128, 128, 0, s>>>(m.d_coords, m.d_tris, m.nt, m.d_geo, rule, n_gh, d_nodes);
+    EBEM_CUDA_TRY(cudaGetLastError());
+    if (count) EBEM_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
+    SAArgs A;
+    A.geo = m.d_geo;
+    A.nodes = d_nodes;
+    A.N = m.nt;
+    A.n_gh = n_gh;
+    A.velP = P.velP;
+    A.velS = P.velS;
+    A.dt = P.dt;
+    A.c4pirho = 4 * kPi * P.rho;
+    A.lag0 = lag0;
+    A.nlag = nlag;
+    A.src0 = 0;
+    A.nsrc = m.nt;
+    A.diag_only = 0;
+    A.E = d_E;
+    A.ld = 3 * (size_t)m.nt;
+    A.ld_lag = A.ld * A.ld;
+    A.accumulate = accumulate;
+    A.count = count ? d_count : nullptr;
+    A.pairs = nullptr;
+    A.npairs = 0;
+    const long long NN = (long long)m.nt * m.nt;
+    int rc = (3 * n_gh <= 32) ? launch_warp<1, 4, EBEM_WARP_MINB, false>(A, NN, m.device, s)
+                              : launch_warp<2, 2, 4, false>(A, NN, m.device, s);
+    if (rc) return rc;
+    if (count) {
+        EBEM_CUDA_TRY(cudaMemcpyAsync(host_count, d_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        EBEM_CUDA_TRY(cudaStreamSynchronize(s));
+    }
     return EBEM_OK;
 }
 

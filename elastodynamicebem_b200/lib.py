@@ -48,6 +48,8 @@ PROTOTYPES = {
                                     C.POINTER(C.c_int), C.c_void_p]),
     "ebem_pp_sa": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                              C.c_void_p, C.c_void_p]),
+    "ebem_assemble_sa_noalloc": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                           C.c_int, C.c_void_p, C.POINTER(C.c_longlong)]),
     "ebem_assemble_sa_ex": (C.c_int, [C.c_void_p, C.POINTER(ProblemC)] + [C.c_int] * 5 + [C.c_void_p, C.c_longlong,
                                       C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_longlong)]),
     "ebem_timemarch_sa_ex": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_int, C.c_void_p,

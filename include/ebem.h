@@ -124,6 +124,29 @@ int ebem_assemble_sa_panel(const ebem_mesh* mesh, const ebem_problem* prob, int 
 #define EBEM_PREC_FP64 0
 #define EBEM_PREC_MIXED 1
 
+/* The full assembly of ebem_assemble_sa (FP64, all source rows), for callers
+ * that may not allocate device memory while they run: code that executes
+ * inside a host framework whose device memory is all handed out by its own
+ * pool, or a time-critical loop where a cudaMalloc/cudaFree (which can
+ * synchronise the device) is not allowed.  No counterpart in the reference.
+ *
+ * It allocates nothing: the two small device buffers the ordinary assembly
+ * allocates for itself (the mesh's mapped outer nodes and the non-null
+ * counter) live here in one statically allocated 1 MiB device array that
+ * every GPU loading the library keeps until the process exits.  Limit:
+ * N x n_gh <= 32760 outer nodes (e.g. 2800 triangles with 7 nodes, 1280 with
+ * 19); larger meshes are rejected with EBEM_ERR_INVALID.  E must be a device
+ * buffer of 9 N^2 nlag doubles.
+ *
+ * The first call on a device looks up the device address of the array (a
+ * one-time set-up); make that first call before any stream capture.  All
+ * calls on a device share the array and each call rewrites it (the counter
+ * is zeroed by every call that asks for nonnull): calls whose work can
+ * overlap on the GPU (different streams, no ordering between them) race and
+ * must be serialised by the caller. */
+int ebem_assemble_sa_noalloc(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag,
+                             double* E, int accumulate, void* stream, long long* nonnull);
+
 /* ebem_assemble_sa_panel with a precision mode. */
 int ebem_assemble_sa_ex(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag, int src0,
                         int nsrc, double* E, long long ld, int accumulate, int prec, void* stream, long long* nonnull);
