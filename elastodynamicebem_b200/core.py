@@ -304,3 +304,54 @@ def pp_dir_matrices(dmesh: DeviceMesh, prm: ProblemParams, n_sub: int, n_sing: i
                                                 FIX_REFERENCE_DEFECTS if fix else 0, xs.ctypes.data, float(t),
                                                 G.ctypes.data, P.ctypes.data))
     return G.reshape(3 * N, 3 * nhat).T, P.reshape(3 * Nv, 3 * nhat).T
+
+
+# ---------------------------------------------------------------------------
+# batched assembly
+
+class BatchPlan:
+    """Many (mesh, problem) instances assembled by one persistent,
+    graph-captured launch (``ebem_batch_*``).  ``assemble()`` returns one
+    tensor per instance, E_k[l][row, col] with shape (nlag_k, 3N_k, 3N_k)."""
+
+    def __init__(self, dmeshes, params, n_gh: int, nlag=None, prec: int = PREC_FP64):
+        L = _lib.load()
+        self.dmeshes = list(dmeshes)
+        self.params = list(params)
+        n = len(self.dmeshes)
+        self._probs = (_lib.ProblemC * n)(*[_lib.problem_struct(p) for p in self.params])
+        handles = (C.c_void_p * n)(*[d.handle.value for d in self.dmeshes])
+        if nlag is None:
+            nlag = [num_blocks(d, p) for d, p in zip(self.dmeshes, self.params)]
+        self.nlag = [int(x) for x in nlag]
+        nl = (C.c_int * n)(*self.nlag)
+        self._h = C.c_void_p()
+        _lib.check(L.ebem_batch_create(C.cast(handles, C.c_void_p), C.cast(self._probs, C.c_void_p),
+                                       C.cast(nl, C.c_void_p), n, int(n_gh), int(prec), C.byref(self._h)))
+        self.outputs = None
+
+    def assemble(self, outputs=None, stream=None):
+        if outputs is None:
+            if self.outputs is None:
+                self.outputs = [torch.empty((l, 3 * d.N, 3 * d.N), dtype=torch.float64, device="cuda")
+                                for d, l in zip(self.dmeshes, self.nlag)]
+            outputs = self.outputs
+        ptrs = (C.c_void_p * len(outputs))(*[o.data_ptr() for o in outputs])
+        _lib.check(_lib.load().ebem_batch_assemble(self._h, C.cast(ptrs, C.c_void_p), _stream_ptr(stream)))
+        return [o.view(l, 3 * d.N, 3 * d.N).transpose(1, 2) for o, d, l in zip(outputs, self.dmeshes, self.nlag)]
+
+    def info(self):
+        w, c, ms, pairs = C.c_int(), C.c_int(), C.c_float(), C.c_longlong()
+        _lib.check(_lib.load().ebem_batch_info(self._h, C.byref(w), C.byref(c), C.byref(ms), C.byref(pairs)))
+        return {"warps_per_block": w.value, "pairs_per_grab": c.value, "tuned_ms": ms.value, "pairs": pairs.value}
+
+    def close(self):
+        if self._h:
+            _lib.load().ebem_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -631,4 +631,175 @@ int ebem_assemble_sa_noalloc(const ebem_mesh* m, const ebem_problem* p, int n_gh
     return rc;
 }
 
+// ---------------------------------------------------------------------------
+// batched assembly plans
+
+}  // extern "C"
+
+struct ebem_batch {
+    int device = 0, n = 0, n_gh = 0, prec = 0;
+    std::vector<const ebem_mesh*> meshes;
+    std::vector<int> nlag;
+    BatchInst* h_insts = nullptr;          // pinned host copy of the table
+    BatchInst* d_insts = nullptr;
+    unsigned long long* d_next = nullptr;  // work counter, reset inside the graph
+    long long total = 0;
+    int wpb = 4, chunk = 4;
+    float tuned_ms = -1.0f;
+    bool tuned = false;
+    cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+int batch_run_direct(ebem_batch* b, int wpb, int chunk, cudaStream_t s) {
+    EBEM_CUDA_TRY(cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), s));
+    return launch_sa_batch(b->d_insts, b->n, b->total, b->n_gh, b->prec == EBEM_PREC_MIXED, wpb, chunk, b->d_next,
+                           b->device, s);
+}
+
+// Autotuner: time every (warps per block, pairs per grab) candidate once on the
+// batch itself and keep the fastest, then capture the launch in a CUDA graph.
+int batch_tune_and_capture(ebem_batch* b, cudaStream_t s) {
+    std::vector<int> wpbs = (3 * b->n_gh <= 32) ? std::vector<int>{2, 4} : std::vector<int>{2};
+    const int chunks[3] = {1, 4, 16};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    EBEM_CUDA_TRY(cudaEventCreate(&e0));
+    EBEM_CUDA_TRY(cudaEventCreate(&e1));
+    int rc = batch_run_direct(b, wpbs.back(), 4, s);          // warm-up (module load, caches)
+    float best = 1e30f;
+    for (int w : wpbs)
+        for (int c : chunks) {
+            if (rc) break;
+            cudaEventRecord(e0, s);
+            rc = batch_run_direct(b, w, c, s);
+            cudaEventRecord(e1, s);
+            if (!rc && cudaEventSynchronize(e1) == cudaSuccess) {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best) { best = ms; b->wpb = w; b->chunk = c; }
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    b->tuned_ms = best;
+    b->tuned = true;
+    if (!b->cap) EBEM_CUDA_TRY(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+    EBEM_CUDA_TRY(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    int crc = batch_run_direct(b, b->wpb, b->chunk, b->cap);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->cap, &g);
+    if (crc) { if (g) cudaGraphDestroy(g); return crc; }
+    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(e));
+    b->graph = g;
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("batch graph instantiation: ") + cudaGetErrorString(e));
+    return EBEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ebem_batch_destroy(ebem_batch* b) {
+    if (!b) return EBEM_OK;
+    DeviceGuard dg(b->device);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    if (b->d_insts) cudaFree(b->d_insts);
+    if (b->d_next) cudaFree(b->d_next);
+    if (b->h_insts) cudaFreeHost(b->h_insts);
+    delete b;
+    return EBEM_OK;
+}
+
+int ebem_batch_create(const ebem_mesh* const* meshes, const ebem_problem* probs, const int* nlag, int n, int n_gh,
+                      int prec, ebem_batch** out) {
+    if (!out) return fail(EBEM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!meshes || !probs || n < 1) return fail(EBEM_ERR_INVALID, "need at least one instance");
+    if (n_gh != 3 && n_gh != 7 && n_gh != 12 && n_gh != 19)
+        return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+    if (prec != EBEM_PREC_FP64 && prec != EBEM_PREC_MIXED) return fail(EBEM_ERR_INVALID, "unknown precision mode");
+    for (int k = 0; k < n; k++) {
+        if (!meshes[k]) return fail(EBEM_ERR_INVALID, "NULL mesh in the batch");
+        if (int rc = check_problem(&probs[k])) return rc;
+        if (meshes[k]->d.device != meshes[0]->d.device) return fail(EBEM_ERR_INVALID, "all meshes of a batch must live on one device");
+    }
+    ebem_batch* b = new ebem_batch();
+    b->device = meshes[0]->d.device;
+    b->n = n;
+    b->n_gh = n_gh;
+    b->prec = prec;
+    DeviceGuard dg(b->device);
+    auto bail = [&](int rc) { ebem_batch_destroy(b); return rc; };
+    if (cudaMallocHost(&b->h_insts, sizeof(BatchInst) * n) != cudaSuccess ||
+        cudaMalloc(&b->d_insts, sizeof(BatchInst) * n) != cudaSuccess ||
+        cudaMalloc(&b->d_next, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(fail(EBEM_ERR_NOMEM, "batch table allocation failed"));
+    }
+    long long begin = 0;
+    for (int k = 0; k < n; k++) {
+        MeshData& md = const_cast<MeshData&>(meshes[k]->d);
+        int L = 0;
+        if (int rc = ebem_num_blocks(meshes[k], &probs[k], &L)) return bail(rc);
+        const int nl = nlag ? nlag[k] : L;
+        if (nl < 1) return bail(fail(EBEM_ERR_INVALID, "each instance needs nlag >= 1"));
+        if (int rc = map_nodes(md, n_gh, 0)) return bail(rc);
+        PhysParams P = phys_from(&probs[k]);
+        BatchInst& I = b->h_insts[k];
+        I.geo = md.d_geo;
+        I.nodes = md.d_nodes;
+        I.E = nullptr;
+        I.N = md.nt;
+        I.nlag = nl;
+        I.velP = P.velP;
+        I.velS = P.velS;
+        I.dt = P.dt;
+        I.c4pirho = 4 * kPi * P.rho;
+        I.pair_begin = begin;
+        begin += (long long)md.nt * md.nt;
+        b->meshes.push_back(meshes[k]);
+        b->nlag.push_back(nl);
+    }
+    b->total = begin;
+    *out = b;
+    return EBEM_OK;
+}
+
+int ebem_batch_assemble(ebem_batch* b, double* const* E, void* stream) {
+    if (!b || !E) return fail(EBEM_ERR_INVALID, "NULL batch or outputs");
+    DeviceGuard dg(b->device);
+    for (int k = 0; k < b->n; k++) {
+        if (!E[k] || !is_device_ptr(E[k])) return fail(EBEM_ERR_INVALID, "batch outputs must be device buffers");
+        b->h_insts[k].E = E[k];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    // the table (output pointers) is read by the kernel at run time, so a new
+    // set of outputs needs no new graph
+    EBEM_CUDA_TRY(cudaMemcpyAsync(b->d_insts, b->h_insts, sizeof(BatchInst) * b->n, cudaMemcpyHostToDevice, s));
+    if (!b->tuned) {
+        if (int rc = batch_tune_and_capture(b, s)) return rc;
+    }
+    EBEM_CUDA_TRY(cudaGraphLaunch(b->exec, s));
+    // the pinned table must not change before this call's copy has run
+    EBEM_CUDA_TRY(cudaStreamSynchronize(s));
+    return EBEM_OK;
+}
+
+int ebem_batch_info(const ebem_batch* b, int* warps_per_block, int* pairs_per_grab, float* tuned_ms,
+                    long long* pairs) {
+    if (!b) return fail(EBEM_ERR_INVALID, "batch is NULL");
+    if (warps_per_block) *warps_per_block = b->wpb;
+    if (pairs_per_grab) *pairs_per_grab = b->chunk;
+    if (tuned_ms) *tuned_ms = b->tuned_ms;
+    if (pairs) *pairs = b->total;
+    return EBEM_OK;
+}
+
 }  // extern "C"

@@ -69,6 +69,19 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
 int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, double* d_E,
                                int accumulate, bool count, unsigned long long* host_count, cudaStream_t s);
 size_t noalloc_max_nodes();
+
+// One instance of a batched assembly (device table entry).
+struct BatchInst {
+    const TriGeom* geo;
+    const NodeW* nodes;
+    double* E;              // 9 N^2 nlag doubles, lags 0..nlag-1
+    int N, nlag;
+    double velP, velS, dt, c4pirho;
+    long long pair_begin;   // first index of this instance in the concatenated pair space
+};
+// Persistent batched assembly over all instances; d_next must be zero.
+int launch_sa_batch(const BatchInst* d_insts, int ninst, long long total, int n_gh, int mixed, int wpb, int chunk,
+                    unsigned long long* d_next, int device, cudaStream_t s);
 int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_sub, int n_sing, int lag0, int nlag,
                         double* d_E, size_t ld, size_t ld_lag, cudaStream_t s);
 

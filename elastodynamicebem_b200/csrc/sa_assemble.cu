@@ -200,6 +200,240 @@ __device__ __forceinline__ void store_entry(const SAArgs& A, int q, int i, int j
     else *dst = v;
 }
 
+// The whole time-level walk of one (source i, field j) pair by one warp.
+template <int R, bool MIXED>
+__device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W, const double* glx, const double* glw,
+                                              int i, int j, int lane, unsigned long long& my_count) {
+    const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    const TriGeom& F = A.geo[j];
+    const TriGeom& Sg = A.geo[i];
+    double v0 = F.ctr[0] - Sg.ctr[0], v1 = F.ctr[1] - Sg.ctr[1], v2 = F.ctr[2] - Sg.ctr[2];
+    double d = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+    double distMin = d - F.maxL - Sg.maxL;
+    double distMax = d + F.maxL + Sg.maxL;
+    int llo = -1, lhi = -2;
+    for (int q = 0; q < A.nlag; q++) {
+        int l = A.lag0 + q;
+        if (lag_nonnull(l, A.velP, A.velS, A.dt, distMin, distMax)) {
+            if (llo < 0) llo = l;
+            lhi = l;
+        }
+    }
+    if (lane == 0 && llo >= 0) my_count += (unsigned long long)(lhi - llo + 1);
+    if (!A.accumulate) {
+        for (int idx = lane; idx < A.nlag * 9; idx += 32) {
+            const int q = idx / 9, e = idx - 9 * q, l = A.lag0 + q;
+            if (llo < 0 || l < llo || l > lhi) store_entry(A, q, i, j, e, 0.0);
+        }
+    }
+    if (llo < 0) return;
+    // slot u of this lane = child c of outer node g, slot = lane + 32 u = 3 g + c
+    LaneChild C[R];
+    bool hasmom[R];
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+        const int slot = lane + 32 * u;
+        LaneChild& Cu = C[u];
+        Cu.live = false;
+        Cu.zeta = 0.0; Cu.sigma = 0.0; Cu.dMIN = 0.0; Cu.w = 0.0;
+        hasmom[u] = false;
+        const int g = slot / 3, c = slot - 3 * (slot / 3);
+        if (g < A.n_gh) {
+            NodeW sp = A.nodes[(size_t)i * A.n_gh + g];
+            NodeGeo G;
+            node_geo(G, sp, F);
+            Cu.zeta = G.zeta;
+            Cu.sigma = G.sigma;
+            Cu.dMIN = G.dMIN;
+            Cu.w = sp.w;
+            if (node_child_e(Cu.g, G, c)) {
+                Cu.live = true;
+                m_sincos(Cu.g.gamma, &Cu.sg, &Cu.cg);
+            }
+        }
+        if (Cu.live) {
+            const ChildE& gg = Cu.g;
+            W.F[slot] = gg.F;
+            W.cbp[slot] = gg.cb * gg.ct + gg.sb * gg.st;     // cos(beta - theta_V1)
+            W.sbp[slot] = gg.sb * gg.ct - gg.cb * gg.st;     // sin(beta - theta_V1)
+            W.zeta[slot] = Cu.zeta;
+            W.zs[slot] = Cu.zeta * Cu.sigma;
+            W.scale[slot] = Cu.w * gg.sgnC;
+            if (MIXED) {
+                W.Ff[slot] = (float)W.F[slot];
+                W.cbpf[slot] = (float)W.cbp[slot];
+                W.sbpf[slot] = (float)W.sbp[slot];
+                W.zetaf[slot] = (float)W.zeta[slot];
+                W.zsf[slot] = (float)W.zs[slot];
+                W.scalef[slot] = (float)W.scale[slot];
+            }
+        }
+    }
+    __syncwarp();
+    const int klo = max(1, llo - 1), khi = lhi + 1;
+    double Fm2[6] = {0, 0, 0, 0, 0, 0}, Fm1[6] = {0, 0, 0, 0, 0, 0}, Fk[6];
+    const double vp2 = A.velP * A.velP, vs2 = A.velS * A.velS, den = vp2 * vs2;
+    for (int k = klo; k <= khi; k++) {
+        const double t = k * A.dt;
+        LevelCtx L;
+        L.t2 = t * t;
+        L.RP = A.velP * t;
+        L.RS = A.velS * t;
+        L.k1 = 1.0 / vp2;
+        L.k5 = (vp2 + vs2) / den;
+        L.k6 = (vp2 - vs2) / den;
+        double S = 0.0, T[6] = {0, 0, 0, 0, 0, 0};
+        Piece pc[R][3];
+        int np[R], nsubs[R][3];
+        double hs[R][3];
+        int nn = 0, npl = 0;
+#pragma unroll
+        for (int u = 0; u < R; u++) {
+            const int slot = lane + 32 * u;
+            const LaneChild& Cu = C[u];
+            // decision phase (per child)
+            int type = T_NONE;
+            double rhoP = -1.0, rhoS = -1.0;
+            if (Cu.live) type = classify(Cu.zeta, L.RP, L.RS, Cu.dMIN, rhoP, rhoS);
+            AccE Ac = {0, 0, 0, 0, 0, 0, 0};
+            int full = 0;
+            np[u] = 0;
+            if (type != T_NONE) child_decide(Ac, pc[u], np[u], full, Cu, L, rhoP, rhoS, type);
+            // whole-range moments, computed by the whole warp once per child
+            const bool need = full && !hasmom[u];
+            unsigned mm = __ballot_sync(0xffffffffu, need);
+            while (mm) {
+                const int b = __ffs(mm) - 1;
+                mm &= mm - 1;
+                const double Fb = __shfl_sync(0xffffffffu, Cu.g.F, b), cbb = __shfl_sync(0xffffffffu, Cu.g.cb, b);
+                const double sbb = __shfl_sync(0xffffffffu, Cu.g.sb, b), zb = __shfl_sync(0xffffffffu, Cu.zeta, b);
+                const double s1b = __shfl_sync(0xffffffffu, Cu.g.s1, b), s0b = __shfl_sync(0xffffffffu, Cu.g.s0, b);
+                double m[14];
+                moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx, glw);
+#pragma unroll
+                for (int e = 0; e < 14; e++) m[e] = warp_sum(m[e]);
+                if (lane == b) {
+#pragma unroll
+                    for (int e = 0; e < 14; e++) W.mom[e][slot] = m[e];
+                }
+            }
+            if (need) hasmom[u] = true;
+            const double zs = Cu.zeta * Cu.sigma;
+            if (full & 1) apply_moments(Ac, W, slot, true, L, zs);
+            if (full & 2) apply_moments(Ac, W, slot, false, L, zs);
+            if (type != T_NONE) child_to_plane(S, T, Ac, Cu.g, Cu.w * Cu.g.sgnC);
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                if (q < np[u]) {
+                    double len = pc[u][q].shi - pc[u][q].slo;
+                    int ns = (int)ceil(len * (1.0 / EBEM_EDGE_H));
+                    ns = max(1, min(ns, 4096));
+                    nsubs[u][q] = ns;
+                    hs[u][q] = len / ns;
+                    nn += 10 * ns;
+                }
+            }
+            npl += np[u];
+        }
+        // partial edge pieces of all children -> per-warp list
+        int totp, totn;
+        int pb = warp_excl_scan(npl, lane, totp);
+        int o = warp_excl_scan(nn, lane, totn);
+#pragma unroll
+        for (int u = 0; u < R; u++) {
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                if (q < np[u]) {
+                    W.slo[pb] = pc[u][q].slo;
+                    W.h[pb] = hs[u][q];
+                    W.off[pb] = o;
+                    W.who[pb] = (lane + 32 * u) | (pc[u][q].pterm ? 64 : 0);
+                    o += 10 * nsubs[u][q];
+                    pb++;
+                }
+            }
+        }
+        if (lane == 31) W.off[totp] = totn;
+        __syncwarp();
+        // all lanes: Gauss-Legendre nodes of the list, plane frame
+        int pp = 0;
+        if (MIXED) {
+            float Sf = 0.0f, Tf[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+            const float k1 = (float)L.k1, t2 = (float)L.t2, k5 = (float)L.k5, k6 = (float)L.k6;
+            for (int idx = lane; idx < totn; idx += 32) {
+                while (idx >= W.off[pp + 1]) pp++;
+                const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
+                const double h = W.h[pp];
+                const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
+                const int who = W.who[pp], cl = who & 63;
+                edge_node_f32(Sf, Tf, s, (float)(0.5 * h * glw[q]), W.Ff[cl], W.cbpf[cl], W.sbpf[cl], W.zetaf[cl],
+                              W.zsf[cl], W.scalef[cl], (who & 64) != 0, k1, t2, k5, k6);
+            }
+            // per-lane FP32 partial sums join the FP64 lane sums reduced below
+            S += (double)Sf;
+#pragma unroll
+            for (int e = 0; e < 6; e++) T[e] += (double)Tf[e];
+            totn = 0;    // the FP64 loop below has nothing left to do
+        }
+        for (int idx = lane; idx < totn; idx += 32) {
+            while (idx >= W.off[pp + 1]) pp++;
+            const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
+            const double h = W.h[pp];
+            const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
+            const int who = W.who[pp], cl = who & 63;
+            double ch, sech, th;
+            hyp(s, ch, sech, th);
+            const double cbq = W.cbp[cl], sbq = W.sbp[cl];
+            const double cq = th * cbq + sech * sbq, sq = sech * cbq - th * sbq;
+            Rad v = radial_edge(W.F[cl] * ch, W.zeta[cl]);
+            W4 w = weigh(v, (who & 64) != 0, L);
+            const double f = 0.5 * h * glw[q] * sech * W.scale[cl];
+            const double fin = f * w.in, fmx = -W.zs[cl] * f * w.mx;
+            S += f * w.sc;
+            T[0] += fin * cq * cq;
+            T[1] += fin * sq * cq;
+            T[2] += fin * sq * sq;
+            T[3] += fmx * cq;
+            T[4] += fmx * sq;
+            T[5] += f * w.zz;
+        }
+        __syncwarp();
+        S = warp_sum(S);
+#pragma unroll
+        for (int e = 0; e < 6; e++) T[e] = warp_sum(T[e]);
+        // F(t_k) = (S I + C^T M C) / 2 in global axes
+        {
+            double M[3][3] = {{T[0], T[1], T[3]}, {T[1], T[2], T[4]}, {T[3], T[4], T[5]}};
+            const double* Cm = F.C;
+            double MC[3][3];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) MC[r][c] = M[r][0] * Cm[c] + M[r][1] * Cm[3 + c] + M[r][2] * Cm[6 + c];
+            double Rm[3][3];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = r; c < 3; c++) Rm[r][c] = Cm[r] * MC[0][c] + Cm[3 + r] * MC[1][c] + Cm[6 + r] * MC[2][c];
+            Fk[0] = 0.5 * (S + Rm[0][0]);
+            Fk[1] = 0.5 * Rm[0][1];
+            Fk[2] = 0.5 * Rm[0][2];
+            Fk[3] = 0.5 * (S + Rm[1][1]);
+            Fk[4] = 0.5 * Rm[1][2];
+            Fk[5] = 0.5 * (S + Rm[2][2]);
+        }
+        const int l = k - 1;
+        if (l >= llo && l <= lhi && lane < 9) {
+            const int e = map[lane];
+            double prev = (l - 1 >= 1) ? Fm2[e] : 0.0;
+            double v = ((Fk[e] + (-2.0) * Fm1[e]) + prev) / A.c4pirho;
+            store_entry(A, l - A.lag0, i, j, lane, (fabs(v) < 1.0e-14) ? 0.0 : v);
+        }
+#pragma unroll
+        for (int e = 0; e < 6; e++) { Fm2[e] = Fm1[e]; Fm1[e] = Fk[e]; }
+    }
+}
+
 // One warp per pair (schedule described in sa_warp.cuh); R children per lane
 // (3 n_gh <= 32 R), WPB warps per block.
 #ifndef EBEM_WARP_MINB
@@ -221,7 +455,6 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs
     __syncthreads();
     const long long NP = A.pairs ? A.npairs : A.diag_only ? (long long)A.nsrc : (long long)A.nsrc * A.N;
     const long long nwarps = (long long)gridDim.x * WPB;
-    const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
     unsigned long long my_count = 0;
     for (long long p = (long long)blockIdx.x * WPB + wib; p < NP; p += nwarps) {
         int i, j;
@@ -233,233 +466,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs
             i = A.src0 + (int)(p % A.nsrc);
             j = A.diag_only ? i : (int)(p / A.nsrc);
         }
-        const TriGeom& F = A.geo[j];
-        const TriGeom& Sg = A.geo[i];
-        double v0 = F.ctr[0] - Sg.ctr[0], v1 = F.ctr[1] - Sg.ctr[1], v2 = F.ctr[2] - Sg.ctr[2];
-        double d = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-        double distMin = d - F.maxL - Sg.maxL;
-        double distMax = d + F.maxL + Sg.maxL;
-        int llo = -1, lhi = -2;
-        for (int q = 0; q < A.nlag; q++) {
-            int l = A.lag0 + q;
-            if (lag_nonnull(l, A.velP, A.velS, A.dt, distMin, distMax)) {
-                if (llo < 0) llo = l;
-                lhi = l;
-            }
-        }
-        if (lane == 0 && llo >= 0) my_count += (unsigned long long)(lhi - llo + 1);
-        if (!A.accumulate) {
-            for (int idx = lane; idx < A.nlag * 9; idx += 32) {
-                const int q = idx / 9, e = idx - 9 * q, l = A.lag0 + q;
-                if (llo < 0 || l < llo || l > lhi) store_entry(A, q, i, j, e, 0.0);
-            }
-        }
-        if (llo < 0) continue;
-        // slot u of this lane = child c of outer node g, slot = lane + 32 u = 3 g + c
-        LaneChild C[R];
-        bool hasmom[R];
-#pragma unroll
-        for (int u = 0; u < R; u++) {
-            const int slot = lane + 32 * u;
-            LaneChild& Cu = C[u];
-            Cu.live = false;
-            Cu.zeta = 0.0; Cu.sigma = 0.0; Cu.dMIN = 0.0; Cu.w = 0.0;
-            hasmom[u] = false;
-            const int g = slot / 3, c = slot - 3 * (slot / 3);
-            if (g < A.n_gh) {
-                NodeW sp = A.nodes[(size_t)i * A.n_gh + g];
-                NodeGeo G;
-                node_geo(G, sp, F);
-                Cu.zeta = G.zeta;
-                Cu.sigma = G.sigma;
-                Cu.dMIN = G.dMIN;
-                Cu.w = sp.w;
-                if (node_child_e(Cu.g, G, c)) {
-                    Cu.live = true;
-                    m_sincos(Cu.g.gamma, &Cu.sg, &Cu.cg);
-                }
-            }
-            if (Cu.live) {
-                const ChildE& gg = Cu.g;
-                W.F[slot] = gg.F;
-                W.cbp[slot] = gg.cb * gg.ct + gg.sb * gg.st;     // cos(beta - theta_V1)
-                W.sbp[slot] = gg.sb * gg.ct - gg.cb * gg.st;     // sin(beta - theta_V1)
-                W.zeta[slot] = Cu.zeta;
-                W.zs[slot] = Cu.zeta * Cu.sigma;
-                W.scale[slot] = Cu.w * gg.sgnC;
-                if (MIXED) {
-                    W.Ff[slot] = (float)W.F[slot];
-                    W.cbpf[slot] = (float)W.cbp[slot];
-                    W.sbpf[slot] = (float)W.sbp[slot];
-                    W.zetaf[slot] = (float)W.zeta[slot];
-                    W.zsf[slot] = (float)W.zs[slot];
-                    W.scalef[slot] = (float)W.scale[slot];
-                }
-            }
-        }
-        __syncwarp();
-        const int klo = max(1, llo - 1), khi = lhi + 1;
-        double Fm2[6] = {0, 0, 0, 0, 0, 0}, Fm1[6] = {0, 0, 0, 0, 0, 0}, Fk[6];
-        const double vp2 = A.velP * A.velP, vs2 = A.velS * A.velS, den = vp2 * vs2;
-        for (int k = klo; k <= khi; k++) {
-            const double t = k * A.dt;
-            LevelCtx L;
-            L.t2 = t * t;
-            L.RP = A.velP * t;
-            L.RS = A.velS * t;
-            L.k1 = 1.0 / vp2;
-            L.k5 = (vp2 + vs2) / den;
-            L.k6 = (vp2 - vs2) / den;
-            double S = 0.0, T[6] = {0, 0, 0, 0, 0, 0};
-            Piece pc[R][3];
-            int np[R], nsubs[R][3];
-            double hs[R][3];
-            int nn = 0, npl = 0;
-#pragma unroll
-            for (int u = 0; u < R; u++) {
-                const int slot = lane + 32 * u;
-                const LaneChild& Cu = C[u];
-                // decision phase (per child)
-                int type = T_NONE;
-                double rhoP = -1.0, rhoS = -1.0;
-                if (Cu.live) type = classify(Cu.zeta, L.RP, L.RS, Cu.dMIN, rhoP, rhoS);
-                AccE Ac = {0, 0, 0, 0, 0, 0, 0};
-                int full = 0;
-                np[u] = 0;
-                if (type != T_NONE) child_decide(Ac, pc[u], np[u], full, Cu, L, rhoP, rhoS, type);
-                // whole-range moments, computed by the whole warp once per child
-                const bool need = full && !hasmom[u];
-                unsigned mm = __ballot_sync(0xffffffffu, need);
-                while (mm) {
-                    const int b = __ffs(mm) - 1;
-                    mm &= mm - 1;
-                    const double Fb = __shfl_sync(0xffffffffu, Cu.g.F, b), cbb = __shfl_sync(0xffffffffu, Cu.g.cb, b);
-                    const double sbb = __shfl_sync(0xffffffffu, Cu.g.sb, b), zb = __shfl_sync(0xffffffffu, Cu.zeta, b);
-                    const double s1b = __shfl_sync(0xffffffffu, Cu.g.s1, b), s0b = __shfl_sync(0xffffffffu, Cu.g.s0, b);
-                    double m[14];
-                    moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx, glw);
-#pragma unroll
-                    for (int e = 0; e < 14; e++) m[e] = warp_sum(m[e]);
-                    if (lane == b) {
-#pragma unroll
-                        for (int e = 0; e < 14; e++) W.mom[e][slot] = m[e];
-                    }
-                }
-                if (need) hasmom[u] = true;
-                const double zs = Cu.zeta * Cu.sigma;
-                if (full & 1) apply_moments(Ac, W, slot, true, L, zs);
-                if (full & 2) apply_moments(Ac, W, slot, false, L, zs);
-                if (type != T_NONE) child_to_plane(S, T, Ac, Cu.g, Cu.w * Cu.g.sgnC);
-#pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    if (q < np[u]) {
-                        double len = pc[u][q].shi - pc[u][q].slo;
-                        int ns = (int)ceil(len * (1.0 / EBEM_EDGE_H));
-                        ns = max(1, min(ns, 4096));
-                        nsubs[u][q] = ns;
-                        hs[u][q] = len / ns;
-                        nn += 10 * ns;
-                    }
-                }
-                npl += np[u];
-            }
-            // partial edge pieces of all children -> per-warp list
-            int totp, totn;
-            int pb = warp_excl_scan(npl, lane, totp);
-            int o = warp_excl_scan(nn, lane, totn);
-#pragma unroll
-            for (int u = 0; u < R; u++) {
-#pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    if (q < np[u]) {
-                        W.slo[pb] = pc[u][q].slo;
-                        W.h[pb] = hs[u][q];
-                        W.off[pb] = o;
-                        W.who[pb] = (lane + 32 * u) | (pc[u][q].pterm ? 64 : 0);
-                        o += 10 * nsubs[u][q];
-                        pb++;
-                    }
-                }
-            }
-            if (lane == 31) W.off[totp] = totn;
-            __syncwarp();
-            // all lanes: Gauss-Legendre nodes of the list, plane frame
-            int pp = 0;
-            if (MIXED) {
-                float Sf = 0.0f, Tf[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-                const float k1 = (float)L.k1, t2 = (float)L.t2, k5 = (float)L.k5, k6 = (float)L.k6;
-                for (int idx = lane; idx < totn; idx += 32) {
-                    while (idx >= W.off[pp + 1]) pp++;
-                    const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
-                    const double h = W.h[pp];
-                    const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
-                    const int who = W.who[pp], cl = who & 63;
-                    edge_node_f32(Sf, Tf, s, (float)(0.5 * h * glw[q]), W.Ff[cl], W.cbpf[cl], W.sbpf[cl], W.zetaf[cl],
-                                  W.zsf[cl], W.scalef[cl], (who & 64) != 0, k1, t2, k5, k6);
-                }
-                // per-lane FP32 partial sums join the FP64 lane sums reduced below
-                S += (double)Sf;
-#pragma unroll
-                for (int e = 0; e < 6; e++) T[e] += (double)Tf[e];
-                totn = 0;    // the FP64 loop below has nothing left to do
-            }
-            for (int idx = lane; idx < totn; idx += 32) {
-                while (idx >= W.off[pp + 1]) pp++;
-                const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
-                const double h = W.h[pp];
-                const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
-                const int who = W.who[pp], cl = who & 63;
-                double ch, sech, th;
-                hyp(s, ch, sech, th);
-                const double cbq = W.cbp[cl], sbq = W.sbp[cl];
-                const double cq = th * cbq + sech * sbq, sq = sech * cbq - th * sbq;
-                Rad v = radial_edge(W.F[cl] * ch, W.zeta[cl]);
-                W4 w = weigh(v, (who & 64) != 0, L);
-                const double f = 0.5 * h * glw[q] * sech * W.scale[cl];
-                const double fin = f * w.in, fmx = -W.zs[cl] * f * w.mx;
-                S += f * w.sc;
-                T[0] += fin * cq * cq;
-                T[1] += fin * sq * cq;
-                T[2] += fin * sq * sq;
-                T[3] += fmx * cq;
-                T[4] += fmx * sq;
-                T[5] += f * w.zz;
-            }
-            __syncwarp();
-            S = warp_sum(S);
-#pragma unroll
-            for (int e = 0; e < 6; e++) T[e] = warp_sum(T[e]);
-            // F(t_k) = (S I + C^T M C) / 2 in global axes
-            {
-                double M[3][3] = {{T[0], T[1], T[3]}, {T[1], T[2], T[4]}, {T[3], T[4], T[5]}};
-                const double* Cm = F.C;
-                double MC[3][3];
-#pragma unroll
-                for (int r = 0; r < 3; r++)
-#pragma unroll
-                    for (int c = 0; c < 3; c++) MC[r][c] = M[r][0] * Cm[c] + M[r][1] * Cm[3 + c] + M[r][2] * Cm[6 + c];
-                double Rm[3][3];
-#pragma unroll
-                for (int r = 0; r < 3; r++)
-#pragma unroll
-                    for (int c = r; c < 3; c++) Rm[r][c] = Cm[r] * MC[0][c] + Cm[3 + r] * MC[1][c] + Cm[6 + r] * MC[2][c];
-                Fk[0] = 0.5 * (S + Rm[0][0]);
-                Fk[1] = 0.5 * Rm[0][1];
-                Fk[2] = 0.5 * Rm[0][2];
-                Fk[3] = 0.5 * (S + Rm[1][1]);
-                Fk[4] = 0.5 * Rm[1][2];
-                Fk[5] = 0.5 * (S + Rm[2][2]);
-            }
-            const int l = k - 1;
-            if (l >= llo && l <= lhi && lane < 9) {
-                const int e = map[lane];
-                double prev = (l - 1 >= 1) ? Fm2[e] : 0.0;
-                double v = ((Fk[e] + (-2.0) * Fm1[e]) + prev) / A.c4pirho;
-                store_entry(A, l - A.lag0, i, j, lane, (fabs(v) < 1.0e-14) ? 0.0 : v);
-            }
-#pragma unroll
-            for (int e = 0; e < 6; e++) { Fm2[e] = Fm1[e]; Fm1[e] = Fk[e]; }
-        }
+        assemble_pair<R, MIXED>(A, W, glx, glw, i, j, lane, my_count);
     }
     if (A.count) {
         if (lane == 0 && my_count) atomicAdd(&blk_count, my_count);
@@ -634,6 +641,95 @@ int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh,
         EBEM_CUDA_TRY(cudaStreamSynchronize(s));
     }
     return EBEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched assembly: many meshes (instances) in one persistent launch.  Each
+// warp grabs `chunk` consecutive pairs of the concatenated pair space
+// (instance b owns pairs [pair_begin[b], pair_begin[b] + N_b^2)) from a global
+// counter and assembles them with the same per-pair walk as the single-mesh
+// kernel, so a batch result equals the single-mesh results to rounding.
+
+template <int R, int WPB, int MINB, bool MIXED>
+__global__ void __launch_bounds__(32 * WPB, MINB)
+sa_batch_kernel(const BatchInst* __restrict__ insts, int ninst, long long total, int n_gh, int chunk,
+                unsigned long long* next) {
+    __shared__ WarpShared<R> Wsh[WPB];
+    __shared__ double glx[10], glw[10];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    WarpShared<R>& W = Wsh[wib];
+    if (threadIdx.x < 10) {
+        const int k = threadIdx.x < 5 ? threadIdx.x : threadIdx.x - 5;
+        glx[threadIdx.x] = (threadIdx.x < 5 ? -1.0 : 1.0) * gl_x(k);
+        glw[threadIdx.x] = gl_w(k);
+    }
+    __syncthreads();
+    unsigned long long unused = 0;
+    while (true) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(next, (unsigned long long)chunk);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if ((long long)base >= total) break;
+        const long long end = min((long long)base + chunk, total);
+        for (long long p = (long long)base; p < end; p++) {
+            int lo = 0, hi = ninst - 1;                 // last instance with pair_begin <= p
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (insts[mid].pair_begin <= p) lo = mid;
+                else hi = mid - 1;
+            }
+            const BatchInst& I = insts[lo];
+            SAArgs A;
+            A.geo = I.geo;
+            A.nodes = I.nodes;
+            A.N = I.N;
+            A.n_gh = n_gh;
+            A.velP = I.velP;
+            A.velS = I.velS;
+            A.dt = I.dt;
+            A.c4pirho = I.c4pirho;
+            A.lag0 = 0;
+            A.nlag = I.nlag;
+            A.src0 = 0;
+            A.nsrc = I.N;
+            A.diag_only = 0;
+            A.E = I.E;
+            A.ld = 3 * (size_t)I.N;
+            A.ld_lag = A.ld * A.ld;
+            A.accumulate = 0;
+            A.count = nullptr;
+            A.pairs = nullptr;
+            A.npairs = 0;
+            const long long q = p - I.pair_begin;
+            assemble_pair<R, MIXED>(A, W, glx, glw, (int)(q % I.N), (int)(q / I.N), lane, unused);
+        }
+    }
+}
+
+template <int R, int WPB, int MINB, bool MIXED>
+static int launch_batch_t(const BatchInst* d_insts, int ninst, long long total, int n_gh, int chunk,
+                          unsigned long long* d_next, int device, cudaStream_t s) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const unsigned blocks = (unsigned)(sms * MINB);       // one resident wave: persistent
+    sa_batch_kernel<R, WPB, MINB, MIXED><<<blocks, 32 * WPB, 0, s>>>(d_insts, ninst, total, n_gh, chunk, d_next);
+    EBEM_CUDA_TRY(cudaGetLastError());
+    return EBEM_OK;
+}
+
+int launch_sa_batch(const BatchInst* d_insts, int ninst, long long total, int n_gh, int mixed, int wpb, int chunk,
+                    unsigned long long* d_next, int device, cudaStream_t s) {
+    if (3 * n_gh <= 32) {
+        if (wpb == 2)
+            return mixed ? launch_batch_t<1, 2, 8, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
+                         : launch_batch_t<1, 2, 8, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
+        return mixed ? launch_batch_t<1, 4, 4, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
+                     : launch_batch_t<1, 4, 4, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
+    }
+    if (3 * n_gh <= 64)
+        return mixed ? launch_batch_t<2, 2, 4, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
+                     : launch_batch_t<2, 2, 4, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
+    return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
 }
 
 }  // namespace ebem

@@ -50,6 +50,12 @@ PROTOTYPES = {
                              C.c_void_p, C.c_void_p]),
     "ebem_assemble_sa_noalloc": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_int, C.c_void_p,
                                            C.c_int, C.c_void_p, C.POINTER(C.c_longlong)]),
+    "ebem_batch_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                    C.POINTER(C.c_void_p)]),
+    "ebem_batch_assemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ebem_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
+                                  C.POINTER(C.c_longlong)]),
+    "ebem_batch_destroy": (C.c_int, [C.c_void_p]),
     "ebem_assemble_sa_ex": (C.c_int, [C.c_void_p, C.POINTER(ProblemC)] + [C.c_int] * 5 + [C.c_void_p, C.c_longlong,
                                       C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_longlong)]),
     "ebem_timemarch_sa_ex": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_int, C.c_void_p,

@@ -143,3 +143,31 @@ def bar_workload(h: float = 0.1) -> Workload:
     pts = np.column_stack([rng.uniform(0, 1, 512), rng.uniform(0, 1, 512), rng.uniform(0, 3, 512)])
     times = prm.dt * np.arange(1, prm.nT + 1)
     return Workload(f"bar_n{m.numberTriangles}", m, prm, 7, DATUM_BAR_H3, pts, times)
+
+
+# ---------------------------------------------------------------------------
+# batched instances
+
+def batch_workload(count: int = 64, seed: int = 4, n_min: int = 128, n_max: int = 2048):
+    """Independent screen / sphere instances of uneven size: type alternating
+    (screen, sphere), N log-uniform in [n_min, n_max] rounded to the nearest
+    generator size (screen 2 n^2, icosphere 20 4^k), dt uniform in
+    [0.02, 0.08] rounded to nT = round(1/dt) steps of T = 1, rho = mu = 1,
+    lambda = mu U[0.5, 3].  Returns a list of (name, mesh, params)."""
+    rng = np.random.default_rng(seed)
+    spheres = [k for k in range(0, 6) if n_min <= 20 * 4 ** k <= n_max]
+    out = []
+    for c in range(count):
+        target = math.exp(rng.uniform(math.log(n_min), math.log(n_max)))
+        nT = max(1, int(round(1.0 / rng.uniform(0.02, 0.08))))
+        lam = float(rng.uniform(0.5, 3.0))
+        if c % 2 == 0 or not spheres:
+            n = max(2, int(round(math.sqrt(target / 2))))
+            m = _mesh.screen_uniform(n)
+            name = f"screen_n{m.numberTriangles}"
+        else:
+            k = min(spheres, key=lambda k: abs(math.log(20 * 4 ** k / target)))
+            m = _mesh.icosphere(k)
+            name = f"sphere_n{m.numberTriangles}"
+        out.append((name, m, ProblemParams(1.0, 1.0, lam, 1.0, nT)))
+    return out

@@ -147,6 +147,28 @@ int ebem_assemble_sa_panel(const ebem_mesh* mesh, const ebem_problem* prob, int 
 int ebem_assemble_sa_noalloc(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag,
                              double* E, int accumulate, void* stream, long long* nonnull);
 
+/* Batched assembly of many instances (meshes with their own problem data and
+ * lag counts) in one persistent, graph-captured launch.  No counterpart in
+ * the reference (it assembles one mesh per run, BEMenerg_coreSA_timeMarching.m).
+ * Every warp takes a few pairs at a time from a global counter across all
+ * instances, so small and large meshes share the GPU without tail effects.
+ * ebem_batch_create records the instances (nlag may be NULL: L of each
+ * instance; instance k assembles lags 0..nlag[k]-1) with one outer rule and
+ * precision mode.  The first ebem_batch_assemble tunes the tile shape (warps
+ * per block x pairs per grab, each candidate timed once on the batch) and
+ * captures the launch in a CUDA graph; every call replays the graph.  E[k]:
+ * device buffer of 9 N_k^2 nlag[k] doubles, same layout as ebem_assemble_sa,
+ * every entry written; results equal ebem_assemble_sa's to rounding (the
+ * same per-pair computation in another kernel).
+ * ebem_batch_info reports the chosen shape, its tuning time and the pair count. */
+typedef struct ebem_batch ebem_batch;
+int ebem_batch_create(const ebem_mesh* const* meshes, const ebem_problem* probs, const int* nlag, int n, int n_gh,
+                      int prec, ebem_batch** out);
+int ebem_batch_assemble(ebem_batch* batch, double* const* E, void* stream);
+int ebem_batch_info(const ebem_batch* batch, int* warps_per_block, int* pairs_per_grab, float* tuned_ms,
+                    long long* pairs);
+int ebem_batch_destroy(ebem_batch* batch);
+
 /* ebem_assemble_sa_panel with a precision mode. */
 int ebem_assemble_sa_ex(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag, int src0,
                         int nsrc, double* E, long long ld, int accumulate, int prec, void* stream, long long* nonnull);
