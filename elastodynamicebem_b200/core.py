@@ -355,3 +355,80 @@ class BatchPlan:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# learned quadrature selector
+
+SELECTOR_RULES = (3, 7, 12, 19)
+SELECTOR_PARAMS = 5252
+
+
+def selector_init(seed: int = 0) -> torch.Tensor:
+    """He-initialised MLP parameters (device, float32)."""
+    p = torch.empty(SELECTOR_PARAMS, dtype=torch.float32, device="cuda")
+    _lib.check(_lib.load().ebem_selector_init(C.c_void_p(p.data_ptr()), int(seed)))
+    return p
+
+
+def selector_features(dmesh: DeviceMesh, prm: ProblemParams, stream=None) -> torch.Tensor:
+    f = torch.empty((dmesh.N * dmesh.N, 12), dtype=torch.float32, device="cuda")
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_selector_features(dmesh.handle, C.byref(p), C.c_void_p(f.data_ptr()),
+                                                  _stream_ptr(stream)))
+    return f
+
+
+def selector_labels(dmesh: DeviceMesh, prm: ProblemParams, tol: float, stream=None) -> torch.Tensor:
+    y = torch.empty(dmesh.N * dmesh.N, dtype=torch.int32, device="cuda")
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_selector_labels(dmesh.handle, C.byref(p), float(tol), C.c_void_p(y.data_ptr()),
+                                                _stream_ptr(stream)))
+    return y
+
+
+def selector_grad(params: torch.Tensor, feats: torch.Tensor, labels: torch.Tensor, stream=None):
+    """(gradient, loss) of the mean cross-entropy over the samples."""
+    g = torch.empty(SELECTOR_PARAMS, dtype=torch.float32, device="cuda")
+    loss = torch.empty(1, dtype=torch.float32, device="cuda")
+    _lib.check(_lib.load().ebem_selector_grad(C.c_void_p(params.data_ptr()), C.c_void_p(feats.data_ptr()),
+                                              C.c_void_p(labels.data_ptr()), int(labels.numel()),
+                                              C.c_void_p(g.data_ptr()), C.c_void_p(loss.data_ptr()),
+                                              _stream_ptr(stream)))
+    return g, float(loss.item())
+
+
+def selector_train(params: torch.Tensor, feats: torch.Tensor, labels: torch.Tensor, epochs: int = 20,
+                   batch: int = 512, lr: float = 3e-3, seed: int = 0, stream=None):
+    """Train in place; returns the per-epoch full-set loss."""
+    losses = np.zeros(epochs, dtype=np.float32)
+    _lib.check(_lib.load().ebem_selector_train(C.c_void_p(params.data_ptr()), C.c_void_p(feats.data_ptr()),
+                                               C.c_void_p(labels.data_ptr()), int(labels.numel()), int(epochs),
+                                               int(batch), float(lr), int(seed), losses.ctypes.data,
+                                               _stream_ptr(stream)))
+    return losses
+
+
+def selector_infer(params: torch.Tensor, dmesh: DeviceMesh, prm: ProblemParams, threshold: float = 0.9, stream=None):
+    c = torch.empty(dmesh.N * dmesh.N, dtype=torch.int32, device="cuda")
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_selector_infer(C.c_void_p(params.data_ptr()), dmesh.handle, C.byref(p),
+                                               float(threshold), C.c_void_p(c.data_ptr()), _stream_ptr(stream)))
+    return c
+
+
+def assemble_sa_selected(dmesh: DeviceMesh, prm: ProblemParams, classes: torch.Tensor, lag0: int = 0,
+                         nlag: int | None = None, out: torch.Tensor | None = None, prec: int = PREC_FP64, stream=None):
+    """E[l][row, col] with each pair assembled on the rule of its class;
+    returns (E, pairs per class)."""
+    if nlag is None:
+        nlag = num_blocks(dmesh, prm) - lag0
+    n3 = 3 * dmesh.N
+    if out is None:
+        out = torch.empty((nlag, n3, n3), dtype=torch.float64, device="cuda")
+    p = _lib.problem_struct(prm)
+    counts = (C.c_longlong * 4)()
+    _lib.check(_lib.load().ebem_assemble_sa_selected(dmesh.handle, C.byref(p), C.c_void_p(classes.data_ptr()),
+                                                     int(lag0), int(nlag), C.c_void_p(out.data_ptr()), int(prec),
+                                                     _stream_ptr(stream), counts))
+    return out.view(nlag, n3, n3).transpose(1, 2), [int(c) for c in counts]

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 
 struct ebem_mesh {
     ebem::MeshData d;
@@ -800,6 +801,82 @@ int ebem_batch_info(const ebem_batch* b, int* warps_per_block, int* pairs_per_gr
     if (tuned_ms) *tuned_ms = b->tuned_ms;
     if (pairs) *pairs = b->total;
     return EBEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// learned quadrature selector
+
+static bool all_device(std::initializer_list<const void*> ps) {
+    for (const void* q : ps)
+        if (!q || !is_device_ptr(q)) return false;
+    return true;
+}
+
+int ebem_selector_init(float* params, unsigned long long seed) {
+    if (!params) return fail(EBEM_ERR_INVALID, "NULL parameters");
+    if (is_device_ptr(params)) {
+        std::vector<float> h(EBEM_SELECTOR_PARAMS);
+        selector_init(h.data(), seed);
+        EBEM_CUDA_TRY(cudaMemcpy(params, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+    } else {
+        selector_init(params, seed);
+    }
+    return EBEM_OK;
+}
+
+int ebem_selector_features(const ebem_mesh* m, const ebem_problem* p, float* feats, void* stream) {
+    if (!m || !all_device({feats})) return fail(EBEM_ERR_INVALID, "mesh and a device feature buffer required");
+    if (int rc = check_problem(p)) return rc;
+    DeviceGuard dg(m->d.device);
+    return selector_features(m->d, phys_from(p), feats, (cudaStream_t)stream);
+}
+
+int ebem_selector_labels(const ebem_mesh* m, const ebem_problem* p, double tol, int* labels, void* stream) {
+    if (!m || !all_device({labels})) return fail(EBEM_ERR_INVALID, "mesh and a device label buffer required");
+    if (int rc = check_problem(p)) return rc;
+    if (!(tol >= 0)) return fail(EBEM_ERR_INVALID, "tolerance must be >= 0");
+    int L = 0;
+    if (int rc = ebem_num_blocks(m, p, &L)) return rc;
+    DeviceGuard dg(m->d.device);
+    return selector_labels(const_cast<MeshData&>(m->d), phys_from(p), L, tol, labels, (cudaStream_t)stream);
+}
+
+int ebem_selector_grad(const float* params, const float* feats, const int* labels, long long n, float* grad,
+                       float* loss, void* stream) {
+    if (n < 1 || !all_device({params, feats, labels, grad}) || (loss && !is_device_ptr(loss)))
+        return fail(EBEM_ERR_INVALID, "device buffers and n >= 1 required");
+    if (int rc = check_device()) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int rc = selector_grad(params, feats, labels, n, grad, loss, s)) return rc;
+    EBEM_CUDA_TRY(cudaStreamSynchronize(s));
+    return EBEM_OK;
+}
+
+int ebem_selector_train(float* params, const float* feats, const int* labels, long long n, int epochs, int batch,
+                        float lr, unsigned long long seed, float* losses, void* stream) {
+    if (n < 1 || epochs < 1 || batch < 1 || !(lr > 0) || !all_device({params, feats, labels}))
+        return fail(EBEM_ERR_INVALID, "device buffers, n, epochs, batch >= 1 and lr > 0 required");
+    if (int rc = check_device()) return rc;
+    return selector_train(params, feats, labels, n, epochs, batch, lr, seed, losses, (cudaStream_t)stream);
+}
+
+int ebem_selector_infer(const float* params, const ebem_mesh* m, const ebem_problem* p, float threshold, int* classes,
+                        void* stream) {
+    if (!m || !all_device({params, classes})) return fail(EBEM_ERR_INVALID, "mesh and device buffers required");
+    if (int rc = check_problem(p)) return rc;
+    DeviceGuard dg(m->d.device);
+    return selector_infer(params, m->d, phys_from(p), threshold, classes, (cudaStream_t)stream);
+}
+
+int ebem_assemble_sa_selected(const ebem_mesh* m, const ebem_problem* p, const int* classes, int lag0, int nlag,
+                              double* E, int prec, void* stream, long long* pairs_per_class) {
+    if (!m || !all_device({classes, E})) return fail(EBEM_ERR_INVALID, "mesh and device buffers required");
+    if (int rc = check_problem(p)) return rc;
+    if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
+    if (prec != EBEM_PREC_FP64 && prec != EBEM_PREC_MIXED) return fail(EBEM_ERR_INVALID, "unknown precision mode");
+    DeviceGuard dg(m->d.device);
+    return assemble_selected(const_cast<MeshData&>(m->d), phys_from(p), classes, lag0, nlag, E, prec, pairs_per_class,
+                             (cudaStream_t)stream);
 }
 
 }  // extern "C"

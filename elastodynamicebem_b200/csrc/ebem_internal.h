@@ -128,4 +128,18 @@ int march_dd_device(const MeshData& m, const double* dV, int LV, const double* d
                     const double* d_gK, int nT, double* d_phi, cudaStream_t s);
 int launch_hist_gemv(const double* A, int n3, long long K, const double* x, double* y, int sm_count, cudaStream_t s);
 
+// ---------------------------------------------------------------------------
+// learned quadrature selector (selector.cu)
+int selector_features(const MeshData& m, const PhysParams& P, float* d_out, cudaStream_t s);
+int selector_labels(MeshData& m, const PhysParams& P, int L, double tol, int* d_labels, cudaStream_t s);
+int selector_grad(const float* d_params, const float* d_feats, const int* d_labels, long long n, float* d_grad,
+                  float* d_loss, cudaStream_t s);
+int selector_train(float* d_params, const float* d_feats, const int* d_labels, long long n, int epochs, int batch,
+                   float lr, unsigned long long seed, float* h_losses, cudaStream_t s);
+int selector_infer(const float* d_params, const MeshData& m, const PhysParams& P, float threshold, int* d_classes,
+                   cudaStream_t s);
+int assemble_selected(MeshData& m, const PhysParams& P, const int* d_classes, int lag0, int nlag, double* d_E, int prec,
+                      long long* h_counts, cudaStream_t s);
+void selector_init(float* h_params, unsigned long long seed);
+
 }  // namespace ebem

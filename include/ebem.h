@@ -169,6 +169,40 @@ int ebem_batch_info(const ebem_batch* batch, int* warps_per_block, int* pairs_pe
                     long long* pairs);
 int ebem_batch_destroy(ebem_batch* batch);
 
+/* Learned quadrature selector (no counterpart in the reference, which uses
+ * one outer rule for all pairs, BEMenerg_setupCore.m:13-28).  A small MLP
+ * (12 -> 64 -> 64 -> 4, ReLU, softmax, FP32; EBEM_SELECTOR_PARAMS floats:
+ * W1[64][12], b1[64], W2[64][64], b2[64], W3[4][64], b3[4]) maps the 12
+ * features of a (source, field) pair to one of the outer rules 3, 7, 12, 19
+ * (class 0..3).  All buffers below are device buffers unless stated.
+ *   _init      He-initialised parameters (host or device buffer).
+ *   _features  N^2 x 12 features of every pair (pair p = field * N + source).
+ *   _labels    N^2 classes from the plain method itself: the smallest rule
+ *              whose blocks (all lags) differ from the 19-node rule's by at
+ *              most tol * max|E| (else class 3); assembles the mesh four times.
+ *   _grad      gradient of the mean cross-entropy over n samples (+ loss).
+ *   _train     Adam over shuffled mini-batches; losses (host, may be NULL)
+ *              receives the full-set loss after each epoch.
+ *   _infer     class of every pair, the maximal rule (3) where the largest
+ *              probability is below threshold.
+ * ebem_assemble_sa_selected assembles each pair with the rule of its class
+ * (E as ebem_assemble_sa, device, every entry written); pairs_per_class (host,
+ * 4 entries, may be NULL) receives the class sizes. */
+#define EBEM_SELECTOR_FEATURES 12
+#define EBEM_SELECTOR_CLASSES 4
+#define EBEM_SELECTOR_PARAMS 5252
+int ebem_selector_init(float* params, unsigned long long seed);
+int ebem_selector_features(const ebem_mesh* mesh, const ebem_problem* prob, float* feats, void* stream);
+int ebem_selector_labels(const ebem_mesh* mesh, const ebem_problem* prob, double tol, int* labels, void* stream);
+int ebem_selector_grad(const float* params, const float* feats, const int* labels, long long n, float* grad,
+                       float* loss, void* stream);
+int ebem_selector_train(float* params, const float* feats, const int* labels, long long n, int epochs, int batch,
+                        float lr, unsigned long long seed, float* losses, void* stream);
+int ebem_selector_infer(const float* params, const ebem_mesh* mesh, const ebem_problem* prob, float threshold,
+                        int* classes, void* stream);
+int ebem_assemble_sa_selected(const ebem_mesh* mesh, const ebem_problem* prob, const int* classes, int lag0, int nlag,
+                              double* E, int prec, void* stream, long long* pairs_per_class);
+
 /* ebem_assemble_sa_panel with a precision mode. */
 int ebem_assemble_sa_ex(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag, int src0,
                         int nsrc, double* E, long long ld, int accumulate, int prec, void* stream, long long* nonnull);
