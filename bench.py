@@ -38,8 +38,12 @@ UNIT = "pair-integrals/s"
 FLOPS_PER_PAIR_INTEGRAL = 19_232.0
 FLOPS_PER_PAIR_INTEGRAL_REF_SCHEDULE = 53_560.0
 
-# DRAM bytes per launch of sa_assemble_kernel from ncu (None until captured)
-NCU_TRAFFIC_PER_LAUNCH = None
+# DRAM bytes (read + write) per launch of the assembly kernel: ncu on the
+# sphere N=320 case measured 65.9 MB + 668.2 MB; the traffic is the N^2 L output
+# (written in 24-byte column pieces), so it is scaled to N=1280 by the output
+# size, x16.
+NCU_TRAFFIC_PER_LAUNCH = (65.931008e6 + 668.248064e6) * 16
+KERNEL = "sa_assemble_warp_kernel"
 
 
 def log(*a):
@@ -150,6 +154,62 @@ def cpu_baseline(workload, target_s: float = 12.0, nthreads: int = 0):
                       f"{dt:.1f} s"}
 
 
+def forms(core, problem, torch, w, dm, L, plain_rate):
+    """The assembly forms against the plain FP64 assembly: mixed precision on
+    the benchmark workload (speed and error of blocks, density, displacement)
+    and the batched persistent launch on 64 instances of uneven size (against
+    one launch per instance)."""
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+    n3 = 3 * dm.N
+    out = {}
+    buf64 = torch.empty((L, n3, n3), dtype=torch.float64, device="cuda")
+    buf32 = torch.empty_like(buf64)
+    t64 = timed(lambda: core.assemble_sa(dm, w.params, w.n_gh, 0, L, out=buf64))
+    t32 = timed(lambda: core.assemble_sa(dm, w.params, w.n_gh, 0, L, out=buf32, prec=core.PREC_MIXED))
+    e_rel = float((buf32 - buf64).norm() / buf64.norm())
+    del buf32
+    phi64, _ = core.timemarch_sa(dm, w.params, w.n_gh, w.datum)
+    phi32, _ = core.timemarch_sa(dm, w.params, w.n_gh, w.datum, prec=core.PREC_MIXED)
+    u64 = core.pp_sa(dm, w.params, phi64, w.points, w.times)
+    u32 = core.pp_sa(dm, w.params, phi32, w.points, w.times)
+    out["mixed"] = {"assembly_ms": t32, "fp64_assembly_ms": t64, "speedup": t64 / t32, "blocks_rel_err": e_rel,
+                    "density_rel_err": float((phi32 - phi64).norm() / phi64.norm()),
+                    "displacement_rel_err": float((u32 - u64).norm() / u64.norm()),
+                    "scope": "FP32 edge Gauss-Legendre nodes, FP64 closed forms / moments / marching"}
+    del buf64, phi64, phi32
+    torch.cuda.empty_cache()
+    inst = problem.batch_workload(count=64, seed=4)
+    dms = [core.DeviceMesh(m) for _, m, _ in inst]
+    prms = [p for _, _, p in inst]
+    nlag = [min(core.num_blocks(d, p), 8) for d, p in zip(dms, prms)]
+    outs = [torch.empty((l, 3 * d.N, 3 * d.N), dtype=torch.float64, device="cuda") for d, l in zip(dms, nlag)]
+    counts = [core.assemble_sa(d, p, 7, 0, l, out=o, count=True)[1] for d, p, l, o in zip(dms, prms, nlag, outs)]
+    plan = core.BatchPlan(dms, prms, 7, nlag=nlag, prec=core.PREC_FP64)
+    t_batch = timed(lambda: plan.assemble(outs))
+    t_seq = timed(lambda: [core.assemble_sa(d, p, 7, 0, l, out=o) for d, p, l, o in zip(dms, prms, nlag, outs)])
+    plan32 = core.BatchPlan(dms, prms, 7, nlag=nlag, prec=core.PREC_MIXED)
+    t_b32 = timed(lambda: plan32.assemble(outs))
+    info = plan.info()
+    out["batched"] = {"instances": len(inst), "N_range": [min(d.N for d in dms), max(d.N for d in dms)],
+                      "lags_per_instance": "min(L, 8)", "pair_integrals": int(sum(counts)),
+                      "batch_ms": t_batch, "one_launch_per_instance_ms": t_seq, "speedup": t_seq / t_batch,
+                      "batch_mixed_ms": t_b32, "pair_integrals_per_s": sum(counts) / t_batch * 1e3,
+                      "tile": {"warps_per_block": info["warps_per_block"], "pairs_per_grab": info["pairs_per_grab"]}}
+    plan.close(); plan32.close()
+    del outs
+    torch.cuda.empty_cache()
+    return out
+
+
 def reference_arm(args, rank: int):
     from elastodynamicebem_b200 import problem
     if rank != 0:
@@ -183,6 +243,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak measurement")
+    ap.add_argument("--no-forms", action="store_true", help="skip the mixed-precision and batched measurements")
     ap.add_argument("--workload", default="sphere1280", choices=["sphere1280", "sphere320"],
                     help="sphere1280 is the benchmark; sphere320 (icosphere 2) is the small profiling case")
     args = ap.parse_args()
@@ -257,7 +318,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
     value = total_pairs * args.steps / t_max
-    kernel_s = my_s / args.steps          # one sa_assemble_kernel launch per step
+    kernel_s = my_s / args.steps          # one assembly kernel launch per step
 
     # end to end through the C ABI with host buffers: mesh upload, assembly,
     # copy of E to pinned host memory, every step
@@ -300,11 +361,16 @@ def main():
                          "peak_source": "measured: cuBLAS DGEMM 8192^3 via torch.matmul float64, best of 5",
                          "flops_per_unit": FLOPS_PER_PAIR_INTEGRAL,
                          "units_per_launch": my_pairs,
-                         "kernel": "sa_assemble_kernel", "kernel_ms": kernel_s * 1e3},
+                         "kernel": KERNEL, "kernel_ms": kernel_s * 1e3},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "path": "ebem_mesh_create + ebem_assemble_sa_panel into pinned host memory + ebem_mesh_destroy"},
             "clocks": clocks,
         }
+        if not args.no_forms and world == 1:
+            del out
+            torch.cuda.empty_cache()
+            line["forms"] = forms(core, problem, torch, w, dm, L, value)
+            out = None
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(w)
         print(json.dumps(line), flush=True)
