@@ -253,6 +253,14 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
         }
         if (Cu.live) {
             const ChildE& gg = Cu.g;
+            LevelCtx L0;
+            L0.k5 = (A.velP * A.velP + A.velS * A.velS) / ((A.velP * A.velS) * (A.velP * A.velS));
+            L0.k6 = (A.velP * A.velP - A.velS * A.velS) / ((A.velP * A.velS) * (A.velP * A.velS));
+            const W4 w0 = origin_weights(Cu.zeta, L0);
+            W.w0[0][slot] = w0.sc;
+            W.w0[1][slot] = w0.in;
+            W.w0[2][slot] = w0.mx;
+            W.w0[3][slot] = w0.zz;
             W.F[slot] = gg.F;
             W.cbp[slot] = gg.cb * gg.ct + gg.sb * gg.st;     // cos(beta - theta_V1)
             W.sbp[slot] = gg.sb * gg.ct - gg.cb * gg.st;     // sin(beta - theta_V1)
@@ -269,6 +277,7 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
             }
         }
     }
+    unsigned stat = 0;          // bit u: child of slot u has become static
     __syncwarp();
     const int klo = max(1, llo - 1), khi = lhi + 1;
     double Fm2[6] = {0, 0, 0, 0, 0, 0}, Fm1[6] = {0, 0, 0, 0, 0, 0}, Fk[6];
@@ -294,11 +303,19 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
             // decision phase (per child)
             int type = T_NONE;
             double rhoP = -1.0, rhoS = -1.0;
-            if (Cu.live) type = classify(Cu.zeta, L.RP, L.RS, Cu.dMIN, rhoP, rhoS);
+            const bool is_static = (stat >> u) & 1u;
+            if (Cu.live && !is_static) type = classify(Cu.zeta, L.RP, L.RS, Cu.dMIN, rhoP, rhoS);
             AccE Ac = {0, 0, 0, 0, 0, 0, 0};
             int full = 0;
             np[u] = 0;
-            if (type != T_NONE) child_decide(Ac, pc[u], np[u], full, Cu, L, rhoP, rhoS, type);
+            if (type != T_NONE) {
+                W4 w0;
+                w0.sc = W.w0[0][slot];
+                w0.in = W.w0[1][slot];
+                w0.mx = W.w0[2][slot];
+                w0.zz = W.w0[3][slot];
+                child_decide(Ac, pc[u], np[u], full, Cu, L, rhoP, rhoS, type, w0);
+            }
             // whole-range moments, computed by the whole warp once per child
             const bool need = full && !hasmom[u];
             unsigned mm = __ballot_sync(0xffffffffu, need);
@@ -321,7 +338,25 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
             const double zs = Cu.zeta * Cu.sigma;
             if (full & 1) apply_moments(Ac, W, slot, true, L, zs);
             if (full & 2) apply_moments(Ac, W, slot, false, L, zs);
-            if (type != T_NONE) child_to_plane(S, T, Ac, Cu.g, Cu.w * Cu.g.sgnC);
+            if (type != T_NONE) {
+                double Sc = 0.0, Tc[6] = {0, 0, 0, 0, 0, 0};
+                child_to_plane(Sc, Tc, Ac, Cu.g, Cu.w * Cu.g.sgnC);
+                S += Sc;
+#pragma unroll
+                for (int e = 0; e < 6; e++) T[e] += Tc[e];
+                // inside the S front with its whole edge (only the full S piece):
+                // level-independent from now on (the fronts only grow)
+                if (type == T_SP_SP && full == 2 && np[u] == 0) {
+                    W.sv[0][slot] = Sc;
+#pragma unroll
+                    for (int e = 0; e < 6; e++) W.sv[1 + e][slot] = Tc[e];
+                    stat |= 1u << u;
+                }
+            } else if (is_static) {
+                S += W.sv[0][slot];
+#pragma unroll
+                for (int e = 0; e < 6; e++) T[e] += W.sv[1 + e][slot];
+            }
 #pragma unroll
             for (int q = 0; q < 3; q++) {
                 if (q < np[u]) {

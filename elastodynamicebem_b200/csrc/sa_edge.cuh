@@ -84,7 +84,9 @@ struct Rad { double A1, A3, B2, C2, D2, B4, C4, D4; };
 
 EBEM_DI Rad radial_at(double rho, double r, double zeta) {
     Rad v;
-    double ir = 1.0 / r, ir3 = ir * ir * ir, z2 = zeta * zeta;
+    // one reciprocal gives both 1/r and 1/(r + rho)
+    const double q = 1.0 / (r * (r + rho));
+    const double ir = (r + rho) * q, ir3 = ir * ir * ir, z2 = zeta * zeta;
     v.A1 = r;
     v.A3 = -ir;
     v.B2 = r + z2 * ir;
@@ -93,7 +95,7 @@ EBEM_DI Rad radial_at(double rho, double r, double zeta) {
     v.D4 = -z2 * ir3 * (1.0 / 3.0);
     if (zeta > 0) {
         v.C2 = m_log(rho + r) - rho * ir;
-        v.C4 = -(r * r + r * rho + rho * rho) * ir3 / (3.0 * (r + rho));
+        v.C4 = -(r * r + r * rho + rho * rho) * ir3 * (r * q) * (1.0 / 3.0);
     } else {
         v.C2 = 0.0;
         v.C4 = 0.0;
@@ -143,8 +145,9 @@ EBEM_DI void theta_cs(const ChildE& g, double s, double& c, double& sn) {
 // Angle theta at a front crossing s = +-acosh(rho/F): phi = asin(F/rho) for
 // s > 0, pi - asin(F/rho) for s < 0 (the reference's Omega values).
 EBEM_DI void crossing_theta(const ChildE& g, double rho, bool positive, double& th, double& c, double& sn) {
-    double sp = g.F / rho;                                       // sin(phi)
-    double cp = sqrt_c((rho - g.F) * (rho + g.F)) / rho;         // |cos(phi)|
+    const double irho = 1.0 / rho;
+    double sp = g.F * irho;                                      // sin(phi)
+    double cp = sqrt_c((rho - g.F) * (rho + g.F)) * irho;        // |cos(phi)|
     double phi = asin_c(sp);
     if (!positive) { phi = kPi - phi; cp = -cp; }
     th = phi - g.beta;                                           // theta = phi - beta

@@ -44,6 +44,8 @@ struct WarpShared {
     int who[96 * R];                            // child slot | (P terms ? 64 : 0)
     double F[32 * R], cbp[32 * R], sbp[32 * R], zeta[32 * R], zs[32 * R], scale[32 * R];
     double mom[14][32 * R];                     // per-child moments (child frame)
+    double w0[4][32 * R];                       // S-term weights of the origin term (level-independent)
+    double sv[7][32 * R];                       // contribution of a child that has become static
     float Ff[32 * R], cbpf[32 * R], sbpf[32 * R], zetaf[32 * R], zsf[32 * R], scalef[32 * R];   // FP32 bulk
 };
 
@@ -186,6 +188,15 @@ EBEM_DI void apply_moments(AccE& A, const WarpShared<R>& W, int slot, bool pterm
 }
 
 EBEM_DI W4 neg(W4 w) { w.sc = -w.sc; w.in = -w.in; w.mx = -w.mx; w.zz = -w.zz; return w; }
+EBEM_DI W4 wsub(W4 a, const W4& b) { a.sc -= b.sc; a.in -= b.in; a.mx -= b.mx; a.zz -= b.zz; return a; }
+
+// S-term weights of the radial functions at the node's projection (rho = 0,
+// r = zeta): level-independent, computed once per child.
+EBEM_DI W4 origin_weights(double zeta, const LevelCtx& L) {
+    Rad V0 = radial_at(0.0, zeta, zeta);
+    if (!(zeta > 0)) { V0.A1 = 0.0; V0.B2 = 0.0; V0.D2 = 0.0; }
+    return weigh(V0, false, L);
+}
 
 // Per-lane child state, level-independent.
 struct LaneChild {
@@ -200,7 +211,7 @@ struct LaneChild {
 // (or flagged in need_mom when they are not computed yet), partial edge
 // pieces returned in pc[0..np).  Mirrors child_level_e piece by piece.
 EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const LaneChild& C, const LevelCtx& L,
-                          double rhoP, double rhoS, int type) {
+                          double rhoP, double rhoS, int type, const W4& w0) {
     const ChildE& g = C.g;
     const bool isP = (type == T_P), spsp = (type == T_SP_SP);
     const double zeta = C.zeta, zs = C.zeta * C.sigma;
@@ -235,15 +246,19 @@ EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const L
         if (-sP > smin) add_circle(A, wPc, thB, cB, sB, thg, cg, sgm, zs);
         if (xS && !isP) {
             // [sS, sP] <-> theta in [thA, thAS];  [-sP, -sS] <-> [thBS, thB]
+            // (either may span the child's whole edge: edge on one side of
+            // the foot of the perpendicular, between the fronts)
             double lo1 = fmax(sS, smin), hi1 = fmin(sP, smax);
             if (hi1 - lo1 > 0) {
                 add_circle(A, wPlo, thA, cA, sA, thAS, cAS, sAS, zs);
-                pc[np++] = {lo1, hi1, 1};
+                if (sS <= smin && sP >= smax) full_mask |= 1;
+                else pc[np++] = {lo1, hi1, 1};
             }
             double lo2 = fmax(-sP, smin), hi2 = fmin(-sS, smax);
             if (hi2 - lo2 > 0) {
                 add_circle(A, wPlo, thBS, cBS, sBS, thB, cB, sB, zs);
-                pc[np++] = {lo2, hi2, 1};
+                if (-sP <= smin && -sS >= smax) full_mask |= 1;
+                else pc[np++] = {lo2, hi2, 1};
             }
         } else {
             double lo = fmax(-sP, smin), hi = fmin(sP, smax);
@@ -255,10 +270,8 @@ EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const L
         }
     }
     if (spsp) {
-        Rad V0 = radial_at(0.0, zeta, zeta);
-        if (!(zeta > 0)) { V0.A1 = 0.0; V0.B2 = 0.0; V0.D2 = 0.0; }
-        Rad VS = radial_at(rhoS, L.RS, zeta);
-        W4 wSc = weigh(rad_sub(VS, V0), false, L);
+        // P&S terms, radial range [0, min(rhoS, R)]: V_S is VSe (not isP here)
+        W4 wSc = wsub(weigh(VSe, false, L), w0);
         if (!xS) {
             add_circle(A, wSc, th0, c0, sn0, thg, cg, sgm, zs);
         } else {
@@ -266,7 +279,7 @@ EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const L
             if (-sS > smin) add_circle(A, wSc, thBS, cBS, sBS, thg, cg, sgm, zs);
             double lo = fmax(-sS, smin), hi = fmin(sS, smax);
             if (hi - lo > 0) {
-                add_circle(A, neg(weigh(V0, false, L)), thAS, cAS, sAS, thBS, cBS, sBS, zs);
+                add_circle(A, neg(w0), thAS, cAS, sAS, thBS, cBS, sBS, zs);
                 if (-sS <= smin && sS >= smax) full_mask |= 2;
                 else pc[np++] = {lo, hi, 0};
             }

@@ -8,7 +8,8 @@ import pytest
 
 from conftest import cuda_available
 
-TOL = 1e-12
+TOL = 1e-12          # FP64: the same per-pair code compiled in two kernels
+TOL_MIXED = 1e-6     # mixed precision: FP32 contraction choices differ between the two kernels
 
 
 @pytest.fixture(scope="module")
@@ -37,7 +38,7 @@ def test_batch_equals_single(ebem, n_gh, prec):
         torch.cuda.synchronize()
         for g, s1 in zip(got, singles):
             assert torch.isfinite(g).all()
-            assert float((g - s1).norm() / s1.norm()) <= TOL
+            assert float((g - s1).norm() / s1.norm()) <= (TOL_MIXED if prec else TOL)
     info = plan.info()
     assert info["warps_per_block"] in (2, 4) and info["pairs_per_grab"] in (1, 4, 16)
     assert info["tuned_ms"] > 0 and info["pairs"] == sum(d.N ** 2 for d in dms)
