@@ -165,6 +165,32 @@ EBEM_DI void clipped_theta(const ChildE& g, double rho, double sx, bool positive
     else crossing_theta(g, rho, positive, th, c, sn);
 }
 
+// Both crossings s = +-sX, sX = acosh(rho/F), of a front of in-plane radius
+// rho with the edge line (the caller has checked that it crosses), clipped to
+// the child as clipped_theta does: (thA, cA, sA) at +sX, (thB, cB, sB) at -sX.
+// One square root, one logarithm and at most one arcsine serve both sides
+// (the angles are phi and pi - phi).
+EBEM_DI void front_cross(const ChildE& g, double rho, double smin, double thg, double cg, double sgm, double& sX,
+                         double& thA, double& cA, double& sA, double& thB, double& cB, double& sB) {
+    const double q = sqrt_c((rho - g.F) * (rho + g.F));
+    sX = m_log((rho + q) / g.F);
+    const bool a0 = sX >= g.s0, ag = !a0 && sX <= smin;
+    const bool b0 = -sX >= g.s0, bg = !b0 && -sX <= smin;
+    double phi = 0.0, sp = 0.0, cp = 0.0;
+    if (!(a0 || ag) || !(b0 || bg)) {
+        const double irho = 1.0 / rho;
+        sp = g.F * irho;
+        cp = q * irho;
+        phi = asin_c(sp);
+    }
+    if (a0) { thA = 0.0; cA = 1.0; sA = 0.0; }
+    else if (ag) { thA = thg; cA = cg; sA = sgm; }
+    else { thA = phi - g.beta; cA = cp * g.cb + sp * g.sb; sA = sp * g.cb - cp * g.sb; }
+    if (b0) { thB = 0.0; cB = 1.0; sB = 0.0; }
+    else if (bg) { thB = thg; cB = cg; sB = sgm; }
+    else { thB = (kPi - phi) - g.beta; cB = -cp * g.cb + sp * g.sb; sB = sp * g.cb + cp * g.sb; }
+}
+
 // Circle-bounded piece between polar angles (tha; ca, sa) and (thb; cb_, sb_):
 // the radial weights w are constant in theta.
 EBEM_DI void add_circle(AccE& A, const W4& w, double tha, double ca, double sa, double thb, double cbb,

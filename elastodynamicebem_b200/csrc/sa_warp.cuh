@@ -230,18 +230,12 @@ EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const L
     const double thg = g.gamma, cg = C.cg, sgm = C.sg;
     // S crossing data (used by the P pieces when the S front crosses, and by the S terms)
     double sS = 0.0, thAS = 0.0, cAS = 1.0, sAS = 0.0, thBS = 0.0, cBS = 1.0, sBS = 0.0;
-    if (xS && !isP) {
-        sS = m_log((rhoS + sqrt_c((rhoS - g.F) * (rhoS + g.F))) / g.F);
-        clipped_theta(g, rhoS, sS, true, smin, thg, cg, sgm, thAS, cAS, sAS);
-        clipped_theta(g, rhoS, -sS, false, smin, thg, cg, sgm, thBS, cBS, sBS);
-    }
+    if (xS && !isP) front_cross(g, rhoS, smin, thg, cg, sgm, sS, thAS, cAS, sAS, thBS, cBS, sBS);
     if (!xP) {
         add_circle(A, wPc, th0, c0, sn0, thg, cg, sgm, zs);
     } else {
-        double sP = m_log((rhoP + sqrt_c((rhoP - g.F) * (rhoP + g.F))) / g.F);
-        double thA, cA, sA, thB, cB, sB;
-        clipped_theta(g, rhoP, sP, true, smin, thg, cg, sgm, thA, cA, sA);
-        clipped_theta(g, rhoP, -sP, false, smin, thg, cg, sgm, thB, cB, sB);
+        double sP, thA, cA, sA, thB, cB, sB;
+        front_cross(g, rhoP, smin, thg, cg, sgm, sP, thA, cA, sA, thB, cB, sB);
         if (smax > sP) add_circle(A, wPc, th0, c0, sn0, thA, cA, sA, zs);
         if (-sP > smin) add_circle(A, wPc, thB, cB, sB, thg, cg, sgm, zs);
         if (xS && !isP) {
