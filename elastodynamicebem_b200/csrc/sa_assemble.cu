@@ -261,6 +261,7 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
             W.w0[1][slot] = w0.in;
             W.w0[2][slot] = w0.mx;
             W.w0[3][slot] = w0.zz;
+            W.amax[slot] = gg.amax;
             W.F[slot] = gg.F;
             W.cbp[slot] = gg.cb * gg.ct + gg.sb * gg.st;     // cos(beta - theta_V1)
             W.sbp[slot] = gg.sb * gg.ct - gg.cb * gg.st;     // sin(beta - theta_V1)
@@ -314,7 +315,7 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
                 w0.in = W.w0[1][slot];
                 w0.mx = W.w0[2][slot];
                 w0.zz = W.w0[3][slot];
-                child_decide(Ac, pc[u], np[u], full, Cu, L, rhoP, rhoS, type, w0);
+                child_decide(Ac, pc[u], np[u], full, Cu, L, rhoP, rhoS, type, w0, W.amax[slot]);
             }
             // whole-range moments, computed by the whole warp once per child
             const bool need = full && !hasmom[u];
@@ -325,15 +326,15 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
                 const double Fb = __shfl_sync(0xffffffffu, Cu.g.F, b), cbb = __shfl_sync(0xffffffffu, Cu.g.cb, b);
                 const double sbb = __shfl_sync(0xffffffffu, Cu.g.sb, b), zb = __shfl_sync(0xffffffffu, Cu.zeta, b);
                 const double s1b = __shfl_sync(0xffffffffu, Cu.g.s1, b), s0b = __shfl_sync(0xffffffffu, Cu.g.s0, b);
-                double m[14];
+                double m[16];
                 moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx, glw);
-#pragma unroll
-                for (int e = 0; e < 14; e++) m[e] = warp_sum(m[e]);
-                if (lane == b) {
-#pragma unroll
-                    for (int e = 0; e < 14; e++) W.mom[e][slot] = m[e];
-                }
+                m[14] = 0.0;
+                m[15] = 0.0;
+                const double tot = warp_reduce_scatter16(m, lane);
+                const int e = scatter16_index(lane);
+                if (!(lane & 1) && e < 14) W.mom[e][b + 32 * u] = tot;
             }
+            __syncwarp();
             if (need) hasmom[u] = true;
             const double zs = Cu.zeta * Cu.sigma;
             if (full & 1) apply_moments(Ac, W, slot, true, L, zs);
@@ -433,9 +434,13 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
             T[5] += f * w.zz;
         }
         __syncwarp();
-        S = warp_sum(S);
+        {
+            double v[8] = {S, T[0], T[1], T[2], T[3], T[4], T[5], 0.0};
+            const double tot = warp_reduce_scatter8(v, lane);
+            S = __shfl_sync(0xffffffffu, tot, scatter8_lane(0));
 #pragma unroll
-        for (int e = 0; e < 6; e++) T[e] = warp_sum(T[e]);
+            for (int e = 0; e < 6; e++) T[e] = __shfl_sync(0xffffffffu, tot, scatter8_lane(1 + e));
+        }
         // F(t_k) = (S I + C^T M C) / 2 in global axes
         {
             double M[3][3] = {{T[0], T[1], T[3]}, {T[1], T[2], T[4]}, {T[3], T[4], T[5]}};

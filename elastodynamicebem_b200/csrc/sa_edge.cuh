@@ -75,6 +75,7 @@ struct ChildE {
     double s0, s1;           // s at theta = 0 (s0, largest) and at theta = gamma (s1)
     double ct, st;           // child frame -> plane frame rotation (V1 direction)
     double sgnC;
+    double amax;             // max(|V1|, |V2|): a front of larger radius covers the whole edge
 };
 
 // Radial antiderivatives at in-plane radius rho (r = sqrt(rho^2+zeta^2)
@@ -272,6 +273,7 @@ EBEM_DI void child_geo_e(ChildE& g, double v1x, double v1y, double v2x, double v
     g.gamma = m_atan2(cr, dg);
     g.s0 = -log_tan_half(cr, db, a * c);          // s at phi = beta
     g.s1 = log_tan_half(cr, da, b * c);           // s at phi = pi - alpha
+    g.amax = fmax(a, b);
     g.ct = v1x / a;
     g.st = v1y / a;
     g.sgnC = sgnC;

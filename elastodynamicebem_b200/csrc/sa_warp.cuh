@@ -45,6 +45,7 @@ struct WarpShared {
     double F[32 * R], cbp[32 * R], sbp[32 * R], zeta[32 * R], zs[32 * R], scale[32 * R];
     double mom[14][32 * R];                     // per-child moments (child frame)
     double w0[4][32 * R];                       // S-term weights of the origin term (level-independent)
+    double amax[32 * R];                        // max(|V1|, |V2|) of each child
     double sv[7][32 * R];                       // contribution of a child that has become static
     float Ff[32 * R], cbpf[32 * R], sbpf[32 * R], zetaf[32 * R], zsf[32 * R], scalef[32 * R];   // FP32 bulk
 };
@@ -211,7 +212,7 @@ struct LaneChild {
 // (or flagged in need_mom when they are not computed yet), partial edge
 // pieces returned in pc[0..np).  Mirrors child_level_e piece by piece.
 EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const LaneChild& C, const LevelCtx& L,
-                          double rhoP, double rhoS, int type, const W4& w0) {
+                          double rhoP, double rhoS, int type, const W4& w0, double amax) {
     const ChildE& g = C.g;
     const bool isP = (type == T_P), spsp = (type == T_SP_SP);
     const double zeta = C.zeta, zs = C.zeta * C.sigma;
@@ -230,12 +231,24 @@ EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const L
     const double thg = g.gamma, cg = C.cg, sgm = C.sg;
     // S crossing data (used by the P pieces when the S front crosses, and by the S terms)
     double sS = 0.0, thAS = 0.0, cAS = 1.0, sAS = 0.0, thBS = 0.0, cBS = 1.0, sBS = 0.0;
-    if (xS && !isP) front_cross(g, rhoS, smin, thg, cg, sgm, sS, thAS, cAS, sAS, thBS, cBS, sBS);
+    // a front whose radius reaches both edge ends covers the whole edge: both
+    // crossings lie beyond the child (clipped to theta = 0 and gamma)
+    if (xS && !isP) {
+        if (rhoS >= amax) {
+            sS = 1e300; thAS = 0.0; cAS = 1.0; sAS = 0.0; thBS = thg; cBS = cg; sBS = sgm;
+        } else {
+            front_cross(g, rhoS, smin, thg, cg, sgm, sS, thAS, cAS, sAS, thBS, cBS, sBS);
+        }
+    }
     if (!xP) {
         add_circle(A, wPc, th0, c0, sn0, thg, cg, sgm, zs);
     } else {
         double sP, thA, cA, sA, thB, cB, sB;
-        front_cross(g, rhoP, smin, thg, cg, sgm, sP, thA, cA, sA, thB, cB, sB);
+        if (rhoP >= amax) {
+            sP = 1e300; thA = 0.0; cA = 1.0; sA = 0.0; thB = thg; cB = cg; sB = sgm;
+        } else {
+            front_cross(g, rhoP, smin, thg, cg, sgm, sP, thA, cA, sA, thB, cB, sB);
+        }
         if (smax > sP) add_circle(A, wPc, th0, c0, sn0, thA, cA, sA, zs);
         if (-sP > smin) add_circle(A, wPc, thB, cB, sB, thg, cg, sgm, zs);
         if (xS && !isP) {
@@ -300,6 +313,46 @@ EBEM_DI double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+
+// One halving step of a warp reduce-scatter: lanes with bit m of their index
+// set keep the upper half of v[0..2h), the others the lower half; each adds
+// its partner's copy of the half it keeps.
+template <int M, int H>
+EBEM_DI void rs_step(double* v, int lane) {
+    const bool up = (lane & M) != 0;
+#pragma unroll
+    for (int k = 0; k < H; k++) {
+        const double send = up ? v[k] : v[k + H];
+        const double keep = up ? v[k + H] : v[k];
+        v[k] = keep + __shfl_xor_sync(0xffffffffu, send, M);
+    }
+}
+
+// Warp sums of 16 per-lane values with 15 shuffles: lane l returns the total
+// of value scatter16_index(l).
+EBEM_DI double warp_reduce_scatter16(double v[16], int lane) {
+    rs_step<16, 8>(v, lane);
+    rs_step<8, 4>(v, lane);
+    rs_step<4, 2>(v, lane);
+    rs_step<2, 1>(v, lane);
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+EBEM_DI int scatter16_index(int lane) {
+    return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+}
+
+// Warp sums of 8 per-lane values with 9 shuffles: lane l returns the total of
+// value 4 b4 + 2 b3 + b2 (b = bits of l); scatter8_lane(e) holds value e.
+EBEM_DI double warp_reduce_scatter8(double v[8], int lane) {
+    rs_step<16, 4>(v, lane);
+    rs_step<8, 2>(v, lane);
+    rs_step<4, 1>(v, lane);
+    double x = v[0];
+    x += __shfl_xor_sync(0xffffffffu, x, 2);
+    x += __shfl_xor_sync(0xffffffffu, x, 1);
+    return x;
+}
+EBEM_DI int scatter8_lane(int e) { return ((e >> 2) & 1) << 4 | ((e >> 1) & 1) << 3 | (e & 1) << 2; }
 
 EBEM_DI int warp_excl_scan(int v, int lane, int& total) {
     int x = v;
