@@ -285,36 +285,59 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
             if (d_count) cudaFree(d_count);
             return fail(EBEM_ERR_INVALID, "host output needs ld == 3 nsrc");
         }
-        // host output: assemble chunks of lags in device memory and copy back
+        // host output: source-row sub-panels are assembled into two device
+        // buffers in turn; each is copied back (a 2D copy into the strided
+        // host panel) on a second stream while the next one is assembled
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
-        size_t per_lag = lag_elems * sizeof(double);
-        size_t budget = std::max<size_t>(per_lag, std::min<size_t>(free_b / 2, (size_t)16 << 30));
-        int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nlag, budget / per_lag));
-        double* d_buf = nullptr;
-        if (cudaMalloc(&d_buf, per_lag * chunk) != cudaSuccess) {
+        const size_t cols = n3 * (size_t)nlag;                     // columns of all lags
+        const size_t per_row = 3 * cols * sizeof(double);          // one source triangle, all lags
+        const size_t budget = std::min<size_t>(free_b / 2, (size_t)16 << 30) / 2;   // per buffer
+        int rows = (int)std::max<size_t>(1, std::min<size_t>(budget / per_row, (size_t)(nsrc + 7) / 8));
+        rows = std::min(rows, nsrc);
+        double* buf[2] = {nullptr, nullptr};
+        cudaStream_t cs = nullptr;
+        cudaEvent_t done[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+        bool ok = cudaMalloc(&buf[0], per_row * rows) == cudaSuccess &&
+                  (rows >= nsrc || cudaMalloc(&buf[1], per_row * rows) == cudaSuccess) &&
+                  cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess;
+        for (int b = 0; ok && b < 2; b++)
+            ok = cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) {
             cudaGetLastError();
-            if (d_count) cudaFree(d_count);
-            return fail(EBEM_ERR_NOMEM, "device staging buffer allocation failed");
+            rc = fail(EBEM_ERR_NOMEM, "device staging buffer allocation failed");
         }
-        for (int q0 = 0; q0 < nlag && rc == EBEM_OK; q0 += chunk) {
-            int nq = std::min(chunk, nlag - q0);
-            double* hE = E + (size_t)q0 * lag_elems;
-            if (accumulate &&
-                cudaMemcpyAsync(d_buf, hE, per_lag * nq, cudaMemcpyHostToDevice, s) != cudaSuccess) {
-                rc = fail(EBEM_ERR_CUDA, "upload failed");
-                break;
-            }
-            rc = launch_sa_assemble(md, P, n_gh, lag0 + q0, nq, src0, nsrc, d_buf, (size_t)ld, lag_elems, accumulate,
-                                    d_count, s, 0, prec == EBEM_PREC_MIXED);
+        for (int k = 0, r0 = 0; rc == EBEM_OK && r0 < nsrc; k++, r0 += rows) {
+            const int nr = std::min(rows, nsrc - r0), b = k & 1;
+            const size_t ldb = 3 * (size_t)nr;
+            double* hE = E + 3 * (size_t)r0;
+            cudaError_t e = cudaSuccess;
+            if (k >= 2) e = cudaStreamWaitEvent(s, copied[b], 0);
+            if (e == cudaSuccess && accumulate)
+                e = cudaMemcpy2DAsync(buf[b], ldb * sizeof(double), hE, (size_t)ld * sizeof(double), ldb * sizeof(double),
+                                      cols, cudaMemcpyHostToDevice, s);
+            if (e != cudaSuccess) { rc = fail(EBEM_ERR_CUDA, "upload failed"); break; }
+            rc = launch_sa_assemble(md, P, n_gh, lag0, nlag, src0 + r0, nr, buf[b], ldb, ldb * n3, accumulate, d_count,
+                                    s, 0, prec == EBEM_PREC_MIXED);
             if (rc) break;
-            if (cudaMemcpyAsync(hE, d_buf, per_lag * nq, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
-                rc = fail(EBEM_ERR_CUDA, "download failed");
-                break;
-            }
+            e = cudaEventRecord(done[b], s);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, done[b], 0);
+            if (e == cudaSuccess)
+                e = cudaMemcpy2DAsync(hE, (size_t)ld * sizeof(double), buf[b], ldb * sizeof(double), ldb * sizeof(double),
+                                      cols, cudaMemcpyDeviceToHost, cs);
+            if (e == cudaSuccess) e = cudaEventRecord(copied[b], cs);
+            if (e != cudaSuccess) { rc = fail(EBEM_ERR_CUDA, "download failed"); break; }
         }
-        cudaError_t e = cudaStreamSynchronize(s);
-        cudaFree(d_buf);
+        cudaError_t e = cs ? cudaStreamSynchronize(cs) : cudaSuccess;
+        cudaError_t e2 = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = e2;
+        for (int b = 0; b < 2; b++) {
+            if (done[b]) cudaEventDestroy(done[b]);
+            if (copied[b]) cudaEventDestroy(copied[b]);
+            if (buf[b]) cudaFree(buf[b]);
+        }
+        if (cs) cudaStreamDestroy(cs);
         if (rc == EBEM_OK && e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, cudaGetErrorString(e));
     }
     if (d_count) {

@@ -124,6 +124,25 @@ def test_host_output_matches_device(ebem):
     assert torch.equal(h, dev)
 
 
+def test_host_output_pipeline(ebem):
+    """Host outputs are assembled in source-row sub-panels whose copies
+    overlap the next sub-panel: accumulation into pageable memory and a row
+    panel that starts inside the mesh equal the device results."""
+    import torch
+    m, prm = _case("screen32")
+    dm = ebem.DeviceMesh(m)
+    L = ebem.num_blocks(dm, prm)
+    n3 = 3 * m.numberTriangles
+    dev = ebem.assemble_sa(dm, prm, 7, 0, L).cpu()
+    acc = torch.full((L, n3, n3), 0.25, dtype=torch.float64)            # pageable
+    h = ebem.assemble_sa(dm, prm, 7, 0, L, out=acc, accumulate=True)
+    assert torch.allclose(h, dev + 0.25, rtol=0, atol=1e-15)
+    src0, nsrc = 5, 13
+    pd = ebem.assemble_sa_panel(dm, prm, 7, 0, L, src0, nsrc).cpu()
+    ph = ebem.assemble_sa_panel(dm, prm, 7, 0, L, src0, nsrc, out=torch.empty((L, n3, 3 * nsrc), dtype=torch.float64))
+    assert torch.equal(ph, pd)
+
+
 def test_sphere1280_sampled_blocks(ebem, oracle):
     """Full headline workload on the device; parity on a seeded sample of
     (source, field, lag) blocks plus size-independent properties."""
