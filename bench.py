@@ -267,13 +267,12 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
 
-    from elastodynamicebem_b200 import core, problem
+    from elastodynamicebem_b200 import core, problem, shard
 
     w = problem.sphere_workload(7, subdivisions=3 if args.workload == "sphere1280" else 2)
     m, prm = w.mesh, w.params
     N = m.numberTriangles
-    src0 = rank * N // world
-    nsrc = (rank + 1) * N // world - src0
+    src0, nsrc = shard.row_panel(rank, world, N)
     dm = core.DeviceMesh(m)
     L = core.num_blocks(dm, prm)
     n3 = 3 * N

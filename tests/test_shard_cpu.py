@@ -1,0 +1,68 @@
+"""The N > 1 path on the CPU: two gloo ranks each assemble their source-row
+panel (here with the oracle, the same blocks the device panel kernel
+produces), gather the panels, and must reproduce the full assembly; the
+panels partition the rows and the timing/count reductions of the benchmark
+(sum of counts, max of times) behave as on NCCL."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_row_panels_partition():
+    from elastodynamicebem_b200 import shard
+    for n in (1, 7, 128, 1280):
+        for w in (1, 2, 3, 8):
+            spans = [shard.row_panel(r, w, n) for r in range(w)]
+            assert spans[0][0] == 0 and sum(s for _, s in spans) == n
+            assert all(a + b == c for (a, b), (c, _) in zip(spans, spans[1:]))
+    with pytest.raises(ValueError):
+        shard.row_panel(2, 2, 10)
+
+
+def _worker(rank, world, port, out):
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import torch
+    import torch.distributed as dist
+    import oracle as O
+    from elastodynamicebem_b200 import mesh, problem, shard
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    m, prm = mesh.screen_uniform(3), problem.ProblemParams(1.0, 1.0, 2.0, 1.0, 10)
+    N = m.numberTriangles
+    L = O.num_blocks(m, prm)
+    src0, nsrc = shard.row_panel(rank, world, N)
+    full = O.assemble_sa(m, prm, 7, 0, L, nthreads=1)[0]          # (L, 3N, 3N) [l][row, col]
+    panel = torch.tensor(full[:, 3 * src0:3 * (src0 + nsrc), :])     # this rank's rows
+    E = shard.gather_panels(panel, N, world).numpy()
+    cnt = torch.tensor([float(np.count_nonzero(np.abs(panel.numpy()).reshape(L, nsrc, 3, N, 3).sum(axis=(2, 4))))])
+    dist.all_reduce(cnt)
+    t = torch.tensor([float(rank + 1)])
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    if rank == 0:
+        np.save(out, E)
+        np.save(out + ".meta.npy", np.array([cnt.item(), t.item(),
+                                             np.count_nonzero(np.abs(full).reshape(L, N, 3, N, 3).sum(axis=(2, 4)))]))
+    dist.destroy_process_group()
+
+
+def test_two_rank_gather_reproduces_full(tmp_path):
+    import socket
+    import torch.multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from elastodynamicebem_b200 import mesh, problem
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = str(tmp_path / "E.npy")
+    mp.start_processes(_worker, args=(2, port, out), nprocs=2, start_method="spawn", join=True)
+    E = np.load(out)
+    cnt, tmax, cfull = np.load(out + ".meta.npy")
+    m, prm = mesh.screen_uniform(3), problem.ProblemParams(1.0, 1.0, 2.0, 1.0, 10)
+    full = O.assemble_sa(m, prm, 7, 0, O.num_blocks(m, prm), nthreads=1)[0]
+    assert np.array_equal(E, full)
+    assert cnt == cfull and tmax == 2.0
