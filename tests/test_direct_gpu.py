@@ -184,3 +184,25 @@ def test_oracle_pp_matches_reference_kernels(oracle, bar):
         Gr, Pr = oracle.ref_pp_dir(m, prm, 4, 3, x, t)
         Go, Po = oracle.pp_dir_matrices(m, prm, 4, 3, x, t)
         assert rel(Go, Gr) <= TOL_REF and rel(Po, Pr) <= TOL_REF
+
+
+def test_dn_stability_reference_defect(ebem):
+    """On the 448-triangle bar the DN marching stays bounded with kernelK's
+    front fixed (H(t - r/c_P)) and grows with the reference's H(r - r/c_P)
+    (kernelK.cu:414-449), measured against the 1-D bar closed form (which
+    ignores the lateral Poisson contraction, so it is a scale, not a bar)."""
+    import torch
+    from elastodynamicebem_b200 import mesh, problem
+    m, prm = mesh.prism_bar(1.0, 1.0, 3.0, 0.25), problem.ProblemParams(1.0, 1.0, 2.0, 2.0, 40)
+    dm = ebem.DeviceMesh(m)
+    LV, LK = ebem.num_blocks_dir(dm, prm)
+    V = ebem.assemble_v(dm, prm, 7, 4, 3, 16, 0, LV)
+    gV = torch.tensor(problem.bar_neumann(m, prm, 3.0), device="cuda")
+    ref = problem.bar_dirichlet(m, prm, 3.0)
+    err = {}
+    for fix in (True, False):
+        K = ebem.assemble_k(dm, prm, 7, 4, 3, 16, 0, LK, fix=fix)
+        u = ebem.march_dn(dm, prm, V, K, gV).cpu().numpy()
+        err[fix] = float(np.linalg.norm(u - ref) / np.linalg.norm(ref))
+    assert err[True] < 0.6            # bounded, at the level of the 1-D model's own error
+    assert err[False] > 2 * err[True]  # the reference's front in kernelK makes the marching grow
