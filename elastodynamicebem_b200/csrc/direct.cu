@@ -317,6 +317,102 @@ __device__ __forceinline__ void k_emit(const KArgs& A, int l, int x, int s, cons
         }
 }
 
+// Third difference over the window of lag l, E_l = T_{l+1} - 3 T_l + 3 T_{l-1}
+// - T_{l-2} on the levels t_k = k dt with levels k < 1 read as 0 (the lag
+// combination of kernelK.cu), taken per node pair on the scalar time
+// functions of one front X (arrival tX = r / c_X):
+//   R = (t - tX) H,  H = [t - tX > 0],  S = (t - tX)^2 (t + 2 tX) / 6 H.
+// Before the front all three vanish; with the whole window after it R is
+// linear, H constant and S a cubic of leading coefficient 1/6, so the
+// differences are exactly (0, 0, dt^3).  Only windows that a front crosses,
+// or that reach below level 1, are summed level by level.
+struct Win3 {
+    double R, H, S;
+};
+
+__host__ __device__ __forceinline__ Win3 front_window3(double tX, int l, double dt) {
+    Win3 d = {0.0, 0.0, 0.0};
+    if ((l + 1) * dt - tX <= 0) return d;
+    if (l >= 3 && (l - 2) * dt - tX > 0) {
+        d.S = dt * dt * dt;
+        return d;
+    }
+    const double c[4] = {-1.0, 3.0, -3.0, 1.0};
+    for (int w = 0; w < 4; w++) {
+        const int k = l - 2 + w;
+        if (k < 1) continue;
+        const double t = k * dt, a = t - tX;
+        if (a > 0) {
+            d.R += c[w] * a;
+            d.H += c[w];
+            d.S += c[w] * (a * a * (t + 2 * tX) / 6);
+        }
+    }
+    return d;
+}
+
+// Third difference of the linear (t - tP) of the reference's H(r - r/c_P)
+// term (kernelK.cu:414-449): zero unless the window reaches below level 1.
+__host__ __device__ __forceinline__ double lin_window3(double tP, int l, double dt) {
+    if (l >= 3) return 0.0;
+    const double c[4] = {-1.0, 3.0, -3.0, 1.0};
+    double d = 0.0;
+    for (int w = 0; w < 4; w++) {
+        const int k = l - 2 + w;
+        if (k >= 1) d += c[w] * (k * dt - tP);
+    }
+    return d;
+}
+
+struct KCoef {
+    double a1, a2, c1, c2, icP, icS, icP2, icS2;
+};
+
+__host__ __device__ inline KCoef k_coef(const Mat& p) {
+    KCoef c;
+    c.a1 = p.lam / (p.lam + p.mu);
+    c.a2 = p.mu / (p.lam + p.mu);
+    c.c1 = p.lam * p.mu / (p.rho * (p.lam + p.mu));
+    c.c2 = 2 * p.mu / p.rho;
+    c.icP = 1 / p.cP;
+    c.icS = 1 / p.cS;
+    c.icP2 = 1 / (p.cP * p.cP);
+    c.icS2 = 1 / (p.cS * p.cS);
+    return c;
+}
+
+// One node pair's share of the lag-l third difference of the double-layer
+// kernel (nucleoKL + nucleoKT - sum_j vms_j nucleoKRj of kernelK.cu), x =
+// outer - inner node, n the field triangle's normal, v = vms.  With the
+// window differences dRP, dRS, dHP, dHS, dRPl (the lambda-mu term's R_P) and
+// dHh = dS_S - dS_P the kernel collapses to
+//   out_ik = b1 (a1 x_i n_k + a2 x_k n_i) + b2 delta_ik - b3 w_i x_k - b4 u_ik,
+//   w = v x x,  u_ik = sum_j eps_jik v_j,
+//   b1 = phik (ir^3 (dRP - dRS) + ir^2 (dHP/c_P - dHS/c_S)),
+//   b2 = phik (x.n) (ir^3 dRS + ir^2 dHS/c_S),
+//   b3 = c2 ir^3 (dRP/c_P^2 - dRS/c_S^2) - 3 c2 ir^5 dHh,
+//   b4 = c1 ir (dRPl/c_P^2 - dRS/c_S^2) - c2 ir^3 dHh,
+// a1 = lambda/(lambda+mu), a2 = mu/(lambda+mu), c1 = lambda mu/(rho(lambda+mu)),
+// c2 = 2 mu/rho.
+__host__ __device__ __forceinline__ void k_pair(double out[9], const double x[3], double ir, const double n[3],
+                                                const double v[3], double phik, double dRP, double dRS, double dHP,
+                                                double dHS, double dRPl, double dHh, const KCoef& c) {
+    const double ir2 = ir * ir, ir3 = ir2 * ir, ir5 = ir3 * ir2;
+    const double xn = x[0] * n[0] + x[1] * n[1] + x[2] * n[2];
+    const double b1 = phik * (ir3 * (dRP - dRS) + ir2 * (dHP * c.icP - dHS * c.icS));
+    const double b2 = phik * xn * (ir3 * dRS + ir2 * dHS * c.icS);
+    const double b3 = c.c2 * ir3 * (dRP * c.icP2 - dRS * c.icS2) - 3 * c.c2 * ir5 * dHh;
+    const double b4 = c.c1 * ir * (dRPl * c.icP2 - dRS * c.icS2) - c.c2 * ir3 * dHh;
+    const double w[3] = {v[1] * x[2] - v[2] * x[1], v[2] * x[0] - v[0] * x[2], v[0] * x[1] - v[1] * x[0]};
+    const double u[9] = {0, v[2], -v[1], -v[2], 0, v[0], v[1], -v[0], 0};
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            out[3 * i + k] = b1 * (c.a1 * x[i] * n[k] + c.a2 * x[k] * n[i]) + ((i == k) ? b2 : 0.0) -
+                             b3 * w[i] * x[k] - b4 * u[3 * i + k];
+}
+
 __global__ void __launch_bounds__(128) k_assemble_kernel(KArgs A) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= (long long)A.N * A.Nv) return;
@@ -343,12 +439,16 @@ __global__ void __launch_bounds__(128) k_assemble_kernel(KArgs A) {
     }
     if (llo < 0) return;
     const int e0 = A.vt_off[s], e1 = A.vt_off[s + 1];
-    double Tm3[9] = {0}, Tm2[9] = {0}, Tm1[9] = {0}, T[9];
-    const int klo = max(1, llo - 2), khi = lhi + 1;
-    for (int k = klo; k <= khi; k++) {
-        const double t = k * A.dt;
-#pragma unroll
-        for (int e = 0; e < 9; e++) T[e] = 0.0;
+    const double cP = A.p.cP, cS = A.p.cS, dt = A.dt;
+    const KCoef cd = k_coef(A.p);
+    for (int l = llo; l <= lhi; l++) {
+        // node pairs provably outside the window's fronts are skipped on r^2:
+        // all four levels before the P front, or all after the S front
+        const bool lin = !A.fix && l < 3;
+        const double thi = (l + 1) * dt, tlo = (l - 2) * dt;
+        const double skipP2 = lin ? 1e300 : (cP * thi) * (cP * thi) * (1 + 1e-12);
+        const double skipS2 = (l >= 3) ? (cS * tlo) * (cS * tlo) * (1 - 1e-12) : -1.0;
+        double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int ee = e0; ee < e1; ee++) {
             const int m = A.vt_tri[ee];
             if (m == x) continue;
@@ -365,19 +465,28 @@ __global__ void __launch_bounds__(128) k_assemble_kernel(KArgs A) {
                     double xo[3];
                     bary_point(xo, A.outer + 3 * o, X.V);
                     const double pt[3] = {xo[0] - y[0], xo[1] - y[1], xo[2] - y[2]};
-                    const double r = sqrt(pt[0] * pt[0] + pt[1] * pt[1] + pt[2] * pt[2]);
-                    double v[9];
-                    kern_k(v, pt, r, F.n, t, vms, phik, A.p, true, !A.fix);
+                    const double r2 = pt[0] * pt[0] + pt[1] * pt[1] + pt[2] * pt[2];
+                    if (r2 > skipP2 || r2 < skipS2) continue;
+                    const double r = sqrt(r2);
+                    const double tP = r / cP, tS = r / cS;
+                    const Win3 P = front_window3(tP, l, dt), S = front_window3(tS, l, dt);
+                    const double dRPl = A.fix ? P.R : ((r - tP > 0) ? lin_window3(tP, l, dt) : 0.0);
+                    const double dHh = S.S - P.S;
                     const double w = (A.wout[o] * X.area) * wi;
+                    double v[9];
+                    k_pair(v, pt, 1.0 / r, F.n, vms, phik, P.R, S.R, P.H, S.H, dRPl, dHh, cd);
 #pragma unroll
                     for (int e = 0; e < 9; e++) T[e] += w * v[e];
                 }
             }
         }
-        const int l = k - 1;
-        if (l >= llo && l <= lhi) k_emit(A, l, x, s, Tm3, Tm2, Tm1, T, true);
+        double* base = A.K + (size_t)(l - A.lag0) * A.ld_lag + (3 * (size_t)s) * A.ld + 3 * (size_t)x;
+        const double c = 4 * kPi * dt;
 #pragma unroll
-        for (int e = 0; e < 9; e++) { Tm3[e] = Tm2[e]; Tm2[e] = Tm1[e]; Tm1[e] = T[e]; }
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+                if (fabs(T[3 * i + j]) > 1.0e-14) base[(size_t)j * A.ld + i] += T[3 * i + j] / c;
     }
 }
 

@@ -14,10 +14,13 @@
 // 4 pi rho (:164-165), accumulated into the output (+=).
 //
 // B200 design: one thread per (source, field) pair (consecutive lanes take
-// consecutive sources of one field triangle); the thread evaluates the
-// node-pair sum K(t_k) once per time level and emits
-// E_l = K_{l+1} - 2 K_l + K_{l-1} from a sliding window (the reference
-// recomputes each instant for three lags and reduces through shared memory).
+// consecutive sources of one field triangle).  The lag combination E_l =
+// K_{l+1} - 2 K_l + K_{l-1} is taken per node pair on the kernel's scalar time
+// functions (ghc_window2), so a node pair costs work only in the lags whose
+// window a front crosses or lies between the fronts, where the difference
+// has a closed form; windows before the P front or after the S front are
+// skipped on r^2 (the reference evaluates every node pair at every instant
+// of every lag and reduces through shared memory).
 #include "ebem_internal.h"
 #include "sa_pair.cuh"
 
@@ -39,21 +42,51 @@ struct GHCArgs {
     size_t ld, ld_lag;
 };
 
-// kernelGHC.cu:204-259 (nucleo) for one node pair, symmetric entries
-// (11,12,13,22,23,33), at instant t.
-__device__ __forceinline__ void nucleo_sym(double nu[6], const double x[3], double r, double t, double cP,
-                                           double cS) {
-    const double r3 = r * r * r, r5 = r3 * r * r;
-    const double HP = (t - (r / cP) > 0) ? 1.0 : 0.0, HS = (t - (r / cS) > 0) ? 1.0 : 0.0;
-    const double tail = (cP * cP * t * t - r * r) / (cP * cP) * HP - (cS * cS * t * t - r * r) / (cS * cS) * HS;
-    const double icP2 = 1 / (cP * cP), icS2 = 1 / (cS * cS);
-    const int ii[6] = {0, 0, 0, 1, 1, 2}, jj[6] = {0, 1, 2, 1, 2, 2};
-#pragma unroll
-    for (int e = 0; e < 6; e++) {
-        const double xx = x[ii[e]] * x[jj[e]];
-        const double dlt = (ii[e] == jj[e]) ? 1.0 : 0.0;
-        nu[e] = (xx / r3) * icP2 * HP + (dlt / r - xx / r3) * icS2 * HS - 0.5 * (dlt / r3 - 3 * (xx / r5)) * tail;
+// Second difference over the window of lag l (levels l-1, l, l+1 of t_k =
+// k dt, kernelGHC.cu:88-99) of the time functions of one front X of the
+// kernel kernelGHC.cu:204-259 (nucleo): H = [t - r/c > 0] and
+// Q = (c^2 t^2 - r^2) / c^2 H.  Before the front both vanish; with the whole
+// window after it H is constant and Q = t^2 - r^2/c^2, so the differences
+// are exactly (0, 2 dt^2).
+struct Win2 {
+    double H, Q;
+};
+
+__host__ __device__ __forceinline__ Win2 ghc_window2(double r, double c, int l, double dt) {
+    Win2 d = {0.0, 0.0};
+    if ((l + 1) * dt - r / c <= 0) return d;
+    if (l >= 1 && (l - 1) * dt - r / c > 0) {
+        d.Q = 2 * dt * dt;
+        return d;
     }
+    const double w[3] = {1.0, -2.0, 1.0};
+    for (int j = 0; j < 3; j++) {
+        const int k = l - 1 + j;
+        if (k < 0) continue;
+        const double t = k * dt;
+        if (t - r / c > 0) {
+            d.H += w[j];
+            d.Q += w[j] * ((c * c * t * t - r * r) / (c * c));
+        }
+    }
+    return d;
+}
+
+// One node pair's share of the lag-l second difference of nucleo, symmetric
+// entries (11,12,13,22,23,33): with dQ = dQ_P - dQ_S,
+//   out_ij = g1 x_i x_j + g2 delta_ij,
+//   g1 = ir^3 (dH_P/c_P^2 - dH_S/c_S^2) + 3/2 ir^5 dQ,  g2 = ir dH_S/c_S^2 - 1/2 ir^3 dQ.
+__host__ __device__ __forceinline__ void ghc_pair(double nu[6], const double x[3], double ir, double dHP, double dHS,
+                                                  double dQ, double icP2, double icS2) {
+    const double ir2 = ir * ir, ir3 = ir2 * ir, ir5 = ir3 * ir2;
+    const double g1 = ir3 * (dHP * icP2 - dHS * icS2) + 1.5 * ir5 * dQ;
+    const double g2 = ir * dHS * icS2 - 0.5 * ir3 * dQ;
+    nu[0] = g1 * x[0] * x[0] + g2;
+    nu[1] = g1 * x[0] * x[1];
+    nu[2] = g1 * x[0] * x[2];
+    nu[3] = g1 * x[1] * x[1] + g2;
+    nu[4] = g1 * x[1] * x[2];
+    nu[5] = g1 * x[2] * x[2] + g2;
 }
 
 __global__ void __launch_bounds__(128) ghc_assemble_kernel(GHCArgs A) {
@@ -78,47 +111,44 @@ __global__ void __launch_bounds__(128) ghc_assemble_kernel(GHCArgs A) {
     int lhi = A.lag0 + A.nlag - 1;
     while (lhi >= A.lag0 && (lhi - 1) * A.velS * A.dt > distMax) lhi--;
     if (lhi < A.lag0) return;
-    const int klo = max(0, A.lag0 - 1), khi = lhi + 1;
     const double aS = A.geo[i].area, aF = A.geo[j].area;
-    double Km2[6] = {0, 0, 0, 0, 0, 0}, Km1[6] = {0, 0, 0, 0, 0, 0}, K[6];
+    const double cP = A.velP, cS = A.velS, dt = A.dt;
+    const double icP2 = 1 / (cP * cP), icS2 = 1 / (cS * cS);
     const size_t n3 = A.ld;
     const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
-    for (int k = klo; k <= khi; k++) {
-        const double t = A.dt * k;
-#pragma unroll
-        for (int e = 0; e < 6; e++) K[e] = 0.0;
+    for (int l = A.lag0; l <= lhi; l++) {
+        const double thi = (l + 1) * dt, tlo = (l - 1) * dt;
+        const double skipP2 = (cP * thi) * (cP * thi) * (1 + 1e-12);
+        const double skipS2 = (l >= 1) ? (cS * tlo) * (cS * tlo) * (1 - 1e-12) : -1.0;
+        double K[6] = {0, 0, 0, 0, 0, 0};
         for (int q = 0; q < A.n_sub * A.n_sing; q++) {
             const double* bq = A.inner + 3 * q;
             double y[3];
             for (int c = 0; c < 3; c++) y[c] = bq[0] * VF[0][c] + bq[1] * VF[1][c] + bq[2] * VF[2][c];
             const double wq = A.win[q % A.n_sing] * aF;
-            for (int l = 0; l < A.n_out; l++) {
-                const double* bl = A.outer + 3 * l;
+            for (int o = 0; o < A.n_out; o++) {
+                const double* bl = A.outer + 3 * o;
                 double x[3];
                 for (int c = 0; c < 3; c++) x[c] = y[c] - (bl[0] * VS[0][c] + bl[1] * VS[1][c] + bl[2] * VS[2][c]);
-                const double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
-                const double w = (A.wout[l] * aS) * wq;
+                const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+                if (r2 > skipP2 || r2 < skipS2) continue;
+                const double r = sqrt(r2);
+                const Win2 P = ghc_window2(r, cP, l, dt), S = ghc_window2(r, cS, l, dt);
+                const double w = (A.wout[o] * aS) * wq;
                 double nu[6];
-                nucleo_sym(nu, x, r, t, A.velP, A.velS);
+                ghc_pair(nu, x, 1 / r, P.H, S.H, P.Q - S.Q, icP2, icS2);
 #pragma unroll
                 for (int e = 0; e < 6; e++) K[e] += w * nu[e];
             }
         }
-        const int l = k - 1;               // lag completed by K_k
-        if (l >= A.lag0 && l <= lhi) {
-            double* base = A.E + (size_t)(l - A.lag0) * A.ld_lag + (3 * (size_t)j) * n3 + 3 * (size_t)i;
+        double* base = A.E + (size_t)(l - A.lag0) * A.ld_lag + (3 * (size_t)j) * n3 + 3 * (size_t)i;
 #pragma unroll
-            for (int c = 0; c < 3; c++)
+        for (int c = 0; c < 3; c++)
 #pragma unroll
-                for (int r = 0; r < 3; r++) {
-                    const int e = map[3 * c + r];
-                    const double prev = (l - 1 >= 0) ? Km2[e] : 0.0;
-                    const double v = (K[e] + (-2.0) * Km1[e]) + prev;
-                    if (fabs(v) > 1.0e-14) base[c * n3 + r] += v / A.c4pirho;
-                }
-        }
-#pragma unroll
-        for (int e = 0; e < 6; e++) { Km2[e] = Km1[e]; Km1[e] = K[e]; }
+            for (int r = 0; r < 3; r++) {
+                const double v = K[map[3 * c + r]];
+                if (fabs(v) > 1.0e-14) base[c * n3 + r] += v / A.c4pirho;
+            }
     }
 }
 
