@@ -12,6 +12,7 @@
 
 struct ebem_mesh {
     ebem::MeshData d;
+    double lo[3], hi[3];    // bounding box of the vertices (host side)
 };
 
 namespace ebem {
@@ -169,6 +170,13 @@ int ebem_mesh_create(const double* coords, int n_vertices, const int32_t* tris, 
     }
     if (int rc = check_device()) return rc;
     ebem_mesh* m = new ebem_mesh();
+    for (int c = 0; c < 3; c++) {
+        m->lo[c] = m->hi[c] = coords[c];
+        for (int v = 1; v < n_vertices; v++) {
+            m->lo[c] = std::min(m->lo[c], coords[3 * v + c]);
+            m->hi[c] = std::max(m->hi[c], coords[3 * v + c]);
+        }
+    }
     cudaGetDevice(&m->d.device);
     m->d.nv = n_vertices;
     m->d.nt = n_triangles;
@@ -386,7 +394,9 @@ int ebem_rhs(const ebem_mesh* m, const ebem_problem* p, int n_gh, int datum, dou
     if (!m || !rhs) return fail(EBEM_ERR_INVALID, "NULL mesh or output");
     if (int rc = check_problem(p)) return rc;
     if (n_gh != 3 && n_gh != 7 && n_gh != 12 && n_gh != 19) return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
-    if (datum < 0 || datum > 7) return fail(EBEM_ERR_INVALID, "unknown datum id (0..7)");
+    if (datum < 0 || datum > 8) return fail(EBEM_ERR_INVALID, "unknown datum id (0..8)");
+    if (datum == 8 && (m->lo[0] < -1 || m->hi[0] > 1 || m->lo[1] < -1 || m->hi[1] > 1 || m->lo[2] != 0 || m->hi[2] != 0))
+        return fail(EBEM_ERR_INVALID, "datum 8 (TEST) is defined on the screen [-1,1]^2 at z = 0");
     DeviceGuard dg(m->d.device);
     cudaStream_t s = (cudaStream_t)stream;
     MeshData& md = const_cast<MeshData&>(m->d);

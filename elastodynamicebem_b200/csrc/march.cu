@@ -68,7 +68,163 @@ __global__ void rhs_kernel(const NodeW* __restrict__ nodes, int N, int n_gh, int
     for (int c = 0; c < 3; c++) rhs[(size_t)n * 3 * N + 3 * t + c] = (fabs(ris[c]) < 1.0e-14) ? 0.0 : ris[c];
 }
 
+// ---------------------------------------------------------------------------
+// Datum 8, the reference's manufactured case 'TEST'
+// (BEMenerg_core_calcNucleoTn.m:13-132): the boundary value on the screen
+// [-1, 1]^2 (z = 0) whose solution is the constant density (1, 1, 1).  The
+// reference integrates nucl_1..3 over the square with integral2 for each pair
+// of instants (BEMenerg_core_TnTest_classic.m:11-13).  Regrouped by instant,
+// nucl_c = f_c(t1) - f_c(t0) with (r = |y - x|, c, s the direction cosines)
+//   f_1 = A c^2 + B (3 c^2 - 1) + S + c s (A + 3 B),
+//   f_2 = A s^2 + B (3 s^2 - 1) + S + c s (A + 3 B),   f_3 = S - B,
+//   A = J_P - J_S, B = I_P - I_S, S = J_S, J_v = H(t - r/v)/(v^2 r),
+//   I_v = H(t - r/v)(t^2 - r^2/v^2)/(2 r^3),
+// so F_c(x, t) = int f_c(t) dy / (4 pi rho) is computed per instant and the
+// right-hand side takes F(t1) - F(t0).  In polar coordinates about x the
+// radial integrals are closed forms (a = min(R, c_S t), b = min(R, c_P t)):
+//   int_0^R r A = b/c_P^2 - a/c_S^2,   int_0^R r S = a/c_S^2,
+//   int_0^R r B = (1/c_S^2 - 1/c_P^2) a/2 + t^2/2 (1/a - 1/b) - (b - a)/(2 c_P^2),
+// and the angle is integrated along each side of the square: with d the
+// distance of x from the side's line and u the signed position along it from
+// the foot of the perpendicular, R = sqrt(d^2 + u^2) and dtheta = d du / R^2.
+// The u-range is cut at the foot, at +-d 2^j (geometric grading: the
+// integrand's singularities sit at u = +-i d) and where r = c_S t or r = c_P t
+// crosses the side; 16-point Gauss-Legendre on each piece.
+__constant__ double c_gl16[2][16];      // 16-point Gauss-Legendre on (-1, 1): nodes, weights
+constexpr int kTestCuts = 64;
+
+__device__ void test_level(double x1, double x2, double t, double cP, double cS, double F[3]) {
+    F[0] = F[1] = F[2] = 0.0;
+    if (t <= 0) return;
+    const double iP2 = 1 / (cP * cP), iS2 = 1 / (cS * cS), rS = cS * t, rP = cP * t;
+    const double cx[4] = {-1, 1, 1, -1}, cy[4] = {-1, -1, 1, 1};
+    for (int k = 0; k < 4; k++) {
+        const double ax = cx[k] - x1, ay = cy[k] - x2;                 // corner k - x; the side runs to corner k+1
+        const double ex = 0.5 * (cx[(k + 1) & 3] - cx[k]), ey = 0.5 * (cy[(k + 1) & 3] - cy[k]);   // unit, length 2
+        const double s0 = -(ax * ex + ay * ey);                         // foot at corner + s0 e
+        const double fx = ax + s0 * ex, fy = ay + s0 * ey;              // foot - x, perpendicular to e
+        const double d = fx * ey - fy * ex;                             // > 0: the square runs counterclockwise about x
+        const double ulo = -s0, uhi = 2 - s0;
+        double cut[kTestCuts];
+        int nc = 0;
+        auto add = [&](double u) {
+            if (u > ulo && u < uhi && nc < kTestCuts - 1) cut[nc++] = u;
+        };
+        cut[nc++] = ulo;
+        add(0.0);
+        for (int q = 0; q < 2; q++) {
+            const double rho = q ? rP : rS;
+            if (rho > d) {
+                const double w = sqrt((rho - d) * (rho + d));
+                add(-w);
+                add(w);
+            }
+        }
+        const double umax = fmax(-ulo, uhi);
+        for (int j = 0; j < 26 && d * (double)(1 << j) < umax; j++) {
+            add(-d * (double)(1 << j));
+            add(d * (double)(1 << j));
+        }
+        cut[nc++] = uhi;
+        for (int i = 1; i < nc; i++)                                   // insertion sort
+            for (int j = i; j > 0 && cut[j] < cut[j - 1]; j--) {
+                const double tmp = cut[j];
+                cut[j] = cut[j - 1];
+                cut[j - 1] = tmp;
+            }
+        for (int q = 0; q + 1 < nc; q++) {
+            const double h = 0.5 * (cut[q + 1] - cut[q]), mid = 0.5 * (cut[q + 1] + cut[q]);
+            if (h <= 0) continue;
+            for (int ia = 0; ia < 16; ia++) {
+                const double u = mid + h * c_gl16[0][ia];
+                const double R2 = d * d + u * u, R = sqrt(R2);
+                const double w = h * c_gl16[1][ia] * d / R2;           // dtheta
+                const double cs = (fx + u * ex) / R, sn = (fy + u * ey) / R;
+                const double a = fmin(R, rS), b = fmin(R, rP);
+                const double RS = a * iS2, RA = b * iP2 - a * iS2;
+                double RB = 0.5 * (iS2 - iP2) * a;
+                if (b > a) RB += 0.5 * t * t * (1 / a - 1 / b) - 0.5 * (b - a) * iP2;
+                const double mixd = cs * sn * (RA + 3 * RB);
+                F[0] += w * (cs * cs * RA + (3 * cs * cs - 1) * RB + RS + mixd);
+                F[1] += w * (sn * sn * RA + (3 * sn * sn - 1) * RB + RS + mixd);
+                F[2] += w * (RS - RB);
+            }
+        }
+    }
+}
+
+// S_k[t] = sum_g w_g F(x_g, t_k) / (4 pi rho), k = 0..nT, one thread per (triangle, level).
+__global__ void rhs_test_level_kernel(const NodeW* __restrict__ nodes, int N, int n_gh, double dt, int nT, double cP,
+                                      double cS, double c4pirho, double* __restrict__ S) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)N * (nT + 1)) return;
+    const int t = (int)(idx % N), k = (int)(idx / N);
+    double acc[3] = {0, 0, 0};
+    for (int g = 0; g < n_gh; g++) {
+        const NodeW p = nodes[(size_t)t * n_gh + g];
+        double F[3];
+        test_level(p.x, p.y, dt * k, cP, cS, F);
+        for (int c = 0; c < 3; c++) acc[c] += F[c] * p.w;
+    }
+    for (int c = 0; c < 3; c++) S[((size_t)k * N + t) * 3 + c] = acc[c] / c4pirho;
+}
+
+// b_n = S_{n+1} - S_n, entries below 1e-14 set to 0 (BEMenerg_core_calcTnBlock.m:50-51).
+__global__ void rhs_test_diff_kernel(const double* __restrict__ S, int N, int nT, double* __restrict__ rhs) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 3LL * N * nT) return;
+    const int n = (int)(idx / (3LL * N));
+    const size_t e = (size_t)(idx % (3LL * N));
+    const double v = S[(size_t)(n + 1) * 3 * N + e] - S[(size_t)n * 3 * N + e];
+    rhs[idx] = (fabs(v) < 1.0e-14) ? 0.0 : v;
+}
+
+static void gauss_legendre16(double x[16], double w[16]) {
+    // Newton's iteration on P_16 from cos(pi (i + 3/4) / (n + 1/2)).
+    const int n = 16;
+    for (int i = 0; i < n; i++) {
+        double z = cos(kPi * (i + 0.75) / (n + 0.5)), dp = 1;
+        for (int it = 0; it < 100; it++) {
+            double p0 = 1, p1 = z;
+            for (int k = 2; k <= n; k++) {
+                const double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (z * p1 - p0) / (z * z - 1);
+            const double dz = p1 / dp;
+            z -= dz;
+            if (fabs(dz) < 1e-16) break;
+        }
+        x[i] = z;
+        w[i] = 2 / ((1 - z * z) * dp * dp);
+    }
+}
+
+static int launch_rhs_test(const MeshData& m, const PhysParams& P, int n_gh, double* d_rhs, cudaStream_t s) {
+    double gl[2][16];
+    gauss_legendre16(gl[0], gl[1]);
+    EBEM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_gl16, gl, sizeof gl, 0, cudaMemcpyHostToDevice, s));
+    double* d_S = nullptr;
+    const size_t nS = 3 * (size_t)m.nt * (P.nT + 1);
+    EBEM_CUDA_TRY(cudaMalloc(&d_S, nS * sizeof(double)));
+    const int threads = 128;
+    const long long lv = (long long)m.nt * (P.nT + 1), nb = 3LL * m.nt * P.nT;
+    rhs_test_level_kernel<<<(unsigned)((lv + threads - 1) / threads), threads, 0, s>>>(
+        m.d_nodes, m.nt, n_gh, P.dt, P.nT, P.velP, P.velS, 4 * kPi * P.rho, d_S);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        rhs_test_diff_kernel<<<(unsigned)((nb + threads - 1) / threads), threads, 0, s>>>(d_S, m.nt, P.nT, d_rhs);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_S);
+    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("TEST right-hand side: ") + cudaGetErrorString(e));
+    return EBEM_OK;
+}
+
 int launch_rhs(const MeshData& m, const PhysParams& P, int n_gh, int datum, double* d_rhs, cudaStream_t s) {
+    if (datum == 8) return launch_rhs_test(m, P, n_gh, d_rhs, s);
     long long total = (long long)m.nt * P.nT;
     int threads = 128;
     rhs_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, s>>>(m.d_nodes, m.nt, n_gh, datum, P.dt,

@@ -27,6 +27,7 @@ DATUM_BAR_H1 = 4            # 1-D bar closed form, h = 1            ('barH1')
 DATUM_BAR_H3 = 5            # 1-D bar closed form, h = 3            ('barH3')
 DATUM_SPHERE_WAVE = 6       # incident Gaussian pulse along x       ('sphereWave')
 DATUM_INDUSTRIAL = 7        # incident Gaussian pulse along z       ('elementoIndustriale')
+DATUM_TEST = 8              # manufactured: solution phi = (1, 1, 1) on [-1,1]^2 ('TEST')
 
 
 @dataclass

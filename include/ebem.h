@@ -228,7 +228,9 @@ int ebem_assemble_ghc(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh,
  * (f/BEMenerg_indir/BEMenerg_core/BEMenerg_core_calcTn/BEMenerg_core_calcTnBlock.m:1),
  * all steps at once.  datum selects g (f/.../BEMenerg_core_calcNucleoTn.m:196-244):
  * 0 (0,0,t^4 e^{-2t}), 1 x sin(2 pi t) H(t), 2 'sphereUniform', 3 'screenUniform',
- * 4 'barH1', 5 'barH3', 6 'sphereWave', 7 'elementoIndustriale'.
+ * 4 'barH1', 5 'barH3', 6 'sphereWave', 7 'elementoIndustriale', 8 'TEST' (the
+ * manufactured case of :13-132 whose solution is phi = (1, 1, 1), defined on
+ * the screen [-1,1]^2 at z = 0; other meshes are rejected).
  * rhs: 3N x nT column-major, host or device. */
 int ebem_rhs(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int datum, double* rhs, void* stream);
 

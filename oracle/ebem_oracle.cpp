@@ -12,6 +12,7 @@
 //                      SA/calcoloMatrice/BEMenerg_coreSA_calcMatrixSubBlock.m:1-111
 //   or_rhs             .../BEMenerg_core_calcTn/BEMenerg_core_calcTnBlock.m:1-63,
 //                      .../BEMenerg_core_calcTn/BEMenerg_core_calcNucleoTn.m:196-244
+//                      (datum 8 'TEST', :13-132, in test_datum_oracle.cpp)
 //   or_march           .../BEMenerg_coreGPU/BEMenerg_coreGPU_timeMarching.m:151-169
 //   or_pp_sa           .../BEMenerg_postProc/BEMenerg_postProcA/*.m
 //   or_assemble_ghc    .../BEMenerg_coreGPU/CUDAkernels/kernelGHC.cu:5-259
@@ -435,7 +436,12 @@ int or_assemble_sa_pairs(const double* coords, int nv, const int* tris, int nt,
     return 0;
 }
 
-// Right-hand side b_n, n = 0..nT-1, column-major 3N x nT.
+int or_tn_test(double x1, double x2, double t0, double t1, double rho, double mu, double lambda, int nang, int nsplit,
+               int nrad, double* out);
+
+// Right-hand side b_n, n = 0..nT-1, column-major 3N x nT.  Datum 8 is the
+// reference's 'TEST' case, whose value is computed for the pair of instants
+// at once (BEMenerg_core_calcNucleoTn(pbParam, puntoT, t0, t1)).
 int or_rhs(const double* coords, int nv, const int* tris, int nt,
            double rho, double mu, double lambda, double dt, int nT, int nGH, int datum_id, double* rhs) {
     BaseRule R = composite1(nGH);
@@ -451,8 +457,13 @@ int or_rhs(const double* coords, int nv, const int* tris, int nt,
             for (int g = 0; g < nGH; g++) {
                 const double* x = &tc[t].nodes[3 * g];
                 double g1[3], g0[3];
-                datum(datum_id, p, Tfin, x, tFin, g1);
-                datum(datum_id, p, Tfin, x, tInz, g0);
+                if (datum_id == 8) {
+                    if (or_tn_test(x[0], x[1], tInz, tFin, rho, mu, lambda, 24, 4, 24, g1)) return -1;
+                    g0[0] = g0[1] = g0[2] = 0;
+                } else {
+                    datum(datum_id, p, Tfin, x, tFin, g1);
+                    datum(datum_id, p, Tfin, x, tInz, g0);
+                }
                 for (int c = 0; c < 3; c++) ris[c] = ris[c] + (g1[c] - g0[c]) * tc[t].w[g];
             }
             for (int c = 0; c < 3; c++) {

@@ -47,6 +47,7 @@ def lib(variant: str = "f64"):
         L.or_assemble_sa.restype = C.c_longlong
         L.or_assemble_sa_pairs.argtypes = mesh_args + par + [C.c_int, C.c_int, _ip, _ip, _ip, _dp, C.c_int]
         L.or_rhs.argtypes = mesh_args + par + [C.c_int, C.c_int, _dp]
+        L.or_tn_test.argtypes = [C.c_double] * 7 + [C.c_int] * 3 + [_dp]
         L.or_march.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, _dp]
         L.or_pp_sa.argtypes = mesh_args + par + [_dp, _dp, C.c_int, _dp, C.c_int, _dp, C.c_int]
         L.or_assemble_ghc.argtypes = mesh_args + par + [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_int]
@@ -114,6 +115,15 @@ def rhs(mesh, prm, n_gh: int, datum_id: int, variant: str = "f64"):
     b = np.zeros(n3 * prm.nT)
     lib(variant).or_rhs(*_m(mesh), *_p(prm), n_gh, datum_id, b)
     return b.reshape(prm.nT, n3).T.copy()        # (3N, nT)
+
+
+def tn_test(x1: float, x2: float, t0: float, t1: float, prm, nang: int = 24, nsplit: int = 4, nrad: int = 24):
+    """The reference's manufactured 'TEST' boundary value at (x1, x2) for the
+    instants (t0, t1) (BEMenerg_core_calcNucleoTn.m:13-132), length 3."""
+    out = np.zeros(3)
+    if lib().or_tn_test(x1, x2, t0, t1, prm.rho, prm.mu, prm.lam, nang, nsplit, nrad, out):
+        raise ValueError("TEST datum: point outside the screen or bad rule")
+    return out
 
 
 def march(E, b):
