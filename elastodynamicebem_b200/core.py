@@ -161,6 +161,47 @@ def march(E: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None, str
     return out
 
 
+class DeviceLU:
+    """LU factors of the device matrix A[row, col] (ebem_lu_create), kept on
+    the device; ``solve`` overwrites contiguous device right-hand sides (one
+    per row of ``b``) with A^{-1} b."""
+
+    def __init__(self, A: torch.Tensor, stream=None):
+        if A.dim() != 2 or A.shape[0] != A.shape[1] or not A.is_cuda:
+            raise ValueError("A must be a square device matrix")
+        self.n = int(A.shape[0])
+        Acm = A.t().contiguous()                    # column-major storage of A
+        self._h = C.c_void_p()
+        _lib.check(_lib.load().ebem_lu_create(_ptr(Acm), self.n, _stream_ptr(stream), C.byref(self._h)))
+
+    def solve(self, b: torch.Tensor, stream=None) -> torch.Tensor:
+        if not b.is_contiguous() or b.numel() % self.n:
+            raise ValueError("b must be contiguous with a multiple of n elements")
+        _lib.check(_lib.load().ebem_lu_solve(self._h, _ptr(b), b.numel() // self.n, _stream_ptr(stream)))
+        return b
+
+    def close(self):
+        if self._h:
+            _lib.load().ebem_lu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def history_gemv(A: torch.Tensor, rows: int, x: torch.Tensor, y: torch.Tensor, stream=None) -> torch.Tensor:
+    """y -= A x with A the contiguous column-major storage of a rows x K
+    matrix (e.g. lags 1..M of a source-row panel), x (K), y (rows)."""
+    K = A.numel() // rows
+    if A.numel() != rows * K or x.numel() != K or y.numel() != rows:
+        raise ValueError("shape mismatch")
+    _lib.check(_lib.load().ebem_history_gemv(_ptr(A), int(rows), int(K), _ptr(x), _ptr(y), _stream_ptr(stream)))
+    return y
+
+
 def timemarch_sa(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, datum: int, out: torch.Tensor | None = None,
                  stream=None, prec: int = PREC_FP64):
     """BEMenerg_coreSA_timeMarching: assembly + right-hand side + marching.

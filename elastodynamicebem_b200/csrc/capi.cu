@@ -421,6 +421,53 @@ int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double
     return out.finish(s);
 }
 
+struct ebem_lu {
+    LuPlan plan;
+    int device = 0;
+};
+
+int ebem_lu_create(const double* A, int n, void* stream, ebem_lu** out) {
+    if (!out) return fail(EBEM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!A || n < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
+    if (int rc = check_device()) return rc;
+    if (!is_device_ptr(A)) return fail(EBEM_ERR_INVALID, "the matrix must be in device memory");
+    ebem_lu* lu = new ebem_lu();
+    cudaGetDevice(&lu->device);
+    if (int rc = lu_plan_create(A, n, (cudaStream_t)stream, &lu->plan)) {
+        lu_plan_destroy(&lu->plan);
+        delete lu;
+        return rc;
+    }
+    *out = lu;
+    return EBEM_OK;
+}
+
+int ebem_lu_solve(ebem_lu* lu, double* b, int nrhs, void* stream) {
+    if (!lu || !b || nrhs < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
+    DeviceGuard dg(lu->device);
+    if (!is_device_ptr(b)) return fail(EBEM_ERR_INVALID, "the right-hand side must be in device memory");
+    return lu_plan_solve(&lu->plan, b, nrhs, (cudaStream_t)stream);
+}
+
+void ebem_lu_destroy(ebem_lu* lu) {
+    if (!lu) return;
+    DeviceGuard dg(lu->device);
+    lu_plan_destroy(&lu->plan);
+    delete lu;
+}
+
+int ebem_history_gemv(const double* A, int rows, long long K, const double* x, double* y, void* stream) {
+    if (!A || !x || !y || rows < 1 || K < 0) return fail(EBEM_ERR_INVALID, "bad arguments");
+    if (int rc = check_device()) return rc;
+    if (!is_device_ptr(A) || !is_device_ptr(x) || !is_device_ptr(y))
+        return fail(EBEM_ERR_INVALID, "A, x and y must be in device memory");
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return launch_hist_gemv(A, rows, K, x, y, sms, (cudaStream_t)stream);
+}
+
 static int timemarch_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, int datum, double* phi, int* num_blocks,
                           void* stream, int prec);
 

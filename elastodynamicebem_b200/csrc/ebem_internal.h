@@ -9,6 +9,8 @@
 #include "../../include/ebem.h"
 #include "sa_device.cuh"
 
+struct cusolverDnContext;   // cuSOLVER dense handle (cusolverDnHandle_t)
+
 namespace ebem { struct NodeW; }
 
 namespace ebem {
@@ -87,6 +89,17 @@ int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_
 
 int launch_rhs(const MeshData& m, const PhysParams& P, int n_gh, int datum, double* d_rhs, cudaStream_t s);
 int march_device(const double* dE, int n3, int L, const double* drhs, int nT, double* dphi, cudaStream_t s);
+// Device LU factors of one n x n matrix (cuSOLVER getrf once, getrs per solve).
+struct LuPlan {
+    int n = 0;
+    double* lu = nullptr;
+    int* ipiv = nullptr;
+    int* info = nullptr;
+    ::cusolverDnContext* h = nullptr;
+};
+int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan);
+int lu_plan_solve(LuPlan* plan, double* db, int nrhs, cudaStream_t s);
+void lu_plan_destroy(LuPlan* plan);
 int launch_pp_sa(const MeshData& m, const PhysParams& P, const double* d_phi, const double* d_pts, int npts,
                  const double* h_times, int ntimes, double* d_u, cudaStream_t s);
 

@@ -382,6 +382,63 @@ done:
 }
 
 // ---------------------------------------------------------------------------
+// LU factors of one matrix kept on the device (the E_0 factorisation of the
+// marching, for callers that drive the steps themselves).
+int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan) {
+    int rc = EBEM_OK;
+    int lwork = 0, hinfo = 0;
+    double* work = nullptr;
+    const size_t nn = (size_t)n * n;
+    plan->n = n;
+    if (cudaMalloc(&plan->lu, nn * sizeof(double)) != cudaSuccess || cudaMalloc(&plan->ipiv, n * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&plan->info, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(EBEM_ERR_NOMEM, "LU allocation failed");
+    }
+    CUSOLVER_TRY(cusolverDnCreate(&plan->h));
+    CUSOLVER_TRY(cusolverDnSetStream(plan->h, s));
+    if (cudaMemcpyAsync(plan->lu, dA, nn * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        rc = fail(EBEM_ERR_CUDA, "matrix copy failed");
+        goto done;
+    }
+    CUSOLVER_TRY(cusolverDnDgetrf_bufferSize(plan->h, n, n, plan->lu, n, &lwork));
+    if (cudaMalloc(&work, (size_t)(lwork > 0 ? lwork : 1) * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(EBEM_ERR_NOMEM, "LU workspace allocation failed");
+        goto done;
+    }
+    CUSOLVER_TRY(cusolverDnDgetrf(plan->h, n, n, plan->lu, n, work, plan->ipiv, plan->info));
+    if (cudaMemcpyAsync(&hinfo, plan->info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        rc = fail(EBEM_ERR_CUDA, "LU factorisation failed");
+        goto done;
+    }
+    if (hinfo != 0) rc = fail(EBEM_ERR_SINGULAR, "matrix is singular (zero pivot " + std::to_string(hinfo) + ")");
+done:
+    if (work) cudaFree(work);
+    return rc;
+}
+
+int lu_plan_solve(LuPlan* plan, double* db, int nrhs, cudaStream_t s) {
+    int rc = EBEM_OK;
+    CUSOLVER_TRY(cusolverDnSetStream(plan->h, s));
+    CUSOLVER_TRY(cusolverDnDgetrs(plan->h, CUBLAS_OP_N, plan->n, nrhs, plan->lu, plan->n, plan->ipiv, db, plan->n,
+                                  plan->info));
+done:
+    return rc;
+}
+
+void lu_plan_destroy(LuPlan* plan) {
+    if (plan->h) cusolverDnDestroy(plan->h);
+    if (plan->lu) cudaFree(plan->lu);
+    if (plan->ipiv) cudaFree(plan->ipiv);
+    if (plan->info) cudaFree(plan->info);
+    plan->h = nullptr;
+    plan->lu = nullptr;
+    plan->ipiv = plan->info = nullptr;
+}
+
+// ---------------------------------------------------------------------------
 // Post-processing (closed form): u(x, t) = sum_{k=1}^{nHat} (M(t - (k-1) dt)
 // - M(t - k dt)) phi_k + M(t - nHat dt) phi_{nHat+1}, nHat = ceil(t/dt) - 1,
 // M(tau) the single-point combined kernel integral over each triangle

@@ -44,6 +44,10 @@ PROTOTYPES = {
                                     C.c_void_p, C.c_int, C.c_void_p]),
     "ebem_rhs": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ebem_march": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "ebem_lu_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "ebem_lu_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "ebem_lu_destroy": (None, [C.c_void_p]),
+    "ebem_history_gemv": (C.c_int, [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ebem_timemarch_sa": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_void_p,
                                     C.POINTER(C.c_int), C.c_void_p]),
     "ebem_pp_sa": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,

@@ -242,6 +242,31 @@ int ebem_rhs(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int datu
  * Returns EBEM_ERR_SINGULAR when E_0 has a zero pivot. */
 int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double* phi, void* stream);
 
+/* Pieces of ebem_march for callers that drive the steps themselves (the
+ * row-panel marching across ranks, where each rank holds the rows
+ * [r0, r0 + rows) of every E_l and one all-gather per step assembles the
+ * right-hand side).
+ *
+ * ebem_lu_create: LU factors (partial pivoting) of the device matrix A
+ * (column-major n x n), kept on the device; replaces
+ * [L, U, P] = lu(sparse(matrix)) of
+ * f/BEMenerg_indir/BEMenerg_core/BEMenerg_coreSA/BEMenerg_coreSA_timeMarching.m:46
+ * (BEMenerg_coreGPU_timeMarching.m:153).  Returns EBEM_ERR_SINGULAR on a
+ * zero pivot.  ebem_lu_solve overwrites the device columns b (n x nrhs) with
+ * A^{-1} b (U\(L\(P*b)), :59).  ebem_lu_destroy frees the factors.
+ *
+ * ebem_history_gemv: y -= A x for device A (rows x K, column-major, leading
+ * dimension rows), x (K) and y (rows): the history sum
+ * tnf = tnf - matrixSaved{indMat} * density(:, currInd - indMat + 1) of
+ * BEMenerg_coreGPU_timeMarching.m:160-166 for all lags at once when A is
+ * [E_1 E_2 ... E_M] restricted to a row panel and x = (phi_{n-1}; ...;
+ * phi_{n-M}). */
+typedef struct ebem_lu ebem_lu;
+int ebem_lu_create(const double* A, int n, void* stream, ebem_lu** out);
+int ebem_lu_solve(ebem_lu* lu, double* b, int nrhs, void* stream);
+void ebem_lu_destroy(ebem_lu* lu);
+int ebem_history_gemv(const double* A, int rows, long long K, const double* x, double* y, void* stream);
+
 /* The semi-analytic indirect solve end to end: assembly of E_0..E_{L-1}
  * (L from ebem_num_blocks), right-hand side, time marching.  Replaces
  * density = BEMenerg_coreSA_timeMarching(pbParam, domainMesh, methodInfo, GHn, GHw)

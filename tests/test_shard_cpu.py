@@ -66,3 +66,66 @@ def test_two_rank_gather_reproduces_full(tmp_path):
     full = O.assemble_sa(m, prm, 7, 0, O.num_blocks(m, prm), nthreads=1)[0]
     assert np.array_equal(E, full)
     assert cnt == cfull and tmax == 2.0
+
+
+def _panel_raw(full, src0, nsrc):
+    """This rank's rows of E_l[row, col] in the panel buffer layout
+    (L, 3N, 3 nsrc): column-major per lag, leading dimension 3 nsrc."""
+    import torch
+    return torch.tensor(full[:, 3 * src0:3 * (src0 + nsrc), :]).transpose(1, 2).contiguous()
+
+
+def _march_worker(rank, world, port, out):
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import torch
+    import torch.distributed as dist
+    import oracle as O
+    from elastodynamicebem_b200 import mesh, problem, shard
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    m, prm = mesh.screen_uniform(3), problem.ProblemParams(1.0, 1.0, 2.0, 1.0, 10)
+    N = m.numberTriangles
+    L = O.num_blocks(m, prm)
+    full = O.assemble_sa(m, prm, 7, 0, L, nthreads=1)[0]
+    b = torch.tensor(O.rhs(m, prm, 7, problem.DATUM_SCREEN_T4EXP).T.copy())       # (nT, 3N)
+    src0, nsrc = shard.row_panel(rank, world, N)
+    phi = shard.march_panels(_panel_raw(full, src0, nsrc), b, N, world, rank, ops=shard.HostOps())
+    np.save(out + f".{rank}.npy", phi.numpy())
+    dist.destroy_process_group()
+
+
+def test_two_rank_panel_marching(tmp_path):
+    """Marching on two ranks' row panels (one all-gather of the history per
+    step) reproduces the oracle's serial marching on both ranks."""
+    import socket
+    import torch.multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from elastodynamicebem_b200 import mesh, problem
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = str(tmp_path / "phi")
+    mp.start_processes(_march_worker, args=(2, port, out), nprocs=2, start_method="spawn", join=True)
+    m, prm = mesh.screen_uniform(3), problem.ProblemParams(1.0, 1.0, 2.0, 1.0, 10)
+    L = O.num_blocks(m, prm)
+    full = O.assemble_sa(m, prm, 7, 0, L, nthreads=1)[0]
+    ref = O.march(full, O.rhs(m, prm, 7, problem.DATUM_SCREEN_T4EXP)).T            # (nT, 3N)
+    for r in range(2):
+        phi = np.load(out + f".{r}.npy")
+        assert np.linalg.norm(phi - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+def test_single_rank_panel_marching():
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from elastodynamicebem_b200 import mesh, problem, shard
+    m, prm = mesh.screen_uniform(2), problem.ProblemParams(1.0, 1.0, 2.0, 1.0, 8)
+    N = m.numberTriangles
+    L = O.num_blocks(m, prm)
+    full = O.assemble_sa(m, prm, 7, 0, L, nthreads=1)[0]
+    b = O.rhs(m, prm, 7, problem.DATUM_SCREEN_T4EXP)
+    phi = shard.march_panels(_panel_raw(full, 0, N), torch.tensor(b.T.copy()), N, 1, 0, ops=shard.HostOps())
+    ref = O.march(full, b).T
+    assert np.linalg.norm(phi.numpy() - ref) <= 1e-12 * np.linalg.norm(ref)
