@@ -161,6 +161,53 @@ def march(E: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None, str
     return out
 
 
+class BandedOperator:
+    """E_0..E_{L-1} of the semi-analytic method in banded storage on the
+    device (ebem_banded_*): per (source, field) pair only its band of non-null
+    lags, 6 symmetric entries per block."""
+
+    def __init__(self, dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, prec: int = PREC_FP64, stream=None):
+        self.dmesh, self.prm = dmesh, prm
+        self._h = C.c_void_p()
+        p = _lib.problem_struct(prm)
+        _lib.check(_lib.load().ebem_banded_assemble(dmesh.handle, C.byref(p), int(n_gh), int(prec),
+                                                    _stream_ptr(stream), C.byref(self._h)))
+
+    def info(self) -> dict:
+        n, L, nn, by = C.c_int(), C.c_int(), C.c_longlong(), C.c_longlong()
+        _lib.check(_lib.load().ebem_banded_info(self._h, C.byref(n), C.byref(L), C.byref(nn), C.byref(by)))
+        return {"N": n.value, "L": L.value, "nonnull": nn.value, "bytes": by.value}
+
+    def to_dense(self, lag0: int = 0, nlag: int | None = None, stream=None) -> torch.Tensor:
+        """E[l][row, col], as assemble_sa returns it."""
+        L = self.info()["L"]
+        nlag = L - lag0 if nlag is None else nlag
+        n3 = 3 * self.dmesh.N
+        out = torch.empty((nlag, n3, n3), dtype=torch.float64, device="cuda")
+        _lib.check(_lib.load().ebem_banded_to_dense(self._h, int(lag0), int(nlag), _ptr(out), _stream_ptr(stream)))
+        return out.transpose(1, 2)
+
+    def march(self, b: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """Density phi (nT, 3N) from the right-hand side b (nT, 3N)."""
+        nT, n3 = b.shape
+        if out is None:
+            out = torch.empty((nT, n3), dtype=torch.float64, device=b.device)
+        _lib.check(_lib.load().ebem_banded_march(self._h, _ptr(b.contiguous()), int(nT), _ptr(out),
+                                                 _stream_ptr(stream) if out.is_cuda else None))
+        return out
+
+    def close(self):
+        if self._h:
+            _lib.load().ebem_banded_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class DeviceLU:
     """LU factors of the device matrix A[row, col] (ebem_lu_create), kept on
     the device; ``solve`` overwrites contiguous device right-hand sides (one

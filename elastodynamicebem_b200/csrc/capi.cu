@@ -421,6 +421,85 @@ int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double
     return out.finish(s);
 }
 
+struct ebem_banded {
+    BandOp op;
+    int device = 0;
+};
+
+int ebem_banded_assemble(const ebem_mesh* m, const ebem_problem* p, int n_gh, int prec, void* stream,
+                         ebem_banded** out) {
+    if (!out) return fail(EBEM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!m) return fail(EBEM_ERR_INVALID, "mesh is NULL");
+    if (int rc = check_problem(p)) return rc;
+    if (n_gh != 3 && n_gh != 7 && n_gh != 12 && n_gh != 19)
+        return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+    if (prec != EBEM_PREC_FP64 && prec != EBEM_PREC_MIXED) return fail(EBEM_ERR_INVALID, "unknown precision mode");
+    int L = 0;
+    if (int rc = ebem_num_blocks(m, p, &L)) return rc;
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    MeshData& md = const_cast<MeshData&>(m->d);
+    if (int rc = map_nodes(md, n_gh, s)) return rc;
+    PhysParams P = phys_from(p);
+    ebem_banded* b = new ebem_banded();
+    b->device = m->d.device;
+    int rc = band_structure(md, P, L, &b->op, s);
+    if (!rc) rc = launch_sa_assemble_banded(md, P, n_gh, L, b->op.Eb, b->op.off, b->op.lo, prec == EBEM_PREC_MIXED, s);
+    if (!rc && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(EBEM_ERR_CUDA, "banded assembly failed");
+    if (rc) {
+        band_free(&b->op);
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return EBEM_OK;
+}
+
+int ebem_banded_info(const ebem_banded* b, int* n_triangles, int* num_blocks, long long* nonnull, long long* bytes) {
+    if (!b) return fail(EBEM_ERR_INVALID, "NULL operator");
+    if (n_triangles) *n_triangles = b->op.N;
+    if (num_blocks) *num_blocks = b->op.L;
+    if (nonnull) *nonnull = b->op.nblocks;
+    if (bytes) {
+        const long long NN = (long long)b->op.N * b->op.N;
+        *bytes = b->op.nblocks * 48 + (NN + 1) * 8 + NN * 4;
+    }
+    return EBEM_OK;
+}
+
+int ebem_banded_to_dense(const ebem_banded* b, int lag0, int nlag, double* E, void* stream) {
+    if (!b || !E) return fail(EBEM_ERR_INVALID, "NULL argument");
+    if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
+    DeviceGuard dg(b->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t n3 = 3 * (size_t)b->op.N;
+    DevOut out;
+    if (int rc = out.init(E, n3 * n3 * nlag)) return rc;
+    if (int rc = band_to_dense(b->op, lag0, nlag, out.d, s)) return rc;
+    return out.finish(s);
+}
+
+int ebem_banded_march(const ebem_banded* b, const double* rhs, int nT, double* phi, void* stream) {
+    if (!b || !rhs || !phi || nT < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
+    DeviceGuard dg(b->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t n3 = 3 * (size_t)b->op.N;
+    DevIn dr;
+    if (int rc = dr.init(rhs, n3 * nT, s)) return rc;
+    DevOut out;
+    if (int rc = out.init(phi, n3 * nT)) return rc;
+    if (int rc = band_march(b->op, dr.d, nT, out.d, s)) return rc;
+    return out.finish(s);
+}
+
+void ebem_banded_destroy(ebem_banded* b) {
+    if (!b) return;
+    DeviceGuard dg(b->device);
+    band_free(&b->op);
+    delete b;
+}
+
 struct ebem_lu {
     LuPlan plan;
     int device = 0;

@@ -97,6 +97,22 @@ struct LuPlan {
     int* info = nullptr;
     ::cusolverDnContext* h = nullptr;
 };
+// Banded Toeplitz blocks (csrc/banded.cu): pair p = i N + j owns the blocks
+// [off[p], off[p+1]) of Eb, one per lag of its band starting at lo[p], the 6
+// symmetric entries (11,12,13,22,23,33) of each.
+struct BandOp {
+    int N = 0, L = 0;
+    long long nblocks = 0;
+    double* Eb = nullptr;
+    long long* off = nullptr;
+    int* lo = nullptr;
+};
+int band_structure(const MeshData& m, const PhysParams& P, int L, BandOp* op, cudaStream_t s);
+void band_free(BandOp* op);
+int band_to_dense(const BandOp& op, int lag0, int nlag, double* d_E, cudaStream_t s);
+int band_march(const BandOp& op, const double* d_rhs, int nT, double* d_phi, cudaStream_t s);
+int launch_sa_assemble_banded(const MeshData& m, const PhysParams& P, int n_gh, int L, double* d_Eb,
+                              const long long* d_boff, const int* d_blo, int mixed, cudaStream_t s);
 int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan);
 int lu_plan_solve(LuPlan* plan, double* db, int nrhs, cudaStream_t s);
 void lu_plan_destroy(LuPlan* plan);

@@ -116,6 +116,12 @@ struct SAArgs {
     unsigned long long* count;
     const int2* pairs;      // optional explicit (source, field) list (npairs entries)
     long long npairs;
+    // banded output (instead of E): pair p = (i - src0) N + j owns the blocks
+    // [boff[p], boff[p+1]) of Eb, one per lag of its band starting at blo[p],
+    // 6 symmetric entries (11,12,13,22,23,33) each
+    double* Eb = nullptr;
+    const long long* boff = nullptr;
+    const int* blo = nullptr;
 };
 
 __device__ __forceinline__ void store_block(const SAArgs& A, int q, int i, int j, const double b[6]) {
@@ -207,20 +213,22 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
     const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
     const TriGeom& F = A.geo[j];
     const TriGeom& Sg = A.geo[i];
-    double v0 = F.ctr[0] - Sg.ctr[0], v1 = F.ctr[1] - Sg.ctr[1], v2 = F.ctr[2] - Sg.ctr[2];
-    double d = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-    double distMin = d - F.maxL - Sg.maxL;
-    double distMax = d + F.maxL + Sg.maxL;
     int llo = -1, lhi = -2;
-    for (int q = 0; q < A.nlag; q++) {
-        int l = A.lag0 + q;
-        if (lag_nonnull(l, A.velP, A.velS, A.dt, distMin, distMax)) {
-            if (llo < 0) llo = l;
-            lhi = l;
+    long long bbase = 0;
+    if (A.Eb) {
+        // the band comes from the structure pass, so writes stay in the pair's blocks
+        const long long p = (long long)(i - A.src0) * A.N + j;
+        bbase = A.boff[p];
+        const int nb = (int)(A.boff[p + 1] - bbase);
+        if (nb > 0) {
+            llo = A.blo[p];
+            lhi = llo + nb - 1;
         }
+    } else {
+        pair_band(F, Sg, A.velP, A.velS, A.dt, A.lag0, A.nlag, &llo, &lhi);
     }
     if (lane == 0 && llo >= 0) my_count += (unsigned long long)(lhi - llo + 1);
-    if (!A.accumulate) {
+    if (!A.accumulate && !A.Eb) {
         for (int idx = lane; idx < A.nlag * 9; idx += 32) {
             const int q = idx / 9, e = idx - 9 * q, l = A.lag0 + q;
             if (llo < 0 || l < llo || l > lhi) store_entry(A, q, i, j, e, 0.0);
@@ -463,7 +471,13 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
             Fk[5] = 0.5 * (S + Rm[2][2]);
         }
         const int l = k - 1;
-        if (l >= llo && l <= lhi && lane < 9) {
+        if (A.Eb) {
+            if (l >= llo && l <= lhi && lane < 6) {
+                double prev = (l - 1 >= 1) ? Fm2[lane] : 0.0;
+                double v = ((Fk[lane] + (-2.0) * Fm1[lane]) + prev) / A.c4pirho;
+                A.Eb[(bbase + (l - llo)) * 6 + lane] = (fabs(v) < 1.0e-14) ? 0.0 : v;
+            }
+        } else if (l >= llo && l <= lhi && lane < 9) {
             const int e = map[lane];
             double prev = (l - 1 >= 1) ? Fm2[e] : 0.0;
             double v = ((Fk[e] + (-2.0) * Fm1[e]) + prev) / A.c4pirho;
@@ -566,6 +580,41 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
     sa_assemble_kernel<<<(unsigned)blocks, threads, 0, s>>>(A);
     EBEM_CUDA_TRY(cudaGetLastError());
     return EBEM_OK;
+}
+
+// Banded output: all lags [0, L) of every pair, written into the band
+// layout that band_structure() built (only the warp kernel has this mode).
+int launch_sa_assemble_banded(const MeshData& m, const PhysParams& P, int n_gh, int L, double* d_Eb,
+                              const long long* d_boff, const int* d_blo, int mixed, cudaStream_t s) {
+    SAArgs A;
+    A.geo = m.d_geo;
+    A.nodes = m.d_nodes;
+    A.N = m.nt;
+    A.n_gh = n_gh;
+    A.velP = P.velP;
+    A.velS = P.velS;
+    A.dt = P.dt;
+    A.c4pirho = 4 * kPi * P.rho;
+    A.lag0 = 0;
+    A.nlag = L;
+    A.src0 = 0;
+    A.nsrc = m.nt;
+    A.diag_only = 0;
+    A.E = nullptr;
+    A.ld = 0;
+    A.ld_lag = 0;
+    A.accumulate = 0;
+    A.count = nullptr;
+    A.pairs = nullptr;
+    A.npairs = 0;
+    A.Eb = d_Eb;
+    A.boff = d_boff;
+    A.blo = d_blo;
+    const long long NN = (long long)m.nt * m.nt;
+    if (3 * n_gh <= 32)
+        return mixed ? launch_warp<1, 4, EBEM_WARP_MINB, true>(A, NN, m.device, s)
+                     : launch_warp<1, 4, EBEM_WARP_MINB, false>(A, NN, m.device, s);
+    return mixed ? launch_warp<2, 2, 4, true>(A, NN, m.device, s) : launch_warp<2, 2, 4, false>(A, NN, m.device, s);
 }
 
 // ---------------------------------------------------------------------------

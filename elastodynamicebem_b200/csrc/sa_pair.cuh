@@ -211,6 +211,26 @@ EBEM_DI bool lag_nonnull(int l, double velP, double velS, double dt, double dist
     return ((l - 1) * velS * dt < distMax) && ((l + 1) * velP * dt >= distMin);
 }
 
+// The non-null lags of the pair (source S, field F) within [lag0, lag0 + nlag):
+// the null test is monotone in the lag, so they form one band [*llo, *lhi]
+// (*llo = -1 when empty).
+EBEM_DI void pair_band(const TriGeom& F, const TriGeom& S, double velP, double velS, double dt, int lag0, int nlag,
+                       int* llo, int* lhi) {
+    const double v0 = F.ctr[0] - S.ctr[0], v1 = F.ctr[1] - S.ctr[1], v2 = F.ctr[2] - S.ctr[2];
+    const double d = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+    const double distMin = d - F.maxL - S.maxL;
+    const double distMax = d + F.maxL + S.maxL;
+    *llo = -1;
+    *lhi = -2;
+    for (int q = 0; q < nlag; q++) {
+        const int l = lag0 + q;
+        if (lag_nonnull(l, velP, velS, dt, distMin, distMax)) {
+            if (*llo < 0) *llo = l;
+            *lhi = l;
+        }
+    }
+}
+
 // F(t_k) for one pair: sum over the outer nodes of the source triangle of the
 // weighted closed-form inner integrals, combined (calcMatrixSubBlock.m:101-104)
 // and rotated back to global axes; 6 symmetric entries (11,12,13,22,23,33).

@@ -44,6 +44,13 @@ PROTOTYPES = {
                                     C.c_void_p, C.c_int, C.c_void_p]),
     "ebem_rhs": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ebem_march": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "ebem_banded_assemble": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_void_p,
+                                       C.POINTER(C.c_void_p)]),
+    "ebem_banded_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong),
+                                   C.POINTER(C.c_longlong)]),
+    "ebem_banded_to_dense": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "ebem_banded_march": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "ebem_banded_destroy": (None, [C.c_void_p]),
     "ebem_lu_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     "ebem_lu_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "ebem_lu_destroy": (None, [C.c_void_p]),

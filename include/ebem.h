@@ -261,6 +261,34 @@ int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double
  * BEMenerg_coreGPU_timeMarching.m:160-166 for all lags at once when A is
  * [E_1 E_2 ... E_M] restricted to a row panel and x = (phi_{n-1}; ...;
  * phi_{n-M}). */
+/* Banded (block-sparse) Toeplitz blocks and the marching on them.  The
+ * reference keeps every E_l dense (matrixSaved{l},
+ * f/BEMenerg_indir/BEMenerg_core/BEMenerg_coreGPU/BEMenerg_coreGPU_timeMarching.m:139-147;
+ * one .mat file per block in BEMenerg_coreSA_timeMarching.m:96-99), although
+ * a (source, field) block is zero outside the lags that pass the null test of
+ * BEMenerg_coreSA_calcMatrixBlock.m:57-61.  That test is monotone in the lag,
+ * so each pair's non-null lags form one band, and the blocks are symmetric:
+ * this storage keeps 6 doubles per non-null pair-lag (plus 12 bytes per pair
+ * of structure) instead of 9 doubles per pair and lag.
+ *
+ * ebem_banded_assemble: E_0..E_{L-1} (L from ebem_num_blocks) by the
+ * semi-analytic method, FP64 or EBEM_PREC_MIXED, into a device-resident
+ * operator; the values equal those of ebem_assemble_sa.
+ * ebem_banded_info: triangles, L, non-null pair-lags and device bytes held.
+ * ebem_banded_to_dense: E_lag0..E_{lag0+nlag-1} in the layout of
+ * ebem_assemble_sa (host or device).
+ * ebem_banded_march: the marching of ebem_march (LU of E_0 once, history
+ * sum_{l>=1} E_l phi_{n-l} per step) on the banded blocks; rhs and phi
+ * 3N x nT, host or device.
+ * No counterpart in the reference beyond the dense equivalents cited. */
+typedef struct ebem_banded ebem_banded;
+int ebem_banded_assemble(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int prec, void* stream,
+                         ebem_banded** out);
+int ebem_banded_info(const ebem_banded* op, int* n_triangles, int* num_blocks, long long* nonnull, long long* bytes);
+int ebem_banded_to_dense(const ebem_banded* op, int lag0, int nlag, double* E, void* stream);
+int ebem_banded_march(const ebem_banded* op, const double* rhs, int nT, double* phi, void* stream);
+void ebem_banded_destroy(ebem_banded* op);
+
 typedef struct ebem_lu ebem_lu;
 int ebem_lu_create(const double* A, int n, void* stream, ebem_lu** out);
 int ebem_lu_solve(ebem_lu* lu, double* b, int nrhs, void* stream);
