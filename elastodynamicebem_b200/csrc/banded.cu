@@ -17,9 +17,9 @@
 // The marching (BEMenerg_coreGPU_timeMarching.m:151-169) is unchanged in
 // arithmetic content: E_0 is expanded to a dense matrix and factorised once
 // (cuSOLVER getrf); step n forms b_n - sum_{l=1}^{min(n, L-1)} E_l phi_{n-l}
-// with band_hist_kernel (one warp per source row, lanes over the (pair, lag)
-// blocks of 32 pairs at a time, the past densities stored time-contiguous per
-// field triangle) and solves with the LU factors.
+// with band_hist_kernel (warps over ranges of a source row's pairs, lanes
+// over the (pair, lag) blocks of 32 pairs at a time, the past densities stored
+// time-contiguous per field triangle) and solves with the LU factors.
 #include "ebem_internal.h"
 #include "sa_pair.cuh"
 
@@ -192,21 +192,28 @@ int band_to_dense(const BandOp& op, int lag0, int nlag, double* d_E, cudaStream_
 // marching
 
 // y[3i + c] -= sum_j sum_{l = max(lo,1)}^{min(hi, n)} (E_l)_{ij} phi_{n-l, j}:
-// one warp per source row i.  The pairs of the row are taken 32 at a time:
+// each source row i is split into `split` ranges of its pairs, one warp per
+// range, added into y with one atomic per component (the order of those
+// additions varies from run to run, as in the dense history product).  The
+// pairs of a range are taken 32 at a time:
 // each lane loads one pair's offset, first lag and active lag count, a warp
 // scan of the counts numbers the chunk's (pair, lag) blocks, and the lanes
 // run over those blocks (consecutive lanes read consecutive blocks of the
 // band storage), each finding its pair by a binary search over the scanned
 // counts.  phiT[(j nT + t) 3 + c].
 __global__ void __launch_bounds__(256) band_hist_kernel(const double* __restrict__ Eb, const long long* __restrict__ off,
-                                                        const int* __restrict__ lo, int N, int n, int nT,
+                                                        const int* __restrict__ lo, int N, int split, int n, int nT,
                                                         const double* __restrict__ phiT, double* __restrict__ y) {
     const int lane = threadIdx.x & 31;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long i = warp; i < N; i += nwarps) {
+    const int nchunk = (N + 31) / 32;
+    for (long long w = warp; w < (long long)N * split; w += nwarps) {
+        const long long i = w / split;
+        const int part = (int)(w - i * split);
+        const int jb0 = 32 * (int)((long long)nchunk * part / split), jb1 = 32 * (int)((long long)nchunk * (part + 1) / split);
         double a0 = 0, a1 = 0, a2 = 0;
-        for (int jb = 0; jb < N; jb += 32) {
+        for (int jb = jb0; jb < jb1; jb += 32) {
             const int jl = jb + lane;
             long long first = 0;          // block index of the pair's first active lag
             int ls = 0, cnt = 0;          // first active lag, active lags
@@ -252,10 +259,10 @@ __global__ void __launch_bounds__(256) band_hist_kernel(const double* __restrict
             a1 += __shfl_xor_sync(0xffffffffu, a1, o);
             a2 += __shfl_xor_sync(0xffffffffu, a2, o);
         }
-        if (lane == 0) {
-            y[3 * i] -= a0;
-            y[3 * i + 1] -= a1;
-            y[3 * i + 2] -= a2;
+        if (lane == 0 && (a0 != 0.0 || a1 != 0.0 || a2 != 0.0)) {
+            atomicAdd(y + 3 * i, -a0);
+            atomicAdd(y + 3 * i + 1, -a1);
+            atomicAdd(y + 3 * i + 2, -a2);
         }
     }
 }
@@ -304,7 +311,11 @@ int band_march(const BandOp& op, const double* d_rhs, int nT, double* d_phi, cud
     if (cudaGetLastError() != cudaSuccess) rc = fail(EBEM_ERR_CUDA, "E_0 expansion failed");
     if (!rc) rc = lu_plan_create(E0, n3, s, &lu);
     cudaFree(E0);
-    const int hist_blocks = std::min<long long>((N + 7) / 8, (long long)sms * 8);
+    // each source row split over enough warps to keep about 48 warps per SM
+    // streaming (one warp per row leaves HBM idle when N is small)
+    const int nchunk = (N + 31) / 32;
+    const int split = (int)std::max<long long>(1, std::min<long long>(nchunk, ((long long)sms * 48 + N - 1) / N));
+    const int hist_blocks = (int)std::min<long long>(((long long)N * split + 7) / 8, (long long)sms * 8);
     for (int n = 0; n < nT && !rc; n++) {
         double* y = d_phi + (size_t)n * n3;
         if (cudaMemcpyAsync(y, d_rhs + (size_t)n * n3, (size_t)n3 * sizeof(double), cudaMemcpyDeviceToDevice, s) !=
@@ -312,7 +323,7 @@ int band_march(const BandOp& op, const double* d_rhs, int nT, double* d_phi, cud
             rc = fail(EBEM_ERR_CUDA, "right-hand side copy failed");
             break;
         }
-        if (n > 0 && op.L > 1) band_hist_kernel<<<hist_blocks, 256, 0, s>>>(op.Eb, op.off, op.lo, N, n, nT, phiT, y);
+        if (n > 0 && op.L > 1) band_hist_kernel<<<hist_blocks, 256, 0, s>>>(op.Eb, op.off, op.lo, N, split, n, nT, phiT, y);
         if (cudaGetLastError() != cudaSuccess) {
             rc = fail(EBEM_ERR_CUDA, "banded history failed");
             break;
