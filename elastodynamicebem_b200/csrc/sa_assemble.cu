@@ -490,6 +490,9 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
 
 // One warp per pair (schedule described in sa_warp.cuh); R children per lane
 // (3 n_gh <= 32 R), WPB warps per block.
+#ifndef EBEM_WARP_WPB
+#define EBEM_WARP_WPB 4    // warps per block of the one-child-per-lane kernel
+#endif
 #ifndef EBEM_WARP_MINB
 #define EBEM_WARP_MINB 4   // 128 registers: 4 blocks (16 warps) per SM
 #endif
@@ -569,8 +572,8 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
     long long NN = diag_only ? (long long)nsrc : (long long)nsrc * m.nt;
     if (pairs) NN = npairs;
     if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 32)
-        return mixed ? launch_warp<1, 4, EBEM_WARP_MINB, true>(A, NN, m.device, s)
-                     : launch_warp<1, 4, EBEM_WARP_MINB, false>(A, NN, m.device, s);
+        return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
+                     : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
     if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 64)
         return mixed ? launch_warp<2, 2, 4, true>(A, NN, m.device, s) : launch_warp<2, 2, 4, false>(A, NN, m.device, s);
     if (pairs || mixed) return fail(EBEM_ERR_INVALID, "pair lists and mixed precision need the warp kernel");
@@ -612,8 +615,8 @@ int launch_sa_assemble_banded(const MeshData& m, const PhysParams& P, int n_gh, 
     A.blo = d_blo;
     const long long NN = (long long)m.nt * m.nt;
     if (3 * n_gh <= 32)
-        return mixed ? launch_warp<1, 4, EBEM_WARP_MINB, true>(A, NN, m.device, s)
-                     : launch_warp<1, 4, EBEM_WARP_MINB, false>(A, NN, m.device, s);
+        return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
+                     : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
     return mixed ? launch_warp<2, 2, 4, true>(A, NN, m.device, s) : launch_warp<2, 2, 4, false>(A, NN, m.device, s);
 }
 
@@ -722,7 +725,7 @@ int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh,
     A.pairs = nullptr;
     A.npairs = 0;
     const long long NN = (long long)m.nt * m.nt;
-    int rc = (3 * n_gh <= 32) ? launch_warp<1, 4, EBEM_WARP_MINB, false>(A, NN, m.device, s)
+    int rc = (3 * n_gh <= 32) ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s)
                               : launch_warp<2, 2, 4, false>(A, NN, m.device, s);
     if (rc) return rc;
     if (count) {
