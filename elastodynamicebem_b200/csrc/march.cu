@@ -444,8 +444,9 @@ void lu_plan_destroy(LuPlan* plan) {
 // M(tau) the single-point combined kernel integral over each triangle
 // (BEMenerg_postProcA_singlePoint.m:21-61), divided by 4 pi rho and cleaned
 // below 1e-14 (BEMenerg_postProcA_calcMatrix.m:103).  One thread per
-// (triangle, point); consecutive lanes take consecutive triangles of one
-// point, reduce over the warp and add to u with one atomic per component.
+// (triangle, point, time); consecutive lanes take consecutive triangles of
+// one (point, time), reduce over the warp and add to u with one atomic per
+// component.
 __device__ __forceinline__ void pp_block(double M[6], const TriGeom& F, const NodeW& x, double tau, double velP,
                                          double velS, double c4) {
     level_value(M, 1, velP, velS, tau, F, &x, 1);
@@ -466,47 +467,51 @@ __global__ void __launch_bounds__(128) pp_sa_kernel(const TriGeom* __restrict__ 
                                                     int npts, const double* __restrict__ times, int ntimes,
                                                     const double* __restrict__ phi, int nT, double velP, double velS,
                                                     double dt, double c4, double* __restrict__ u) {
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    bool valid = idx < (long long)N * npts;
-    int j = valid ? (int)(idx % N) : 0, p = valid ? (int)(idx / N) : 0;
+    // one thread per (triangle j, point p, time q), j fastest: a warp shares
+    // (p, q) unless it straddles two of them
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long NP = (long long)N * npts;
+    const bool valid = idx < NP * ntimes;
+    const int q = valid ? (int)(idx / NP) : 0;
+    const long long r = valid ? idx - (long long)q * NP : 0;
+    const int j = (int)(r % N), p = (int)(r / N);
     NodeW x;
     x.x = pts[3 * p]; x.y = pts[3 * p + 1]; x.z = pts[3 * p + 2]; x.w = 1.0;
     const TriGeom& F = geo[j];
     const size_t n3 = 3 * (size_t)N;
-    for (int q = 0; q < ntimes; q++) {
-        double t = times[q];
-        double acc[3] = {0, 0, 0};
-        if (valid && t > 0) {
-            int nHat = (int)ceil(t / dt) - 1;
-            if (nHat > nT - 1) nHat = nT - 1;
-            double Mc[6], Mn[6];
-            pp_block(Mc, F, x, t, velP, velS, c4);
-            for (int k = 1; k <= nHat; k++) {
-                pp_block(Mn, F, x, t - k * dt, velP, velS, c4);
-                const double* ph = phi + (size_t)(k - 1) * n3 + 3 * (size_t)j;
-                double D[6];
+    const double t = times[q];
+    double acc[3] = {0, 0, 0};
+    if (valid && t > 0) {
+        int nHat = (int)ceil(t / dt) - 1;
+        if (nHat > nT - 1) nHat = nT - 1;
+        double Mc[6], Mn[6];
+        pp_block(Mc, F, x, t, velP, velS, c4);
+        for (int k = 1; k <= nHat; k++) {
+            pp_block(Mn, F, x, t - k * dt, velP, velS, c4);
+            const double* ph = phi + (size_t)(k - 1) * n3 + 3 * (size_t)j;
+            double D[6];
 #pragma unroll
-                for (int e = 0; e < 6; e++) { D[e] = Mc[e] - Mn[e]; Mc[e] = Mn[e]; }
-                sym_mv_add(acc, D, ph, 1.0);
-            }
-            sym_mv_add(acc, Mc, phi + (size_t)nHat * n3 + 3 * (size_t)j, 1.0);
+            for (int e = 0; e < 6; e++) { D[e] = Mc[e] - Mn[e]; Mc[e] = Mn[e]; }
+            sym_mv_add(acc, D, ph, 1.0);
         }
-        double sum[3];
+        sym_mv_add(acc, Mc, phi + (size_t)nHat * n3 + 3 * (size_t)j, 1.0);
+    }
+    double sum[3];
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            double v = acc[c];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            sum[c] = v;
-        }
-        // a warp may straddle two points: then every lane adds its own value
-        int p_first = __shfl_sync(0xffffffffu, p, 0), p_last = __shfl_sync(0xffffffffu, p, 31);
-        int v_last = __shfl_sync(0xffffffffu, valid ? 1 : 0, 31);
-        if (p_first == p_last && v_last) {
-            if ((threadIdx.x & 31) == 0)
-                for (int c = 0; c < 3; c++) atomicAdd(u + ((size_t)q * npts + p) * 3 + c, sum[c]);
-        } else if (valid) {
-            for (int c = 0; c < 3; c++) atomicAdd(u + ((size_t)q * npts + p) * 3 + c, acc[c]);
-        }
+    for (int c = 0; c < 3; c++) {
+        double v = acc[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        sum[c] = v;
+    }
+    // a warp may straddle two (point, time) outputs: then every lane adds its own value
+    const long long o_me = (long long)q * npts + p;
+    const long long o_first = __shfl_sync(0xffffffffu, o_me, 0), o_last = __shfl_sync(0xffffffffu, o_me, 31);
+    const int v_last = __shfl_sync(0xffffffffu, valid ? 1 : 0, 31);
+    if (o_first == o_last && v_last) {
+        if ((threadIdx.x & 31) == 0)
+            for (int c = 0; c < 3; c++) atomicAdd(u + o_me * 3 + c, sum[c]);
+    } else if (valid) {
+        for (int c = 0; c < 3; c++) atomicAdd(u + o_me * 3 + c, acc[c]);
     }
 }
 
@@ -516,8 +521,12 @@ int launch_pp_sa(const MeshData& m, const PhysParams& P, const double* d_phi, co
     EBEM_CUDA_TRY(cudaMalloc(&d_times, sizeof(double) * ntimes));
     EBEM_CUDA_TRY(cudaMemcpyAsync(d_times, h_times, sizeof(double) * ntimes, cudaMemcpyHostToDevice, s));
     EBEM_CUDA_TRY(cudaMemsetAsync(d_u, 0, sizeof(double) * 3 * (size_t)npts * ntimes, s));
-    long long total = (long long)m.nt * npts;
+    long long total = (long long)m.nt * npts * ntimes;
     int threads = 128;
+    if ((total + threads - 1) / threads > 0x7fffffffLL) {
+        cudaFree(d_times);
+        return fail(EBEM_ERR_INVALID, "too many (triangle, point, time) triples for one launch");
+    }
     pp_sa_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, s>>>(
         m.d_geo, m.nt, d_pts, npts, d_times, ntimes, d_phi, P.nT, P.velP, P.velS, P.dt, 4 * kPi * P.rho, d_u);
     cudaError_t e = cudaGetLastError();

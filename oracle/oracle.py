@@ -213,6 +213,14 @@ def field_integrals(mesh, velP: float, velS: float, j: int, x, t: float, variant
     return out.reshape(6, 3, 3), int(typ)
 
 
+def ref_kernel_ms(name: str) -> float:
+    """Device time (CUDA events) of the last launch of the reference kernel
+    built into oracle/_ref/libref_<name>.so (ghc, k, g or p)."""
+    L = C.CDLL(os.path.join(_HERE, "_ref", f"libref_{name}.so"))
+    L.ref_last_kernel_ms.restype = C.c_float
+    return float(L.ref_last_kernel_ms())
+
+
 def ref_ghc_available() -> bool:
     return os.path.exists(os.path.join(_HERE, "_ref", "libref_ghc.so"))
 

@@ -10,6 +10,29 @@
 #include <cuda_runtime.h>
 #include <vector>
 
+static float g_last_ms = -1.0f;   // device time of the last reference kernel launch (CUDA events)
+
+extern "C" float ref_last_kernel_ms() { return g_last_ms; }
+
+// CUDA events around one launch; the elapsed time lands in g_last_ms.
+struct KernelTimer {
+    cudaEvent_t e0, e1;
+    KernelTimer() {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0);
+    }
+    void stop() {
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&g_last_ms, e0, e1);
+    }
+    ~KernelTimer() {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+};
+
 #if defined(REF_KERNEL_K)
 #include REF_KERNEL_K
 #elif defined(REF_KERNEL_G)
@@ -68,10 +91,12 @@ extern "C" int ref_k(double* matrix, int N, int Nv, int nlag, double deltaT, dou
            *nm3 = D.put(nodesMesh, 3 * (size_t)Nv);
     if (!D.ok) return -3;
     dim3 grid(N, Nv, nlag), block(nSub, nSing);
+    KernelTimer timer;
     kernelK<<<grid, block, nSub * nSing * 9 * sizeof(double)>>>(d_m, deltaT, velP, velS, lambda, mu, rho,
                                                                 4 * 3.141592653589793 * deltaT, w, x, y, z, nGH, cw,
                                                                 ccx, ccy, ccz, v, a, nr, ism, mc, vc, offsetZ,
                                                                 numBlocks, nm3, maxLen);
+    timer.stop();
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(matrix, d_m, nm * sizeof(double), cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? 0 : -2;
@@ -98,8 +123,10 @@ extern "C" int ref_g(double* matrix, int N, int nHat, double velP, double velS, 
            *ml = D.put(maxLenT, N);
     if (!D.ok) return -3;
     dim3 grid(N, nHat, 1), block(nSub, 1, 1);
+    KernelTimer timer;
     kernelPPNEWG<<<grid, block, nSub * 9 * sizeof(double)>>>(d_m, velP, velS, 4 * 3.141592653589793 * rho, sp, dtm, w,
                                                              x, y, z, nSing, v, a, c, ml);
+    timer.stop();
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(matrix, d_m, nm * sizeof(double), cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? 0 : -2;
@@ -125,9 +152,11 @@ extern "C" int ref_p(double* matrix, int N, int Nv, int nHat, double velP, doubl
     double *mc = D.put(matCoeff, 9 * (size_t)N), *vc = D.put(vetCoeff, 3 * (size_t)N);
     if (!D.ok) return -3;
     dim3 grid(Nv, nHat, 1), block(nSub, 1, 1);
+    KernelTimer timer;
     kernelPPNEWP<<<grid, block, nSub * 9 * sizeof(double)>>>(d_m, velP, velS, lambda, mu,
                                                              4 * 3.141592653589793 * rho * deltaT, (double)N, sp, dtm,
                                                              w, x, y, z, nSing, v, a, nr, ism, mc, vc);
+    timer.stop();
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(matrix, d_m, nm * sizeof(double), cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? 0 : -2;

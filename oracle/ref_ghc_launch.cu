@@ -9,6 +9,10 @@
 #include <cuda_runtime.h>
 #include <vector>
 
+static float g_last_ms = -1.0f;   // device time of the last reference kernel launch (CUDA events)
+
+extern "C" float ref_last_kernel_ms() { return g_last_ms; }
+
 extern "C" int ref_ghc(double* matrix_host, int N, int nlag, double deltaT, double velP, double velS,
                        double const4PiRho, const double* GHw, const double* GHn /* nGH x 3 */, int nGH,
                        const double* GHCw, const double* GHCn /* nSub*nSing x 3 */, int nSub, int nSing,
@@ -36,10 +40,18 @@ extern "C" int ref_ghc(double* matrix_host, int N, int nlag, double deltaT, doub
     cudaMemcpy(d_v, vertsT, 9 * (size_t)N * 8, cudaMemcpyHostToDevice);
     cudaMemcpy(d_a, areeT, (size_t)N * 8, cudaMemcpyHostToDevice);
     dim3 grid(N, N, nlag), block(nSub, nSing);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
     kernelGHC<<<grid, block, nSub * nSing * 9 * sizeof(double)>>>(d_m, deltaT, velP, velS, const4PiRho, d_w, d_x, d_y,
                                                                   d_z, nGH, d_cw, d_cx, d_cy, d_cz, d_v, d_a,
                                                                   offsetZ, numBlocks);
+    cudaEventRecord(e1);
     cudaError_t e = cudaDeviceSynchronize();
+    cudaEventElapsedTime(&g_last_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     if (e == cudaSuccess) e = cudaMemcpy(matrix_host, d_m, nm * 8, cudaMemcpyDeviceToHost);
     cudaFree(d_m); cudaFree(d_w); cudaFree(d_x); cudaFree(d_y); cudaFree(d_z); cudaFree(d_cw);
     cudaFree(d_cx); cudaFree(d_cy); cudaFree(d_cz); cudaFree(d_v); cudaFree(d_a);
