@@ -13,6 +13,9 @@
 
 #include <cusolverDn.h>
 
+#include <algorithm>
+#include <cmath>
+
 namespace ebem {
 
 // ---------------------------------------------------------------------------
@@ -487,7 +490,7 @@ __global__ void __launch_bounds__(128) pp_sa_kernel(const TriGeom* __restrict__ 
         double Mc[6], Mn[6];
         pp_block(Mc, F, x, t, velP, velS, c4);
         for (int k = 1; k <= nHat; k++) {
-            pp_block(Mn, F, x, t - k * dt, velP, velS, c4);
+            pp_block(Mn, F, x, __dsub_rn(t, __dmul_rn((double)k, dt)), velP, velS, c4);   // no fused multiply-add
             const double* ph = phi + (size_t)(k - 1) * n3 + 3 * (size_t)j;
             double D[6];
 #pragma unroll
@@ -515,8 +518,153 @@ __global__ void __launch_bounds__(128) pp_sa_kernel(const TriGeom* __restrict__ 
     }
 }
 
+// Shared instants.  By parts the sum above is
+//   u(x, t_q) = M(t_q) phi_0 + sum_{k=1}^{nHat} M(t_q - k dt) (phi_k - phi_{k-1}),
+// and for output times on the time grid the instants t_q - k dt of different
+// (q, k) coincide.  The instants are formed on the host exactly as the
+// per-time kernel forms them (k dt rounded, then subtracted from t_q, no
+// fused multiply-add: the closed form's case selection is discontinuous
+// where a front radius equals the point's distance from the plane, so an
+// instant one unit in the last place off can change M there), deduplicated
+// by value; pp_inst_level_kernel evaluates M once per (triangle, point,
+// distinct instant) and pp_inst_sum_kernel contracts, one block per
+// (time, point).
+__global__ void __launch_bounds__(128) pp_inst_level_kernel(const TriGeom* __restrict__ geo, int N,
+                                                            const double* __restrict__ pts, int p0, int np, int nu,
+                                                            const double* __restrict__ taus, double velP, double velS,
+                                                            double c4, double* __restrict__ Mbuf) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)N * np * nu) return;
+    const int j = (int)(idx % N);
+    const long long r = idx / N;
+    const int ui = (int)(r % nu), pl = (int)(r / nu);
+    const int p = p0 + pl;
+    NodeW x;
+    x.x = pts[3 * p]; x.y = pts[3 * p + 1]; x.z = pts[3 * p + 2]; x.w = 1.0;
+    double M[6];
+    pp_block(M, geo[j], x, taus[ui], velP, velS, c4);
+    double* dst = Mbuf + (((size_t)pl * nu + ui) * N + j) * 6;
+#pragma unroll
+    for (int e = 0; e < 6; e++) dst[e] = M[e];
+}
+
+__global__ void __launch_bounds__(128) pp_inst_sum_kernel(const double* __restrict__ Mbuf, int N, int p0, int np,
+                                                          int nu, const int* __restrict__ tab, int kmax,
+                                                          const int* __restrict__ nhat, int npts,
+                                                          const double* __restrict__ phi, double* __restrict__ u) {
+    const int q = blockIdx.x / np, pl = blockIdx.x - q * np;
+    const int nh = nhat[q];
+    const int* tq = tab + (size_t)q * kmax;
+    const size_t n3 = 3 * (size_t)N;
+    double acc[3] = {0, 0, 0};
+    for (int j = threadIdx.x; j < N; j += blockDim.x)
+        for (int k = 0; k <= nh; k++) {
+            const double* Mv = Mbuf + (((size_t)pl * nu + tq[k]) * N + j) * 6;
+            const double* pk = phi + (size_t)k * n3 + 3 * (size_t)j;
+            double d[3] = {pk[0], pk[1], pk[2]};
+            if (k > 0) {
+                d[0] -= pk[-(long long)n3];
+                d[1] -= pk[1 - (long long)n3];
+                d[2] -= pk[2 - (long long)n3];
+            }
+            double Ml[6];
+#pragma unroll
+            for (int e = 0; e < 6; e++) Ml[e] = Mv[e];
+            sym_mv_add(acc, Ml, d, 1.0);
+        }
+    __shared__ double red[3][4];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        double v = acc[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[c][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) v += red[threadIdx.x][i];
+        u[((size_t)q * npts + p0 + pl) * 3 + threadIdx.x] = v;
+    }
+}
+
+// The shared-instant path of launch_pp_sa; returns 1 (nothing done) when the
+// instants barely repeat (times off the grid), where the per-time kernel
+// does the same work without the buffer.
+static int launch_pp_sa_shared(const MeshData& m, const PhysParams& P, const double* d_phi, const double* d_pts,
+                               int npts, const double* h_times, int ntimes, double* d_u, cudaStream_t s) {
+    std::vector<int> nh(ntimes);
+    int kmax = 1;
+    long long terms = 0;
+    std::vector<double> taus;
+    for (int q = 0; q < ntimes; q++) {
+        const double t = h_times[q];
+        int n = -1;
+        if (t > 0) {
+            n = (int)std::ceil(t / P.dt) - 1;
+            if (n > P.nT - 1) n = P.nT - 1;
+        }
+        nh[q] = n;
+        kmax = std::max(kmax, n + 1);
+        terms += n + 1;
+        for (int k = 0; k <= n; k++) {
+            volatile double a = (double)k * P.dt;      // rounded product, then the difference
+            taus.push_back(t - a);
+        }
+    }
+    std::vector<double> uniq(taus);
+    std::sort(uniq.begin(), uniq.end());
+    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+    const int nu = (int)uniq.size();
+    if (nu == 0 || 2LL * nu > terms) return 1;
+    std::vector<int> tab((size_t)ntimes * kmax, 0);
+    {
+        size_t c = 0;
+        for (int q = 0; q < ntimes; q++)
+            for (int k = 0; k <= nh[q]; k++)
+                tab[(size_t)q * kmax + k] = (int)(std::lower_bound(uniq.begin(), uniq.end(), taus[c++]) - uniq.begin());
+    }
+    const size_t per_point = (size_t)nu * m.nt * 6 * sizeof(double);
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)npts, ((size_t)1 << 30) / per_point));
+    int *d_tab = nullptr, *d_nh = nullptr;
+    double *d_taus = nullptr, *Mbuf = nullptr;
+    if (cudaMalloc(&d_tab, tab.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&d_nh, ntimes * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&d_taus, nu * sizeof(double)) != cudaSuccess || cudaMalloc(&Mbuf, per_point * chunk) != cudaSuccess) {
+        cudaGetLastError();
+        if (d_tab) cudaFree(d_tab);
+        if (d_nh) cudaFree(d_nh);
+        if (d_taus) cudaFree(d_taus);
+        return fail(EBEM_ERR_NOMEM, "post-processing workspace allocation failed");
+    }
+    cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_nh, nh.data(), ntimes * sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_taus, uniq.data(), nu * sizeof(double), cudaMemcpyHostToDevice, s);
+    cudaError_t e = cudaSuccess;
+    for (int p0 = 0; p0 < npts && e == cudaSuccess; p0 += chunk) {
+        const int np = std::min(chunk, npts - p0);
+        const long long lv = (long long)m.nt * np * nu;
+        pp_inst_level_kernel<<<(unsigned)((lv + 127) / 128), 128, 0, s>>>(m.d_geo, m.nt, d_pts, p0, np, nu, d_taus,
+                                                                         P.velP, P.velS, 4 * kPi * P.rho, Mbuf);
+        pp_inst_sum_kernel<<<(unsigned)((long long)ntimes * np), 128, 0, s>>>(Mbuf, m.nt, p0, np, nu, d_tab, kmax, d_nh,
+                                                                              npts, d_phi, d_u);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(Mbuf);
+    cudaFree(d_taus);
+    cudaFree(d_tab);
+    cudaFree(d_nh);
+    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("post-processing kernels: ") + cudaGetErrorString(e));
+    return EBEM_OK;
+}
+
 int launch_pp_sa(const MeshData& m, const PhysParams& P, const double* d_phi, const double* d_pts, int npts,
                  const double* h_times, int ntimes, double* d_u, cudaStream_t s) {
+    {
+        const int rc = launch_pp_sa_shared(m, P, d_phi, d_pts, npts, h_times, ntimes, d_u, s);
+        if (rc != 1) return rc;                         // done (or failed); 1: instants barely repeat
+    }
     double* d_times = nullptr;
     EBEM_CUDA_TRY(cudaMalloc(&d_times, sizeof(double) * ntimes));
     EBEM_CUDA_TRY(cudaMemcpyAsync(d_times, h_times, sizeof(double) * ntimes, cudaMemcpyHostToDevice, s));

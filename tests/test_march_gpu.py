@@ -109,3 +109,26 @@ def test_pp_screen(ebem, oracle):
     # exact value of the formulas at a few points and times
     uq = oracle.pp_sa(m, prm, phi.cpu().numpy().T, pts[:3], times[:2], variant="q").transpose(2, 1, 0)
     assert rel(u[:2, :3], uq) <= 1e-10
+
+
+def test_pp_grid_and_off_grid_times(ebem, oracle):
+    """Output times whose instants t - k dt repeat (on the grid, or all with
+    one offset from it) take the path that evaluates each distinct instant
+    once per (triangle, point); scattered times the per-time path; t <= 0
+    gives zero.  All against the oracle's closed form."""
+    from elastodynamicebem_b200 import problem
+    w = problem.screen_workload()
+    m, prm = w.mesh, w.params
+    dm = ebem.DeviceMesh(m)
+    phi, L = ebem.timemarch_sa(dm, prm, 7, w.datum)
+    pts = w.points[:16]
+    # within the simulated interval: past t = (nT - 1) dt the reference's sum
+    # reads density columns that do not exist (BEMenerg_postProcA_singlePoint.m:21,58)
+    on = np.concatenate([[0.0], prm.dt * np.array([1, 2, 7, 13, prm.nT - 1])])
+    offset = np.concatenate([[0.0], prm.dt * (np.array([0, 1, 6, 12, prm.nT - 2]) + 0.37)])
+    scattered = np.concatenate([[-0.1], np.random.default_rng(4).uniform(0.0, (prm.nT - 1) * prm.dt, 6)])
+    for times in (on, offset, scattered):
+        u = ebem.pp_sa(dm, prm, phi, pts, times).cpu().numpy()
+        uo = oracle.pp_sa(m, prm, phi.cpu().numpy().T, pts, times).transpose(2, 1, 0)
+        assert np.abs(u[0]).max() == 0.0 if times[0] == 0.0 else True
+        assert rel(u, uo) <= 1e-9
