@@ -152,6 +152,79 @@ __global__ void __launch_bounds__(128) ghc_assemble_kernel(GHCArgs A) {
     }
 }
 
+// Warp-per-pair variant for rules with at least 160 node pairs: the lanes
+// take the node pairs (inner node q, outer node o) of the pair, the same
+// per-node-pair arithmetic as ghc_assemble_kernel, and a warp reduction per
+// lag gives the 6 entries (the thread kernel leaves half of each warp's
+// lanes idle on the skip test and keeps 7 warps per SM busy).
+__global__ void __launch_bounds__(128) ghc_assemble_warp_kernel(GHCArgs A) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int n_in = A.n_sub * A.n_sing, NP = n_in * A.n_out;
+    const double cP = A.velP, cS = A.velS, dt = A.dt;
+    const double icP2 = 1 / (cP * cP), icS2 = 1 / (cS * cS);
+    const size_t n3 = A.ld;
+    for (long long p = warp; p < (long long)A.N * A.N; p += nwarps) {
+        const int i = (int)(p % A.N);      // source (outer rule)
+        const int j = (int)(p / A.N);      // field (inner rule)
+        if (i == j) continue;
+        double VS[3][3], VF[3][3];
+        for (int v = 0; v < 3; v++)
+            for (int c = 0; c < 3; c++) {
+                VS[v][c] = A.coords[3 * A.tris[3 * i + v] + c];
+                VF[v][c] = A.coords[3 * A.tris[3 * j + v] + c];
+            }
+        double distMax = 0;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                double d0 = VS[a][0] - VF[b][0], d1 = VS[a][1] - VF[b][1], d2 = VS[a][2] - VF[b][2];
+                distMax = fmax(distMax, sqrt(d0 * d0 + d1 * d1 + d2 * d2));
+            }
+        int lhi = A.lag0 + A.nlag - 1;
+        while (lhi >= A.lag0 && (lhi - 1) * A.velS * A.dt > distMax) lhi--;
+        if (lhi < A.lag0) continue;
+        const double aS = A.geo[i].area, aF = A.geo[j].area;
+        for (int l = A.lag0; l <= lhi; l++) {
+            const double thi = (l + 1) * dt, tlo = (l - 1) * dt;
+            const double skipP2 = (cP * thi) * (cP * thi) * (1 + 1e-12);
+            const double skipS2 = (l >= 1) ? (cS * tlo) * (cS * tlo) * (1 - 1e-12) : -1.0;
+            double K[6] = {0, 0, 0, 0, 0, 0};
+            for (int np = lane; np < NP; np += 32) {
+                const int q = np / A.n_out, o = np - q * A.n_out;
+                const double* bq = A.inner + 3 * q;
+                const double* bl = A.outer + 3 * o;
+                double x[3];
+                for (int c = 0; c < 3; c++)
+                    x[c] = (bq[0] * VF[0][c] + bq[1] * VF[1][c] + bq[2] * VF[2][c]) -
+                           (bl[0] * VS[0][c] + bl[1] * VS[1][c] + bl[2] * VS[2][c]);
+                const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+                if (r2 > skipP2 || r2 < skipS2) continue;
+                const double r = sqrt(r2);
+                const Win2 P = ghc_window2(r, cP, l, dt), S = ghc_window2(r, cS, l, dt);
+                const double w = (A.wout[o] * aS) * (A.win[q % A.n_sing] * aF);
+                double nu[6];
+                ghc_pair(nu, x, 1 / r, P.H, S.H, P.Q - S.Q, icP2, icS2);
+#pragma unroll
+                for (int e = 0; e < 6; e++) K[e] += w * nu[e];
+            }
+#pragma unroll
+            for (int e = 0; e < 6; e++)
+                for (int off = 16; off > 0; off >>= 1) K[e] += __shfl_xor_sync(0xffffffffu, K[e], off);
+            if (lane < 9) {
+                const int c = lane / 3, r = lane - 3 * c;
+                const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+                double v = 0;
+#pragma unroll
+                for (int e = 0; e < 6; e++)
+                    if (e == map[lane]) v = K[e];
+                double* base = A.E + (size_t)(l - A.lag0) * A.ld_lag + (3 * (size_t)j) * n3 + 3 * (size_t)i;
+                if (fabs(v) > 1.0e-14) base[c * n3 + r] += v / A.c4pirho;
+            }
+        }
+    }
+}
+
 int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_sub, int n_sing, int lag0, int nlag,
                         double* d_E, size_t ld, size_t ld_lag, cudaStream_t s) {
     double ob[28 * 3], ow[28];
@@ -191,7 +264,16 @@ int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_
     A.ld_lag = ld_lag;
     long long NN = (long long)m.nt * m.nt;
     int threads = 128;
-    ghc_assemble_kernel<<<(unsigned)((NN + threads - 1) / threads), threads, 0, s>>>(A);
+    // warp per pair from 160 node pairs per pair on (measured: 336 node pairs
+    // 1.57x faster than the thread kernel, 84 node pairs 1.2x slower)
+    if ((long long)n_gh * n_sub * n_sing >= 160) {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
+        const long long want = (NN + 3) / 4, cap = (long long)sms * 64;
+        ghc_assemble_warp_kernel<<<(unsigned)(want < cap ? want : cap), threads, 0, s>>>(A);
+    } else {
+        ghc_assemble_kernel<<<(unsigned)((NN + threads - 1) / threads), threads, 0, s>>>(A);
+    }
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(d_tab);
