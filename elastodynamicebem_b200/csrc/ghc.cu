@@ -152,7 +152,8 @@ __global__ void __launch_bounds__(128) ghc_assemble_kernel(GHCArgs A) {
     }
 }
 
-// Warp-per-pair variant for rules with at least 160 node pairs: the lanes
+// Warp-per-pair variant for small meshes and rules with at least 160 node
+// pairs (see the dispatch in launch_ghc_assemble): the lanes
 // take the node pairs (inner node q, outer node o) of the pair, the same
 // per-node-pair arithmetic as ghc_assemble_kernel, and a warp reduction per
 // lag gives the 6 entries (the thread kernel leaves half of each warp's
@@ -264,11 +265,13 @@ int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_
     A.ld_lag = ld_lag;
     long long NN = (long long)m.nt * m.nt;
     int threads = 128;
-    // warp per pair from 160 node pairs per pair on (measured: 336 node pairs
-    // 1.57x faster than the thread kernel, 84 node pairs 1.2x slower)
-    if ((long long)n_gh * n_sub * n_sing >= 160) {
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
+    // warp per pair when the thread kernel would not fill the GPU (fewer
+    // pairs than two waves of threads) and a pair has 160+ node pairs
+    // (measured: sphere of 320 triangles, 336 node pairs, 1.57x faster; 84 node
+    // pairs 1.2x slower; bar of 2800 triangles, 7.8 M pairs, 1.2x slower)
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
+    if ((long long)n_gh * n_sub * n_sing >= 160 && NN < (long long)sms * 4096) {
         const long long want = (NN + 3) / 4, cap = (long long)sms * 64;
         ghc_assemble_warp_kernel<<<(unsigned)(want < cap ? want : cap), threads, 0, s>>>(A);
     } else {
