@@ -211,7 +211,15 @@ struct LaneChild {
 // lo-subtractions into A (child frame), whole-range pieces from the moments
 // (or flagged in need_mom when they are not computed yet), partial edge
 // pieces returned in pc[0..np).  Mirrors child_level_e piece by piece.
-EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const LaneChild& C, const LevelCtx& L,
+#ifndef EBEM_NOINLINE_DECIDE
+#define EBEM_NOINLINE_DECIDE 0     // 1: one out-of-line copy of the decision phase
+#endif
+#if EBEM_NOINLINE_DECIDE
+static __device__ __noinline__
+#else
+EBEM_DI
+#endif
+void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const LaneChild& C, const LevelCtx& L,
                           double rhoP, double rhoS, int type, const W4& w0, double amax) {
     const ChildE& g = C.g;
     const bool isP = (type == T_P), spsp = (type == T_SP_SP);
