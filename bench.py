@@ -95,6 +95,13 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def physical_gpu(local_rank: int) -> str:
+    """The nvidia-smi id (index or UUID) of this rank's device: the
+    local_rank-th entry of CUDA_VISIBLE_DEVICES when it is set."""
+    ids = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    return ids[local_rank] if local_rank < len(ids) else str(local_rank)
+
+
 # --------------------------------------------------------------------------
 def fp64_peak_tflops(torch) -> float:
     """Measured FP64 throughput: cuBLAS DGEMM (torch.matmul, float64,
@@ -294,7 +301,7 @@ def main():
     if world > 1:
         dist.barrier()
 
-    sampler = ClockSampler(local_rank if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
+    sampler = ClockSampler(physical_gpu(local_rank))
     sampler.start()
     time.sleep(0.3)
     torch.cuda.synchronize()
