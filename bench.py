@@ -39,10 +39,10 @@ FLOPS_PER_PAIR_INTEGRAL = 19_232.0
 FLOPS_PER_PAIR_INTEGRAL_REF_SCHEDULE = 53_560.0
 
 # DRAM bytes (read + write) per launch of the assembly kernel: ncu on the
-# sphere N=320 case measured 61.4 MB + 614.6 MB; the traffic is the N^2 L output
+# sphere N=320 case measured 30.7 MB + 339.8 MB; the traffic is the N^2 L output
 # (written in 24-byte column pieces), so it is scaled to N=1280 by the output
 # size, x16.
-NCU_TRAFFIC_PER_LAUNCH = (61.41184e6 + 614.560256e6) * 16
+NCU_TRAFFIC_PER_LAUNCH = (30.733056e6 + 339.811584e6) * 16
 KERNEL = "sa_assemble_warp_kernel"
 
 
