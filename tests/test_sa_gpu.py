@@ -1,7 +1,7 @@
 """Parity of the CUDA semi-analytic assembly (through the C ABI) with the CPU
 oracle (C++ restatement of the reference's SA path).
 
-Two oracles judge the device result on the same double inputs:
+Two oracles check the device result on the same double inputs:
   * "q"   the reference's formulas evaluated in binary128 (the exact value of
           those formulas to ~1e-30);
   * "f64" the same restatement in double precision, i.e. the reference's own
