@@ -493,6 +493,9 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
 #ifndef EBEM_WARP_WPB
 #define EBEM_WARP_WPB 4    // warps per block of the one-child-per-lane kernel
 #endif
+#ifndef EBEM_WARP2_MINB
+#define EBEM_WARP2_MINB 4  // blocks per SM of the two-children-per-lane kernel (12- and 19-node rules)
+#endif
 #ifndef EBEM_WARP_MINB
 #define EBEM_WARP_MINB 3   // 170 registers: 3 blocks (12 warps) per SM (2.7 % faster than 4 blocks / 128 registers)
 #endif
@@ -575,7 +578,7 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
         return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
                      : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
     if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 64)
-        return mixed ? launch_warp<2, 2, 4, true>(A, NN, m.device, s) : launch_warp<2, 2, 4, false>(A, NN, m.device, s);
+        return mixed ? launch_warp<2, 2, EBEM_WARP2_MINB, true>(A, NN, m.device, s) : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
     if (pairs || mixed) return fail(EBEM_ERR_INVALID, "pair lists and mixed precision need the warp kernel");
     int threads = 128;
     long long blocks = (NN + threads - 1) / threads;
@@ -617,7 +620,7 @@ int launch_sa_assemble_banded(const MeshData& m, const PhysParams& P, int n_gh, 
     if (3 * n_gh <= 32)
         return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
                      : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
-    return mixed ? launch_warp<2, 2, 4, true>(A, NN, m.device, s) : launch_warp<2, 2, 4, false>(A, NN, m.device, s);
+    return mixed ? launch_warp<2, 2, EBEM_WARP2_MINB, true>(A, NN, m.device, s) : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -726,7 +729,7 @@ int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh,
     A.npairs = 0;
     const long long NN = (long long)m.nt * m.nt;
     int rc = (3 * n_gh <= 32) ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s)
-                              : launch_warp<2, 2, 4, false>(A, NN, m.device, s);
+                              : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
     if (rc) return rc;
     if (count) {
         EBEM_CUDA_TRY(cudaMemcpyAsync(host_count, d_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
