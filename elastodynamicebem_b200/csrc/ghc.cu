@@ -116,10 +116,28 @@ __global__ void __launch_bounds__(128) ghc_assemble_kernel(GHCArgs A) {
     const double icP2 = 1 / (cP * cP), icS2 = 1 / (cS * cS);
     const size_t n3 = A.ld;
     const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    // the node pairs' exact distance range (one pass): a lag whose window lies
+    // before the P front or after the S front for all of them adds nothing
+    // (the null test above bounds the lags by vertex distances only)
+    double r2min = 1e300, r2max = 0.0;
+    for (int q = 0; q < A.n_sub * A.n_sing; q++) {
+        const double* bq = A.inner + 3 * q;
+        double y[3];
+        for (int c = 0; c < 3; c++) y[c] = bq[0] * VF[0][c] + bq[1] * VF[1][c] + bq[2] * VF[2][c];
+        for (int o = 0; o < A.n_out; o++) {
+            const double* bl = A.outer + 3 * o;
+            double x[3];
+            for (int c = 0; c < 3; c++) x[c] = y[c] - (bl[0] * VS[0][c] + bl[1] * VS[1][c] + bl[2] * VS[2][c]);
+            const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            r2min = fmin(r2min, r2);
+            r2max = fmax(r2max, r2);
+        }
+    }
     for (int l = A.lag0; l <= lhi; l++) {
         const double thi = (l + 1) * dt, tlo = (l - 1) * dt;
         const double skipP2 = (cP * thi) * (cP * thi) * (1 + 1e-12);
         const double skipS2 = (l >= 1) ? (cS * tlo) * (cS * tlo) * (1 - 1e-12) : -1.0;
+        if (r2min > skipP2 || r2max < skipS2) continue;
         double K[6] = {0, 0, 0, 0, 0, 0};
         for (int q = 0; q < A.n_sub * A.n_sing; q++) {
             const double* bq = A.inner + 3 * q;
