@@ -194,6 +194,23 @@ def test_row_pp_dir(ebem, bar):
     assert err <= 1e-12
 
 
+def test_row_dn_marching(ebem, bar):
+    import torch
+    from elastodynamicebem_b200 import problem
+    from test_direct_gpu import _march_dn_numpy
+    m, prm, dm, (LV, LK) = bar
+    V = ebem.assemble_v(dm, prm, 7, 4, 3, 16, 0, LV).clone()
+    K = ebem.assemble_k(dm, prm, 7, 4, 3, 16, 0, LK).clone()
+    gV = torch.tensor(problem.bar_neumann(m, prm, 3.0), device="cuda")
+    ours = dev_ms(lambda: ebem.march_dn(dm, prm, V, K, gV))
+    u = ebem.march_dn(dm, prm, V, K, gV).cpu().numpy()
+    ref, uo = cpu_ms(lambda: _march_dn_numpy(m, prm, V.cpu().numpy(), K.cpu().numpy(), gV.cpu().numpy()))
+    err = rel(u, uo)
+    record("a18 DN marching", f"bar N={m.numberTriangles}, Nv={m.number_nodes}, nT={prm.nT}", ours, ref,
+           "the reference's per-step least squares in numpy/LAPACK (BEMenerg_dir_timeMarchingN.m:268-299)", err)
+    assert err <= 1e-9
+
+
 def test_zz_print_table():
     if not ROWS:
         pytest.skip("no rows measured")
