@@ -211,7 +211,8 @@ int ebem_mesh_destroy(ebem_mesh* m) {
     if (m->d.d_coords) cudaFree(m->d.d_coords);
     if (m->d.d_tris) cudaFree(m->d.d_tris);
     if (m->d.d_geo) cudaFree(m->d.d_geo);
-    if (m->d.d_nodes) cudaFree(m->d.d_nodes);
+    for (NodeW* t : m->d.d_node_tables)
+        if (t) cudaFree(t);
     free_direct(m->d);
     delete m;
     return EBEM_OK;
@@ -246,10 +247,12 @@ int ebem_num_blocks(const ebem_mesh* m, const ebem_problem* p, int* num_blocks) 
     DeviceGuard dg(m->d.device);
     unsigned long long* d = nullptr;
     EBEM_CUDA_TRY(cudaMalloc(&d, sizeof(unsigned long long)));
-    EBEM_CUDA_TRY(cudaMemset(d, 0, sizeof(unsigned long long)));
-    max_vertex_dist_kernel<<<296, 256>>>(m->d.d_coords, m->d.nv, d);
     unsigned long long bits = 0;
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = cudaMemset(d, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+        max_vertex_dist_kernel<<<296, 256>>>(m->d.d_coords, m->d.nv, d);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaMemcpy(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, cudaGetErrorString(e));
@@ -282,7 +285,11 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
     unsigned long long* d_count = nullptr;
     if (nonnull) {
         EBEM_CUDA_TRY(cudaMalloc(&d_count, sizeof(unsigned long long)));
-        EBEM_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
+        cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) {
+            cudaFree(d_count);
+            return fail(EBEM_ERR_CUDA, std::string("pair counter: ") + cudaGetErrorString(e));
+        }
     }
     int rc = EBEM_OK;
     if (is_device_ptr(E)) {
@@ -590,6 +597,10 @@ int ebem_pp_sa(const ebem_mesh* m, const ebem_problem* p, const double* phi, con
     if (!m || !phi || !pts || !times || !u || npts < 1 || ntimes < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
     if (int rc = check_problem(p)) return rc;
     if (is_device_ptr(times)) return fail(EBEM_ERR_INVALID, "times must be a host array");
+    // u(x, t) uses density column ceil(t / dt) (BEMenerg_postProcA_singlePoint.m:21,58),
+    // which exists for t <= tfin; the reference fails past it
+    for (int q = 0; q < ntimes; q++)
+        if (!(times[q] <= p->tfin * (1 + 1e-12))) return fail(EBEM_ERR_INVALID, "evaluation time beyond tfin");
     DeviceGuard dg(m->d.device);
     cudaStream_t s = (cudaStream_t)stream;
     PhysParams P = phys_from(p);

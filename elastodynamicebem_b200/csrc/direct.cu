@@ -143,13 +143,22 @@ int prep_direct(MeshData& m, cudaStream_t s) {
         free_direct(m);
         return fail(EBEM_ERR_NOMEM, "direct-formulation mesh data allocation failed");
     }
-    EBEM_CUDA_TRY(cudaMemcpyAsync(m.d_vt_off, off.data(), sizeof(int32_t) * off.size(), cudaMemcpyHostToDevice, s));
-    EBEM_CUDA_TRY(cudaMemcpyAsync(m.d_vt_tri, lst.data(), sizeof(int32_t) * lst.size(), cudaMemcpyHostToDevice, s));
-    dir_prep_kernel<<<(m.nt + 127) / 128, 128, 0, s>>>(m.d_coords, m.d_tris, m.nt, m.d_dir);
-    EBEM_CUDA_TRY(cudaGetLastError());
+    // d_dir marks the data as built: on a failure below it is released, so
+    // the next call starts over instead of using a half-built table
     std::vector<DirTri> h(m.nt);
-    EBEM_CUDA_TRY(cudaMemcpyAsync(h.data(), m.d_dir, sizeof(DirTri) * h.size(), cudaMemcpyDeviceToHost, s));
-    EBEM_CUDA_TRY(cudaStreamSynchronize(s));
+    cudaError_t e = cudaMemcpyAsync(m.d_vt_off, off.data(), sizeof(int32_t) * off.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(m.d_vt_tri, lst.data(), sizeof(int32_t) * lst.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        dir_prep_kernel<<<(m.nt + 127) / 128, 128, 0, s>>>(m.d_coords, m.d_tris, m.nt, m.d_dir);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), m.d_dir, sizeof(DirTri) * h.size(), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        free_direct(m);
+        return fail(EBEM_ERR_CUDA, std::string("direct-formulation mesh data: ") + cudaGetErrorString(e));
+    }
     m.max_len = 0.0;
     for (const DirTri& d : h) m.max_len = std::max(m.max_len, d.maxL);
     return EBEM_OK;

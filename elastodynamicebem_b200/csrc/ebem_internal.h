@@ -33,7 +33,13 @@ struct MeshData {
     double* d_coords = nullptr;   // nv x 3
     int32_t* d_tris = nullptr;    // nt x 3 (0-based)
     TriGeom* d_geo = nullptr;     // nt
-    // mapped outer nodes cached per rule: (x, y, z, weight) per (triangle, node)
+    // mapped outer nodes, (x, y, z, weight) per (triangle, node): one table
+    // per Gauss-Hammer rule, built on first use and freed only with the mesh,
+    // so that a pointer held by a batch plan stays valid when the mesh is
+    // later used with another rule.  d_nodes / nodes_rule name the table of
+    // the last map_nodes call.
+    static constexpr int kNodeRules = 6;          // rules of 1, 3, 7, 12, 19, 28 nodes
+    NodeW* d_node_tables[kNodeRules] = {};
     int nodes_rule = 0;
     NodeW* d_nodes = nullptr;     // nt x nodes_rule
     // direct formulation (built on first use): per-triangle P1 data and the

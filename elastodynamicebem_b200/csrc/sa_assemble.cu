@@ -78,22 +78,46 @@ int prep_mesh(MeshData& m, cudaStream_t s) {
 }
 
 int map_nodes(MeshData& m, int n_gh, cudaStream_t s) {
-    if (m.nodes_rule == n_gh && m.d_nodes) return EBEM_OK;
+    static const int kSlotRule[MeshData::kNodeRules] = {1, 3, 7, 12, 19, 28};
+    int slot = -1;
+    for (int k = 0; k < MeshData::kNodeRules; k++)
+        if (kSlotRule[k] == n_gh) slot = k;
+    if (slot < 0) return fail(EBEM_ERR_INVALID, "unsupported Gauss-Hammer rule");
+    if (NodeW* t = m.d_node_tables[slot]) {
+        m.d_nodes = t;
+        m.nodes_rule = n_gh;
+        return EBEM_OK;
+    }
     double bary[28 * 3], w[28];
     int rc = gh_composite(n_gh, 1, bary, w);
     if (rc) return fail(rc, "unsupported Gauss-Hammer rule");
-    if (m.d_nodes) { cudaFree(m.d_nodes); m.d_nodes = nullptr; }
+    // the table enters the cache only once the mapping has finished, so a
+    // failed call leaves no half-built table behind
+    NodeW* table = nullptr;
     double* d_tab = nullptr;
-    EBEM_CUDA_TRY(cudaMalloc(&m.d_nodes, sizeof(NodeW) * (size_t)m.nt * n_gh));
-    EBEM_CUDA_TRY(cudaMalloc(&d_tab, sizeof(double) * 4 * n_gh));
-    EBEM_CUDA_TRY(cudaMemcpyAsync(d_tab, bary, sizeof(double) * 3 * n_gh, cudaMemcpyHostToDevice, s));
-    EBEM_CUDA_TRY(cudaMemcpyAsync(d_tab + 3 * n_gh, w, sizeof(double) * n_gh, cudaMemcpyHostToDevice, s));
-    int total = m.nt * n_gh, threads = 128;
-    map_nodes_kernel<<<(total + threads - 1) / threads, threads, 0, s>>>(m.d_coords, m.d_tris, m.nt, m.d_geo, d_tab,
-                                                                           d_tab + 3 * n_gh, n_gh, m.d_nodes);
-    EBEM_CUDA_TRY(cudaGetLastError());
-    EBEM_CUDA_TRY(cudaStreamSynchronize(s));
+    if (cudaMalloc(&table, sizeof(NodeW) * (size_t)m.nt * n_gh) != cudaSuccess ||
+        cudaMalloc(&d_tab, sizeof(double) * 4 * n_gh) != cudaSuccess) {
+        cudaGetLastError();
+        if (table) cudaFree(table);
+        return fail(EBEM_ERR_NOMEM, "outer-node table allocation failed");
+    }
+    cudaError_t e = cudaMemcpyAsync(d_tab, bary, sizeof(double) * 3 * n_gh, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_tab + 3 * n_gh, w, sizeof(double) * n_gh, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        int total = m.nt * n_gh, threads = 128;
+        map_nodes_kernel<<<(total + threads - 1) / threads, threads, 0, s>>>(m.d_coords, m.d_tris, m.nt, m.d_geo, d_tab,
+                                                                               d_tab + 3 * n_gh, n_gh, table);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(d_tab);
+    if (e != cudaSuccess) {
+        cudaFree(table);
+        return fail(EBEM_ERR_CUDA, std::string("outer-node mapping: ") + cudaGetErrorString(e));
+    }
+    m.d_node_tables[slot] = table;
+    m.d_nodes = table;
     m.nodes_rule = n_gh;
     return EBEM_OK;
 }

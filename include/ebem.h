@@ -42,7 +42,10 @@ extern "C" {
 #define EBEM_ERR_NODEVICE (-4)  /* no CUDA device visible */
 #define EBEM_ERR_SINGULAR (-5)  /* E_0 factorisation found a zero pivot */
 
-/* Opaque device-resident mesh: vertices, triangles and per-triangle frames. */
+/* Opaque device-resident mesh: vertices, triangles and per-triangle frames.
+ * It caches device data built on first use (the mapped outer nodes of each
+ * rule, the direct formulation's vertex adjacency), so one handle must not
+ * be used by two host threads at once; distinct handles are independent. */
 typedef struct ebem_mesh ebem_mesh;
 
 /* The reference's pbParam (f/utility/fileRead/readInputFile.m:12-74):
@@ -159,7 +162,9 @@ int ebem_assemble_sa_noalloc(const ebem_mesh* mesh, const ebem_problem* prob, in
  * captures the launch in a CUDA graph; every call replays the graph.  E[k]:
  * device buffer of 9 N_k^2 nlag[k] doubles, same layout as ebem_assemble_sa,
  * every entry written; results equal ebem_assemble_sa's to rounding (the
- * same per-pair computation in another kernel).
+ * same per-pair computation in another kernel).  The plan reads its meshes'
+ * device data at every replay: destroy it before any of its meshes (using
+ * the meshes in other calls meanwhile, with any rule, is fine).
  * ebem_batch_info reports the chosen shape, its tuning time and the pair count. */
 typedef struct ebem_batch ebem_batch;
 int ebem_batch_create(const ebem_mesh* const* meshes, const ebem_problem* probs, const int* nlag, int n, int n_gh,
@@ -312,8 +317,9 @@ int ebem_timemarch_sa_ex(const ebem_mesh* mesh, const ebem_problem* prob, int n_
  * Replaces campoVett = BEMenerg_postProcA_setup(pbParam, domainMesh, density,
  * numPoints, xVal, tVal)
  * (f/BEMenerg_indir/BEMenerg_postProc/BEMenerg_postProcA/BEMenerg_postProcA_setup.m:1).
- * phi: 3N x nT; pts: npts x 3 (row-major); times: host array; u: 3 x npts x
- * ntimes (u[(q*npts + p)*3 + c]); phi/pts/u host or device. */
+ * phi: 3N x nT; pts: npts x 3 (row-major); times: host array, each <= tfin
+ * (EBEM_ERR_INVALID otherwise; t <= 0 gives zero); u: 3 x npts x ntimes
+ * (u[(q*npts + p)*3 + c]); phi/pts/u host or device. */
 int ebem_pp_sa(const ebem_mesh* mesh, const ebem_problem* prob, const double* phi, const double* pts, int npts,
                const double* times, int ntimes, double* u, void* stream);
 

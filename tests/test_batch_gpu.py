@@ -44,6 +44,31 @@ def test_batch_equals_single(ebem, n_gh, prec):
     assert info["tuned_ms"] > 0 and info["pairs"] == sum(d.N ** 2 for d in dms)
 
 
+@pytest.mark.gpu
+def test_batch_survives_other_rules_on_its_meshes(ebem):
+    """A plan holds device pointers to its meshes' mapped outer nodes; using
+    the same meshes with other rules afterwards leaves those tables in place,
+    so the plan's next replay gives the same blocks."""
+    import torch
+    from elastodynamicebem_b200 import problem
+    inst = problem.batch_workload(count=4, seed=12, n_min=16, n_max=200)
+    dms = [ebem.DeviceMesh(m) for _, m, _ in inst]
+    prms = [p for _, _, p in inst]
+    nlag = [min(ebem.num_blocks(d, p), 6) for d, p in zip(dms, prms)]
+    plan = ebem.BatchPlan(dms, prms, 7, nlag=nlag)
+    first = [g.clone() for g in plan.assemble()]
+    for d, p in zip(dms, prms):
+        for n_gh in (3, 12, 19):
+            ebem.assemble_sa(d, p, n_gh, 0, 1)
+    outs = [torch.full((l, 3 * d.N, 3 * d.N), float("nan"), dtype=torch.float64, device="cuda")
+            for d, l in zip(dms, nlag)]
+    again = plan.assemble(outs)
+    torch.cuda.synchronize()
+    for g, f in zip(again, first):
+        assert float((g - f).norm() / f.norm()) <= 1e-14
+    plan.close()
+
+
 def test_batch_workload_shape():
     from elastodynamicebem_b200 import problem
     inst = problem.batch_workload()

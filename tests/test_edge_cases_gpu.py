@@ -99,6 +99,15 @@ def test_invalid_arguments(ebem):
     bad = lib.problem_struct(problem.ProblemParams(-1.0, 1.0, 2.0, 1.0, 10))
     assert L_.ebem_assemble_sa(dm.handle, C.byref(bad), 7, 0, 4, out.data_ptr(), 0, None, None) == -1  # rho <= 0
     assert L_.ebem_last_error()
+    # post-processing times past tfin: the density has no column for them
+    phi0 = torch.zeros((prm.nT, n3), dtype=torch.float64, device="cuda")
+    pts = np.array([[0.1, 0.2, 0.3]])
+    with pytest.raises(lib.EbemError):
+        ebem.pp_sa(dm, prm, phi0, pts, np.array([0.5, prm.Tfin * 1.01]))
+    with pytest.raises(lib.EbemError):
+        ebem.pp_sa(dm, prm, phi0, pts, np.array([float("nan")]))
+    u = ebem.pp_sa(dm, prm, phi0, pts, np.array([-1.0, prm.Tfin]))
+    assert float(u.abs().max()) == 0.0
     # a zero E_0 cannot be factorised
     E = torch.zeros((2, n3, n3), dtype=torch.float64, device="cuda")
     b = torch.ones((3, n3), dtype=torch.float64, device="cuda")
