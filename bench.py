@@ -348,6 +348,20 @@ def main():
         if s > 0:
             e2e_times.append(dt)
     e2e_value = total_pairs / statistics.median(e2e_times) if e2e_times else None
+    # the host link's device-to-host rate into the same pinned buffer (1 GiB,
+    # CUDA events): an end-to-end step takes at least d2h bytes / this rate
+    flat = host.view(-1)
+    nb = min(flat.numel(), 1 << 27)
+    src = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    cur = torch.cuda.current_stream()
+    flat[:nb].copy_(src, non_blocking=True)
+    l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0.record(cur)
+    flat[:nb].copy_(src, non_blocking=True)
+    l1.record(cur)
+    torch.cuda.synchronize()
+    link_gbs = nb * 8 / (l0.elapsed_time(l1) / 1e3) / 1e9
+    del src
 
     if rank == 0:
         peak = float("nan") if args.no_peak else fp64_peak_tflops(torch)
@@ -369,7 +383,9 @@ def main():
                          "units_per_launch": my_pairs,
                          "kernel": KERNEL, "kernel_ms": kernel_s * 1e3},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "path": "ebem_mesh_create + ebem_assemble_sa_panel into pinned host memory + ebem_mesh_destroy"},
+                    "path": "ebem_mesh_create + ebem_assemble_sa_panel into pinned host memory + ebem_mesh_destroy",
+                    "host_link_d2h_gbs": link_gbs,
+                    "copy_bound": total_pairs / (d2h / (link_gbs * 1e9))},
             "clocks": clocks,
         }
         if not args.no_forms and world == 1:

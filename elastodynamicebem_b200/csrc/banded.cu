@@ -115,13 +115,13 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(long long* __r
 static int exclusive_scan(long long* d, long long n, cudaStream_t s) {
     const long long nb = (n + kScanBlock - 1) / kScanBlock;
     long long* sums = nullptr;
-    EBEM_CUDA_TRY(cudaMalloc(&sums, nb * sizeof(long long)));
+    EBEM_CUDA_TRY(ws_malloc(&sums, nb * sizeof(long long), s));
     scan_sums_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(d, n, sums);
     scan_top_kernel<<<1, 1024, 0, s>>>(sums, nb);
     scan_apply_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(d, n, sums);
     cudaError_t e = cudaGetLastError();
+    ws_free(sums, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(sums);
     if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("band structure scan: ") + cudaGetErrorString(e));
     return EBEM_OK;
 }
@@ -299,18 +299,16 @@ int band_march(const BandOp& op, const double* d_rhs, int nT, double* d_phi, cud
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long NN = (long long)N * N;
-    if (cudaMalloc(&E0, (size_t)n3 * n3 * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&phiT, (size_t)n3 * nT * sizeof(double)) != cudaSuccess) {
-        cudaGetLastError();
-        if (E0) cudaFree(E0);
-        if (phiT) cudaFree(phiT);
+    if (ws_malloc(&E0, (size_t)n3 * n3 * sizeof(double), s) != cudaSuccess ||
+        ws_malloc(&phiT, (size_t)n3 * nT * sizeof(double), s) != cudaSuccess) {
+        ws_free(E0, s);
         return fail(EBEM_ERR_NOMEM, "banded marching workspace allocation failed");
     }
     cudaMemsetAsync(E0, 0, (size_t)n3 * n3 * sizeof(double), s);
     band_e0_kernel<<<(unsigned)((NN + 127) / 128), 128, 0, s>>>(op.Eb, op.off, op.lo, N, E0);
     if (cudaGetLastError() != cudaSuccess) rc = fail(EBEM_ERR_CUDA, "E_0 expansion failed");
     if (!rc) rc = lu_plan_create(E0, n3, s, &lu);
-    cudaFree(E0);
+    ws_free(E0, s);
     // each source row split over enough warps to keep about 48 warps per SM
     // streaming (one warp per row leaves HBM idle when N is small)
     const int nchunk = (N + 31) / 32;
@@ -333,7 +331,7 @@ int band_march(const BandOp& op, const double* d_rhs, int nT, double* d_phi, cud
     }
     if (!rc && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(EBEM_ERR_CUDA, "banded marching failed");
     lu_plan_destroy(&lu);
-    cudaFree(phiT);
+    ws_free(phiT, s);
     return rc;
 }
 

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <initializer_list>
+#include <mutex>
 
 struct ebem_mesh {
     ebem::MeshData d;
@@ -25,6 +26,52 @@ int fail(int code, const std::string& msg) {
     g_last_error = msg;
     return code;
 }
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxDevices] = {};
+
+// The workspace pool of device dev, created on first use.
+cudaError_t workspace_pool(int dev, cudaMemPool_t* pool) {
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&p, &props);
+        if (e != cudaSuccess) return e;
+        unsigned long long keep = kWorkspaceKeep;
+        e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(p);
+            return e;
+        }
+        g_pool[dev] = p;
+    }
+    *pool = g_pool[dev];
+    return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t ws_malloc(void** p, size_t bytes, cudaStream_t s) {
+    *p = nullptr;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    cudaMemPool_t pool = nullptr;
+    if (e == cudaSuccess) e = workspace_pool(dev, &pool);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes > 0 ? bytes : 1, pool, s);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+    }
+    return e;
+}
+
+cudaError_t ws_free(void* p, cudaStream_t s) { return p ? cudaFreeAsync(p, s) : cudaSuccess; }
 
 PhysParams phys_from(const ebem_problem* p) {
     PhysParams P;
@@ -97,17 +144,17 @@ __global__ void max_vertex_dist_kernel(const double* __restrict__ c, int nv, uns
 struct DevIn {
     const double* d = nullptr;
     double* owned = nullptr;
+    cudaStream_t st = nullptr;
     int init(const double* p, size_t n, cudaStream_t s) {
         if (is_device_ptr(p)) { d = p; return EBEM_OK; }
-        if (cudaMalloc(&owned, n * sizeof(double)) != cudaSuccess) {
-            cudaGetLastError();
+        st = s;
+        if (ws_malloc(&owned, n * sizeof(double), s) != cudaSuccess)
             return fail(EBEM_ERR_NOMEM, "device staging allocation failed");
-        }
         EBEM_CUDA_TRY(cudaMemcpyAsync(owned, p, n * sizeof(double), cudaMemcpyHostToDevice, s));
         d = owned;
         return EBEM_OK;
     }
-    ~DevIn() { if (owned) cudaFree(owned); }
+    ~DevIn() { ws_free(owned, st); }
 };
 
 // A host-or-device output array: device pointer used directly, host pointer
@@ -116,15 +163,14 @@ struct DevOut {
     double* d = nullptr;
     double* host = nullptr;
     size_t n = 0;
-    int init(double* p, size_t count) {
+    cudaStream_t st = nullptr;
+    int init(double* p, size_t count, cudaStream_t s) {
         n = count;
         if (is_device_ptr(p)) { d = p; return EBEM_OK; }
         host = p;
-        if (cudaMalloc(&d, n * sizeof(double)) != cudaSuccess) {
-            cudaGetLastError();
-            d = nullptr;
+        st = s;
+        if (ws_malloc(&d, n * sizeof(double), s) != cudaSuccess)
             return fail(EBEM_ERR_NOMEM, "device staging allocation failed");
-        }
         return EBEM_OK;
     }
     int finish(cudaStream_t s) {
@@ -134,7 +180,7 @@ struct DevOut {
         }
         return EBEM_OK;
     }
-    ~DevOut() { if (host && d) cudaFree(d); }
+    ~DevOut() { if (host) ws_free(d, st); }
 };
 
 }  // namespace
@@ -147,6 +193,24 @@ extern "C" {
 int ebem_version(void) { return EBEM_VERSION; }
 
 const char* ebem_last_error(void) { return g_last_error.c_str(); }
+
+int ebem_release_workspace(void) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    for (int dev = 0; dev < kMaxDevices; dev++) {
+        if (!g_pool[dev]) continue;
+        cudaError_t e = cudaSetDevice(dev);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemPoolTrimTo(g_pool[dev], 0);
+        if (e != cudaSuccess) {
+            if (prev >= 0) cudaSetDevice(prev);
+            return fail(EBEM_ERR_CUDA, std::string("workspace release: ") + cudaGetErrorString(e));
+        }
+    }
+    if (prev >= 0) cudaSetDevice(prev);
+    return EBEM_OK;
+}
 
 int ebem_quad_gh(int n_nodes, int n_sub, double* nodes, double* weights) {
     if (!nodes || !weights) return fail(EBEM_ERR_INVALID, "NULL output");
@@ -246,15 +310,15 @@ int ebem_num_blocks(const ebem_mesh* m, const ebem_problem* p, int* num_blocks) 
     if (int rc = check_problem(p)) return rc;
     DeviceGuard dg(m->d.device);
     unsigned long long* d = nullptr;
-    EBEM_CUDA_TRY(cudaMalloc(&d, sizeof(unsigned long long)));
+    EBEM_CUDA_TRY(ws_malloc(&d, sizeof(unsigned long long), 0));
     unsigned long long bits = 0;
-    cudaError_t e = cudaMemset(d, 0, sizeof(unsigned long long));
+    cudaError_t e = cudaMemsetAsync(d, 0, sizeof(unsigned long long), 0);
     if (e == cudaSuccess) {
         max_vertex_dist_kernel<<<296, 256>>>(m->d.d_coords, m->d.nv, d);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost);
-    cudaFree(d);
+    ws_free(d, 0);
     if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, cudaGetErrorString(e));
     double maxD;
     std::memcpy(&maxD, &bits, sizeof(double));
@@ -284,10 +348,10 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
     const size_t lag_elems = (size_t)ld * n3;
     unsigned long long* d_count = nullptr;
     if (nonnull) {
-        EBEM_CUDA_TRY(cudaMalloc(&d_count, sizeof(unsigned long long)));
+        EBEM_CUDA_TRY(ws_malloc(&d_count, sizeof(unsigned long long), s));
         cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
         if (e != cudaSuccess) {
-            cudaFree(d_count);
+            ws_free(d_count, s);
             return fail(EBEM_ERR_CUDA, std::string("pair counter: ") + cudaGetErrorString(e));
         }
     }
@@ -297,7 +361,7 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
                                 prec == EBEM_PREC_MIXED);
     } else {
         if (ld != 3LL * nsrc) {
-            if (d_count) cudaFree(d_count);
+            ws_free(d_count, s);
             return fail(EBEM_ERR_INVALID, "host output needs ld == 3 nsrc");
         }
         // host output: source-row sub-panels are assembled into two device
@@ -313,8 +377,8 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
         double* buf[2] = {nullptr, nullptr};
         cudaStream_t cs = nullptr;
         cudaEvent_t done[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
-        bool ok = cudaMalloc(&buf[0], per_row * rows) == cudaSuccess &&
-                  (rows >= nsrc || cudaMalloc(&buf[1], per_row * rows) == cudaSuccess) &&
+        bool ok = ws_malloc(&buf[0], per_row * rows, s) == cudaSuccess &&
+                  (rows >= nsrc || ws_malloc(&buf[1], per_row * rows, s) == cudaSuccess) &&
                   cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess;
         for (int b = 0; ok && b < 2; b++)
             ok = cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming) == cudaSuccess &&
@@ -350,7 +414,7 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
         for (int b = 0; b < 2; b++) {
             if (done[b]) cudaEventDestroy(done[b]);
             if (copied[b]) cudaEventDestroy(copied[b]);
-            if (buf[b]) cudaFree(buf[b]);
+            ws_free(buf[b], s);          // both streams have finished with it
         }
         if (cs) cudaStreamDestroy(cs);
         if (rc == EBEM_OK && e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, cudaGetErrorString(e));
@@ -359,7 +423,7 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
         unsigned long long c = 0;
         cudaError_t e = cudaMemcpyAsync(&c, d_count, sizeof(c), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        cudaFree(d_count);
+        ws_free(d_count, s);
         if (rc == EBEM_OK && e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, cudaGetErrorString(e));
         *nonnull = (long long)c;
     }
@@ -387,7 +451,7 @@ int ebem_assemble_ghc(const ebem_mesh* m, const ebem_problem* p, int n_gh, int n
     PhysParams P = phys_from(p);
     const size_t n3 = 3 * (size_t)md.nt;
     DevOut out;
-    if (int rc = out.init(E, n3 * n3 * nlag)) return rc;
+    if (int rc = out.init(E, n3 * n3 * nlag, s)) return rc;
     if (out.host) EBEM_CUDA_TRY(cudaMemcpyAsync(out.d, E, n3 * n3 * nlag * sizeof(double), cudaMemcpyHostToDevice, s));
     if (int rc = launch_ghc_assemble(md, P, n_gh, n_sub, n_sing, lag0, nlag, out.d, n3, n3 * n3, s)) return rc;
     if (sa_diagonal) {
@@ -410,7 +474,7 @@ int ebem_rhs(const ebem_mesh* m, const ebem_problem* p, int n_gh, int datum, dou
     if (int rc = map_nodes(md, n_gh, s)) return rc;
     PhysParams P = phys_from(p);
     DevOut out;
-    if (int rc = out.init(rhs, 3 * (size_t)md.nt * P.nT)) return rc;
+    if (int rc = out.init(rhs, 3 * (size_t)md.nt * P.nT, s)) return rc;
     if (int rc = launch_rhs(md, P, n_gh, datum, out.d, s)) return rc;
     return out.finish(s);
 }
@@ -423,7 +487,7 @@ int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double
     if (int rc = dE.init(E, (size_t)n3 * n3 * L, s)) return rc;
     if (int rc = dr.init(rhs, (size_t)n3 * nT, s)) return rc;
     DevOut out;
-    if (int rc = out.init(phi, (size_t)n3 * nT)) return rc;
+    if (int rc = out.init(phi, (size_t)n3 * nT, s)) return rc;
     if (int rc = march_device(dE.d, n3, L, dr.d, nT, out.d, s)) return rc;
     return out.finish(s);
 }
@@ -482,7 +546,7 @@ int ebem_banded_to_dense(const ebem_banded* b, int lag0, int nlag, double* E, vo
     cudaStream_t s = (cudaStream_t)stream;
     const size_t n3 = 3 * (size_t)b->op.N;
     DevOut out;
-    if (int rc = out.init(E, n3 * n3 * nlag)) return rc;
+    if (int rc = out.init(E, n3 * n3 * nlag, s)) return rc;
     if (int rc = band_to_dense(b->op, lag0, nlag, out.d, s)) return rc;
     return out.finish(s);
 }
@@ -495,7 +559,7 @@ int ebem_banded_march(const ebem_banded* b, const double* rhs, int nT, double* p
     DevIn dr;
     if (int rc = dr.init(rhs, n3 * nT, s)) return rc;
     DevOut out;
-    if (int rc = out.init(phi, n3 * nT)) return rc;
+    if (int rc = out.init(phi, n3 * nT, s)) return rc;
     if (int rc = band_march(b->op, dr.d, nT, out.d, s)) return rc;
     return out.finish(s);
 }
@@ -608,7 +672,7 @@ int ebem_pp_sa(const ebem_mesh* m, const ebem_problem* p, const double* phi, con
     if (int rc = dphi.init(phi, 3 * (size_t)m->d.nt * P.nT, s)) return rc;
     if (int rc = dpts.init(pts, 3 * (size_t)npts, s)) return rc;
     DevOut out;
-    if (int rc = out.init(u, 3 * (size_t)npts * ntimes)) return rc;
+    if (int rc = out.init(u, 3 * (size_t)npts * ntimes, s)) return rc;
     if (int rc = launch_pp_sa(m->d, P, dphi.d, dpts.d, npts, times, ntimes, out.d, s)) return rc;
     return out.finish(s);
 }
@@ -659,7 +723,7 @@ int ebem_assemble_k(const ebem_mesh* m, const ebem_problem* p, int n_gh, int n_s
     PhysParams P = phys_from(p);
     const size_t n = 9 * (size_t)md.nt * md.nv * nlag;
     DevOut out;
-    if (int rc = out.init(K, n)) return rc;
+    if (int rc = out.init(K, n, s)) return rc;
     if (accumulate) {
         if (out.host) EBEM_CUDA_TRY(cudaMemcpyAsync(out.d, K, n * sizeof(double), cudaMemcpyHostToDevice, s));
     } else {
@@ -685,7 +749,7 @@ int ebem_assemble_v(const ebem_mesh* m, const ebem_problem* p, int n_gh, int n_s
     PhysParams P = phys_from(p);
     const size_t n3 = 3 * (size_t)md.nt;
     DevOut out;
-    if (int rc = out.init(V, n3 * n3 * nlag)) return rc;
+    if (int rc = out.init(V, n3 * n3 * nlag, s)) return rc;
     EBEM_CUDA_TRY(cudaMemsetAsync(out.d, 0, n3 * n3 * nlag * sizeof(double), s));
     if (int rc = launch_ghc_assemble(md, P, n_gh, n_sub, n_sing, lag0, nlag, out.d, n3, n3 * n3, s)) return rc;
     if (int rc = launch_v_diag(md, P, n_gh, n_diag, lag0, nlag, out.d, s)) return rc;
@@ -706,7 +770,7 @@ int ebem_march_dn(const ebem_mesh* m, const ebem_problem* p, const double* V, in
     if (int rc = dK.init(K, R * Cn * LK, s)) return rc;
     if (int rc = dgv.init(gV, R * p->nt, s)) return rc;
     DevOut out;
-    if (int rc = out.init(u, Cn * p->nt)) return rc;
+    if (int rc = out.init(u, Cn * p->nt, s)) return rc;
     if (int rc = march_dn_device(md, dV.d, LV, dK.d, LK, dgv.d, p->nt, out.d, s)) return rc;
     return out.finish(s);
 }
@@ -726,7 +790,7 @@ int ebem_march_dd(const ebem_mesh* m, const ebem_problem* p, const double* V, in
     if (int rc = dr.init(rhs, R * p->nt, s)) return rc;
     if (int rc = dgk.init(gK, Cn * p->nt, s)) return rc;
     DevOut out;
-    if (int rc = out.init(phi, R * p->nt)) return rc;
+    if (int rc = out.init(phi, R * p->nt, s)) return rc;
     if (int rc = march_dd_device(md, dV.d, LV, dK.d, LK, dr.d, dgk.d, p->nt, out.d, s)) return rc;
     return out.finish(s);
 }
@@ -749,7 +813,7 @@ int ebem_pp_dir(const ebem_mesh* m, const ebem_problem* p, int n_sub, int n_sing
     if (int rc = db.init(b, 3 * (size_t)md.nv * P.nT, s)) return rc;
     if (int rc = dp.init(pts, 3 * (size_t)npts, s)) return rc;
     DevOut out;
-    if (int rc = out.init(u, 3 * (size_t)npts * ntimes)) return rc;
+    if (int rc = out.init(u, 3 * (size_t)npts * ntimes, s)) return rc;
     if (int rc = launch_pp_dir(md, P, n_sub, n_sing, flags & EBEM_FIX_REFERENCE_DEFECTS, dp.d, npts, times, ntimes, da.d,
                                db.d, out.d, nullptr, nullptr, 0, s))
         return rc;
@@ -771,8 +835,8 @@ int ebem_pp_dir_matrices(const ebem_mesh* m, const ebem_problem* p, int n_sub, i
     DevIn dx;
     if (int rc = dx.init(x, 3, s)) return rc;
     DevOut oG, oP;
-    if (int rc = oG.init(G, 9 * (size_t)nhat * md.nt)) return rc;
-    if (int rc = oP.init(Pm, 9 * (size_t)nhat * md.nv)) return rc;
+    if (int rc = oG.init(G, 9 * (size_t)nhat * md.nt, s)) return rc;
+    if (int rc = oP.init(Pm, 9 * (size_t)nhat * md.nv, s)) return rc;
     EBEM_CUDA_TRY(cudaMemsetAsync(oG.d, 0, 9 * (size_t)nhat * md.nt * sizeof(double), s));
     EBEM_CUDA_TRY(cudaMemsetAsync(oP.d, 0, 9 * (size_t)nhat * md.nv * sizeof(double), s));
     if (int rc = launch_pp_dir(md, P, n_sub, n_sing, flags & EBEM_FIX_REFERENCE_DEFECTS, dx.d, 1, &t, 1, nullptr,

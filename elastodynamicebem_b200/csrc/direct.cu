@@ -699,7 +699,8 @@ __global__ void __launch_bounds__(128) v_diag_kernel(const DirTri* __restrict__ 
 struct Tables {
     double* d = nullptr;
     size_t outer = 0, wout = 0, inner = 0, win = 0, dn = 0, dw = 0;
-    ~Tables() { if (d) cudaFree(d); }
+    cudaStream_t st = nullptr;
+    ~Tables() { ws_free(d, st); }
 };
 
 static int upload_tables(Tables& T, int n_gh, int n_sub, int n_sing, int n_diag, cudaStream_t s) {
@@ -723,7 +724,8 @@ static int upload_tables(Tables& T, int n_gh, int n_sub, int n_sing, int n_diag,
         T.dw = buf.size(); buf.insert(buf.end(), dw.begin(), dw.end());
     }
     if (buf.empty()) buf.push_back(0.0);
-    EBEM_CUDA_TRY(cudaMalloc(&T.d, buf.size() * sizeof(double)));
+    T.st = s;
+    EBEM_CUDA_TRY(ws_malloc(&T.d, buf.size() * sizeof(double), s));
     EBEM_CUDA_TRY(cudaMemcpyAsync(T.d, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     return EBEM_OK;
 }
@@ -974,7 +976,7 @@ int launch_pp_dir(const MeshData& m, const PhysParams& P, int n_sub, int n_sing,
     Tables T;
     if (int rc = upload_tables(T, 0, n_sub, n_sing, 0, s)) return rc;
     double* d_times = nullptr;
-    EBEM_CUDA_TRY(cudaMalloc(&d_times, sizeof(double) * ntimes));
+    EBEM_CUDA_TRY(ws_malloc(&d_times, sizeof(double) * ntimes, s));
     cudaError_t e = cudaMemcpyAsync(d_times, h_times, sizeof(double) * ntimes, cudaMemcpyHostToDevice, s);
     PPArgs A;
     A.tri = m.d_dir;
@@ -1009,9 +1011,9 @@ int launch_pp_dir(const MeshData& m, const PhysParams& P, int n_sub, int n_sing,
             pp_p_kernel<<<gp, 128, 0, s>>>(A);
             e = cudaGetLastError();
         }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     }
-    cudaFree(d_times);
+    ws_free(d_times, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("direct post-processing: ") + cudaGetErrorString(e));
     return EBEM_OK;
 }
@@ -1083,10 +1085,10 @@ int march_dn_device(const MeshData& m, const double* dV, int LV, const double* d
         if (e != cudaSuccess && rc == EBEM_OK) rc = fail(EBEM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
         return rc == EBEM_OK;
     };
-    if (!cu(cudaMalloc(&A, sizeof(double) * (size_t)R * Cn), "alloc") || !cu(cudaMalloc(&tau, sizeof(double) * Cn), "alloc") ||
-        !cu(cudaMalloc(&beta, sizeof(double) * (size_t)R * nT), "alloc") ||
-        !cu(cudaMalloc(&rev, sizeof(double) * (size_t)Cn * nT), "alloc") || !cu(cudaMalloc(&y, sizeof(double) * R), "alloc") ||
-        !cu(cudaMalloc(&info, sizeof(int)), "alloc")) {
+    if (!cu(ws_malloc(&A, sizeof(double) * (size_t)R * Cn, s), "alloc") || !cu(ws_malloc(&tau, sizeof(double) * Cn, s), "alloc") ||
+        !cu(ws_malloc(&beta, sizeof(double) * (size_t)R * nT, s), "alloc") ||
+        !cu(ws_malloc(&rev, sizeof(double) * (size_t)Cn * nT, s), "alloc") || !cu(ws_malloc(&y, sizeof(double) * R, s), "alloc") ||
+        !cu(ws_malloc(&info, sizeof(int), s), "alloc")) {
         rc = fail(EBEM_ERR_NOMEM, "direct time-marching workspace allocation failed");
         goto done;
     }
@@ -1110,7 +1112,7 @@ int march_dn_device(const MeshData& m, const double* dV, int LV, const double* d
         goto done;
     }
     lwork = std::max(lwork, lw2);
-    if (!cu(cudaMalloc(&work, sizeof(double) * (size_t)std::max(lwork, 1)), "alloc")) goto done;
+    if (!cu(ws_malloc(&work, sizeof(double) * (size_t)std::max(lwork, 1), s), "alloc")) goto done;
     if (cusolverDnDgeqrf(hs, R, Cn, A, R, tau, work, lwork, info) != CUSOLVER_STATUS_SUCCESS) {
         rc = fail(EBEM_ERR_CUDA, "QR factorisation failed");
         goto done;
@@ -1147,7 +1149,7 @@ int march_dn_device(const MeshData& m, const double* dV, int LV, const double* d
 done:
     if (hs) cusolverDnDestroy(hs);
     if (hb) cublasDestroy(hb);
-    cudaFree(A); cudaFree(tau); cudaFree(work); cudaFree(beta); cudaFree(rev); cudaFree(y); cudaFree(info);
+    ws_free(A, s); ws_free(tau, s); ws_free(work, s); ws_free(beta, s); ws_free(rev, s); ws_free(y, s); ws_free(info, s);
     return rc;
 }
 
@@ -1162,12 +1164,10 @@ int march_dd_device(const MeshData& m, const double* dV, int LV, const double* d
     double* b = nullptr;
     cublasHandle_t hb = nullptr;
     int rc = EBEM_OK;
-    if (cudaMalloc(&b, sizeof(double) * (size_t)R * nT) != cudaSuccess) {
-        cudaGetLastError();
+    if (ws_malloc(&b, sizeof(double) * (size_t)R * nT, s) != cudaSuccess)
         return fail(EBEM_ERR_NOMEM, "right-hand side allocation failed");
-    }
     if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) {
-        cudaFree(b);
+        ws_free(b, s);
         return fail(EBEM_ERR_CUDA, "cuBLAS handle creation failed");
     }
     cublasSetStream(hb, s);
@@ -1182,7 +1182,7 @@ int march_dd_device(const MeshData& m, const double* dV, int LV, const double* d
     if (!rc) rc = march_device(dV, R, LV, b, nT, d_phi, s);
     cudaStreamSynchronize(s);
     cublasDestroy(hb);
-    cudaFree(b);
+    ws_free(b, s);
     return rc;
 }
 

@@ -19,6 +19,21 @@ namespace ebem {
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 
+// Per-call device workspace, stream-ordered, from a memory pool the library
+// keeps for each device.  Up to kWorkspaceKeep bytes stay reserved in the pool
+// between calls, so a repeated call allocates without a driver call and
+// without the device-wide synchronisation of cudaMalloc / cudaFree.  A buffer
+// is released with ws_free on the stream that last uses it (on the current
+// device, as when it was allocated).  ebem_release_workspace() hands the
+// reserved memory back.
+constexpr unsigned long long kWorkspaceKeep = 2ull << 30;
+cudaError_t ws_malloc(void** p, size_t bytes, cudaStream_t s);
+cudaError_t ws_free(void* p, cudaStream_t s);
+template <class T>
+cudaError_t ws_malloc(T** p, size_t bytes, cudaStream_t s) {
+    return ws_malloc(reinterpret_cast<void**>(p), bytes, s);
+}
+
 #define EBEM_CUDA_TRY(expr)                                                        \
     do {                                                                           \
         cudaError_t _e = (expr);                                                   \

@@ -258,8 +258,11 @@ int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_
     for (double v : ib) tab[o++] = v;
     for (double v : iw) tab[o++] = v;
     double* d_tab = nullptr;
-    EBEM_CUDA_TRY(cudaMalloc(&d_tab, nb * sizeof(double)));
-    EBEM_CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), nb * sizeof(double), cudaMemcpyHostToDevice, s));
+    EBEM_CUDA_TRY(ws_malloc(&d_tab, nb * sizeof(double), s));
+    if (cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), nb * sizeof(double), cudaMemcpyHostToDevice, s)) {
+        ws_free(d_tab, s);
+        return fail(EBEM_ERR_CUDA, std::string("rule table upload: ") + cudaGetErrorString(e));
+    }
     GHCArgs A;
     A.coords = m.d_coords;
     A.tris = m.d_tris;
@@ -296,8 +299,8 @@ int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_
         ghc_assemble_kernel<<<(unsigned)((NN + threads - 1) / threads), threads, 0, s>>>(A);
     }
     cudaError_t e = cudaGetLastError();
+    ws_free(d_tab, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d_tab);
     if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("numerical-inner assembly: ") + cudaGetErrorString(e));
     return EBEM_OK;
 }

@@ -210,7 +210,7 @@ static int launch_rhs_test(const MeshData& m, const PhysParams& P, int n_gh, dou
     EBEM_CUDA_TRY(cudaMemcpyToSymbolAsync(c_gl16, gl, sizeof gl, 0, cudaMemcpyHostToDevice, s));
     double* d_S = nullptr;
     const size_t nS = 3 * (size_t)m.nt * (P.nT + 1);
-    EBEM_CUDA_TRY(cudaMalloc(&d_S, nS * sizeof(double)));
+    EBEM_CUDA_TRY(ws_malloc(&d_S, nS * sizeof(double), s));
     const int threads = 128;
     const long long lv = (long long)m.nt * (P.nT + 1), nb = 3LL * m.nt * P.nT;
     rhs_test_level_kernel<<<(unsigned)((lv + threads - 1) / threads), threads, 0, s>>>(
@@ -220,8 +220,8 @@ static int launch_rhs_test(const MeshData& m, const PhysParams& P, int n_gh, dou
         rhs_test_diff_kernel<<<(unsigned)((nb + threads - 1) / threads), threads, 0, s>>>(d_S, m.nt, P.nT, d_rhs);
         e = cudaGetLastError();
     }
+    ws_free(d_S, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d_S);
     if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("TEST right-hand side: ") + cudaGetErrorString(e));
     return EBEM_OK;
 }
@@ -327,9 +327,9 @@ int march_device(const double* dE, int n3, int L, const double* drhs, int nT, do
     const size_t nn = (size_t)n3 * n3;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaMalloc(&lu, nn * sizeof(double)) != cudaSuccess || cudaMalloc(&ipiv, n3 * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&info, sizeof(int)) != cudaSuccess || cudaMalloc(&rev, (size_t)n3 * nT * sizeof(double)) != cudaSuccess) {
-        cudaGetLastError();
+    if (ws_malloc(&lu, nn * sizeof(double), s) != cudaSuccess || ws_malloc(&ipiv, n3 * sizeof(int), s) != cudaSuccess ||
+        ws_malloc(&info, sizeof(int), s) != cudaSuccess ||
+        ws_malloc(&rev, (size_t)n3 * nT * sizeof(double), s) != cudaSuccess) {
         rc = fail(EBEM_ERR_NOMEM, "time-marching workspace allocation failed");
         goto done;
     }
@@ -340,8 +340,7 @@ int march_device(const double* dE, int n3, int L, const double* drhs, int nT, do
         goto done;
     }
     CUSOLVER_TRY(cusolverDnDgetrf_bufferSize(h, n3, n3, lu, n3, &lwork));
-    if (cudaMalloc(&work, (size_t)(lwork > 0 ? lwork : 1) * sizeof(double)) != cudaSuccess) {
-        cudaGetLastError();
+    if (ws_malloc(&work, (size_t)(lwork > 0 ? lwork : 1) * sizeof(double), s) != cudaSuccess) {
         rc = fail(EBEM_ERR_NOMEM, "LU workspace allocation failed");
         goto done;
     }
@@ -376,11 +375,11 @@ int march_device(const double* dE, int n3, int L, const double* drhs, int nT, do
     }
 done:
     if (h) cusolverDnDestroy(h);
-    if (lu) cudaFree(lu);
-    if (work) cudaFree(work);
-    if (rev) cudaFree(rev);
-    if (ipiv) cudaFree(ipiv);
-    if (info) cudaFree(info);
+    ws_free(lu, s);
+    ws_free(work, s);
+    ws_free(rev, s);
+    ws_free(ipiv, s);
+    ws_free(info, s);
     return rc;
 }
 
@@ -628,13 +627,12 @@ static int launch_pp_sa_shared(const MeshData& m, const PhysParams& P, const dou
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)npts, ((size_t)1 << 30) / per_point));
     int *d_tab = nullptr, *d_nh = nullptr;
     double *d_taus = nullptr, *Mbuf = nullptr;
-    if (cudaMalloc(&d_tab, tab.size() * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&d_nh, ntimes * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&d_taus, nu * sizeof(double)) != cudaSuccess || cudaMalloc(&Mbuf, per_point * chunk) != cudaSuccess) {
-        cudaGetLastError();
-        if (d_tab) cudaFree(d_tab);
-        if (d_nh) cudaFree(d_nh);
-        if (d_taus) cudaFree(d_taus);
+    if (ws_malloc(&d_tab, tab.size() * sizeof(int), s) != cudaSuccess ||
+        ws_malloc(&d_nh, ntimes * sizeof(int), s) != cudaSuccess ||
+        ws_malloc(&d_taus, nu * sizeof(double), s) != cudaSuccess || ws_malloc(&Mbuf, per_point * chunk, s) != cudaSuccess) {
+        ws_free(d_tab, s);
+        ws_free(d_nh, s);
+        ws_free(d_taus, s);
         return fail(EBEM_ERR_NOMEM, "post-processing workspace allocation failed");
     }
     cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice, s);
@@ -650,11 +648,11 @@ static int launch_pp_sa_shared(const MeshData& m, const PhysParams& P, const dou
                                                                               npts, d_phi, d_u);
         e = cudaGetLastError();
     }
+    ws_free(Mbuf, s);
+    ws_free(d_taus, s);
+    ws_free(d_tab, s);
+    ws_free(d_nh, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(Mbuf);
-    cudaFree(d_taus);
-    cudaFree(d_tab);
-    cudaFree(d_nh);
     if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("post-processing kernels: ") + cudaGetErrorString(e));
     return EBEM_OK;
 }
@@ -665,21 +663,23 @@ int launch_pp_sa(const MeshData& m, const PhysParams& P, const double* d_phi, co
         const int rc = launch_pp_sa_shared(m, P, d_phi, d_pts, npts, h_times, ntimes, d_u, s);
         if (rc != 1) return rc;                         // done (or failed); 1: instants barely repeat
     }
-    double* d_times = nullptr;
-    EBEM_CUDA_TRY(cudaMalloc(&d_times, sizeof(double) * ntimes));
-    EBEM_CUDA_TRY(cudaMemcpyAsync(d_times, h_times, sizeof(double) * ntimes, cudaMemcpyHostToDevice, s));
-    EBEM_CUDA_TRY(cudaMemsetAsync(d_u, 0, sizeof(double) * 3 * (size_t)npts * ntimes, s));
     long long total = (long long)m.nt * npts * ntimes;
     int threads = 128;
-    if ((total + threads - 1) / threads > 0x7fffffffLL) {
-        cudaFree(d_times);
+    if ((total + threads - 1) / threads > 0x7fffffffLL)
         return fail(EBEM_ERR_INVALID, "too many (triangle, point, time) triples for one launch");
+    double* d_times = nullptr;
+    EBEM_CUDA_TRY(ws_malloc(&d_times, sizeof(double) * ntimes, s));
+    cudaError_t e = cudaMemcpyAsync(d_times, h_times, sizeof(double) * ntimes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_u, 0, sizeof(double) * 3 * (size_t)npts * ntimes, s);
+    if (e != cudaSuccess) {
+        ws_free(d_times, s);
+        return fail(EBEM_ERR_CUDA, std::string("post-processing set-up: ") + cudaGetErrorString(e));
     }
     pp_sa_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, s>>>(
         m.d_geo, m.nt, d_pts, npts, d_times, ntimes, d_phi, P.nT, P.velP, P.velS, P.dt, 4 * kPi * P.rho, d_u);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
+    ws_free(d_times, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d_times);
     if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("post-processing kernel: ") + cudaGetErrorString(e));
     return EBEM_OK;
 }

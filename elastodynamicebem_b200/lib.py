@@ -29,6 +29,7 @@ class ProblemC(C.Structure):
 PROTOTYPES = {
     "ebem_version": (C.c_int, []),
     "ebem_last_error": (C.c_char_p, []),
+    "ebem_release_workspace": (C.c_int, []),
     "ebem_quad_gh": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ebem_mesh_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "ebem_mesh_destroy": (C.c_int, [C.c_void_p]),

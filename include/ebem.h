@@ -64,6 +64,13 @@ int ebem_version(void);
 /* Message of the last failing call on this thread ("" if none). */
 const char* ebem_last_error(void);
 
+/* Per-call device workspace comes from a stream-ordered memory pool that the
+ * library keeps for each device; up to 2 GiB per device stay reserved between
+ * calls so that repeated calls neither allocate nor synchronise the device.
+ * ebem_release_workspace returns every device's reserved workspace memory
+ * that no call in flight uses (after the calls in flight have finished). */
+int ebem_release_workspace(void);
+
 /* Gauss-Hammer composite rule.  Replaces f/utility/quadRules/
  * GaussHammerComposite.m:1 (with the base tables of GaussHammer_base.m).
  * n_nodes in {1,3,7,12,19,28}; n_sub in {1,4,16,64,...} (a square);

@@ -132,3 +132,23 @@ def test_pp_grid_and_off_grid_times(ebem, oracle):
         uo = oracle.pp_sa(m, prm, phi.cpu().numpy().T, pts, times).transpose(2, 1, 0)
         assert np.abs(u[0]).max() == 0.0 if times[0] == 0.0 else True
         assert rel(u, uo) <= 1e-9
+
+
+def test_workspace_pool_reuse_and_release(ebem, oracle):
+    """Per-call workspaces come from the library's stream-ordered pool: repeated
+    calls reuse it, ebem_release_workspace hands it back, and calls after the
+    release allocate again; every call gives the same displacement (to
+    rounding: the per-time path adds with atomics)."""
+    from elastodynamicebem_b200 import lib, problem
+    w = problem.screen_workload()
+    dm = ebem.DeviceMesh(w.mesh)
+    phi, L = ebem.timemarch_sa(dm, w.params, 7, w.datum)
+    pts, times = w.points[:16], w.times
+    u1 = ebem.pp_sa(dm, w.params, phi, pts, times).cpu().numpy()
+    u2 = ebem.pp_sa(dm, w.params, phi, pts, times).cpu().numpy()
+    lib.check(lib.load().ebem_release_workspace())
+    u3 = ebem.pp_sa(dm, w.params, phi, pts, times).cpu().numpy()
+    # the history product adds with atomics: equal to rounding, not bitwise
+    assert rel(u2, u1) <= 1e-13 and rel(u3, u1) <= 1e-13
+    phi2, _ = ebem.timemarch_sa(dm, w.params, 7, w.datum)
+    assert rel(phi2.cpu().numpy(), phi.cpu().numpy()) <= 1e-13
