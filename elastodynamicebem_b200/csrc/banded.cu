@@ -307,7 +307,7 @@ int band_march(const BandOp& op, const double* d_rhs, int nT, double* d_phi, cud
     cudaMemsetAsync(E0, 0, (size_t)n3 * n3 * sizeof(double), s);
     band_e0_kernel<<<(unsigned)((NN + 127) / 128), 128, 0, s>>>(op.Eb, op.off, op.lo, N, E0);
     if (cudaGetLastError() != cudaSuccess) rc = fail(EBEM_ERR_CUDA, "E_0 expansion failed");
-    if (!rc) rc = lu_plan_create(E0, n3, s, &lu);
+    if (!rc) rc = lu_plan_create(E0, n3, s, &lu, true);
     ws_free(E0, s);
     // each source row split over enough warps to keep about 48 warps per SM
     // streaming (one warp per row leaves HBM idle when N is small)

@@ -1078,45 +1078,60 @@ int march_dn_device(const MeshData& m, const double* dV, int LV, const double* d
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cusolverDnHandle_t hs = nullptr;
     cublasHandle_t hb = nullptr;
-    double *A = nullptr, *tau = nullptr, *work = nullptr, *beta = nullptr, *rev = nullptr, *y = nullptr;
+    double *A = nullptr, *Q = nullptr, *X = nullptr, *tau = nullptr, *work = nullptr, *beta = nullptr, *rev = nullptr,
+           *y = nullptr;
     int* info = nullptr;
-    const double one = 1.0;
+    const double one = 1.0, zero = 0.0;
     auto cu = [&](cudaError_t e, const char* what) {
         if (e != cudaSuccess && rc == EBEM_OK) rc = fail(EBEM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
         return rc == EBEM_OK;
     };
-    if (!cu(ws_malloc(&A, sizeof(double) * (size_t)R * Cn, s), "alloc") || !cu(ws_malloc(&tau, sizeof(double) * Cn, s), "alloc") ||
+    auto blas_ok = [&](cublasStatus_t st, const char* what) {
+        if (st != CUBLAS_STATUS_SUCCESS && rc == EBEM_OK)
+            rc = fail(EBEM_ERR_CUDA, std::string(what) + " failed (cuBLAS status " + std::to_string((int)st) + ")");
+        return rc == EBEM_OK;
+    };
+    auto sol_ok = [&](cusolverStatus_t st, const char* what) {
+        if (st != CUSOLVER_STATUS_SUCCESS && rc == EBEM_OK)
+            rc = fail(EBEM_ERR_CUDA, std::string(what) + " failed (cuSOLVER status " + std::to_string((int)st) + ")");
+        return rc == EBEM_OK;
+    };
+    const size_t RC = (size_t)R * Cn;
+    if (!cu(ws_malloc(&A, sizeof(double) * RC, s), "alloc") || !cu(ws_malloc(&Q, sizeof(double) * RC, s), "alloc") ||
+        !cu(ws_malloc(&X, sizeof(double) * RC, s), "alloc") || !cu(ws_malloc(&tau, sizeof(double) * Cn, s), "alloc") ||
         !cu(ws_malloc(&beta, sizeof(double) * (size_t)R * nT, s), "alloc") ||
         !cu(ws_malloc(&rev, sizeof(double) * (size_t)Cn * nT, s), "alloc") || !cu(ws_malloc(&y, sizeof(double) * R, s), "alloc") ||
         !cu(ws_malloc(&info, sizeof(int), s), "alloc")) {
         rc = fail(EBEM_ERR_NOMEM, "direct time-marching workspace allocation failed");
         goto done;
     }
-    if (cusolverDnCreate(&hs) != CUSOLVER_STATUS_SUCCESS || cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) {
-        rc = fail(EBEM_ERR_CUDA, "cuSOLVER/cuBLAS handle creation failed");
-        goto done;
-    }
-    cusolverDnSetStream(hs, s);
-    cublasSetStream(hb, s);
+    if ((rc = solver_handle(s, &hs)) || (rc = blas_handle(s, &hb))) goto done;
     // beta_V,n = sum_j V_{n-j} g_j
     if (!cu(cudaMemsetAsync(beta, 0, sizeof(double) * (size_t)R * nT, s), "memset")) goto done;
     if ((rc = beta_gemm(hb, dV, LV, R, R, d_gV, nT, beta))) goto done;
-    // A = K_0 + I_Gamma, QR once
-    if (!cu(cudaMemcpyAsync(A, dK, sizeof(double) * (size_t)R * Cn, cudaMemcpyDeviceToDevice, s), "copy")) goto done;
+    // A = K_0 + I_Gamma = Q_1 R_1 (thin QR, once); the least-squares solution
+    // of every step is u = X y with X = R_1^{-1} Q_1^T (Cn x R), formed once
+    // (the reference solves (K_0 + I_Gamma) \ y densely at every step)
+    if (!cu(cudaMemcpyAsync(A, dK, sizeof(double) * RC, cudaMemcpyDeviceToDevice, s), "copy")) goto done;
     mass_add_kernel<<<(m.nt + 127) / 128, 128, 0, s>>>(m.d_dir, m.d_tris, m.nt, A);
     if (!cu(cudaGetLastError(), "mass matrix")) goto done;
-    if (cusolverDnDgeqrf_bufferSize(hs, R, Cn, A, R, &lwork) != CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnDormqr_bufferSize(hs, CUBLAS_SIDE_LEFT, CUBLAS_OP_T, R, 1, Cn, A, R, tau, y, R, &lw2) !=
-            CUSOLVER_STATUS_SUCCESS) {
-        rc = fail(EBEM_ERR_CUDA, "QR workspace query failed");
+    if (!sol_ok(cusolverDnDgeqrf_bufferSize(hs, R, Cn, A, R, &lwork), "QR workspace query") ||
+        !sol_ok(cusolverDnDorgqr_bufferSize(hs, R, Cn, Cn, A, R, tau, &lw2), "Q workspace query"))
         goto done;
-    }
     lwork = std::max(lwork, lw2);
     if (!cu(ws_malloc(&work, sizeof(double) * (size_t)std::max(lwork, 1), s), "alloc")) goto done;
-    if (cusolverDnDgeqrf(hs, R, Cn, A, R, tau, work, lwork, info) != CUSOLVER_STATUS_SUCCESS) {
-        rc = fail(EBEM_ERR_CUDA, "QR factorisation failed");
+    if (!sol_ok(cusolverDnDgeqrf(hs, R, Cn, A, R, tau, work, lwork, info), "QR factorisation")) goto done;
+    if (!cu(cudaMemcpyAsync(Q, A, sizeof(double) * RC, cudaMemcpyDeviceToDevice, s), "copy")) goto done;
+    if (!sol_ok(cusolverDnDorgqr(hs, R, Cn, Cn, Q, R, tau, work, lwork, info), "forming Q_1")) goto done;
+    // X = Q_1^T (transpose; X zeroed first although geam reads no B when
+    // beta = 0), then R_1 X = Q_1^T in place
+    if (!cu(cudaMemsetAsync(X, 0, sizeof(double) * RC, s), "memset")) goto done;
+    if (!blas_ok(cublasDgeam(hb, CUBLAS_OP_T, CUBLAS_OP_N, Cn, R, &one, Q, R, &zero, X, Cn, X, Cn), "transpose"))
         goto done;
-    }
+    if (!blas_ok(cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, Cn, R, &one,
+                             A, R, X, Cn),
+                 "triangular solve for X"))
+        goto done;
     // u in reversed time order: u_n at column nT-1-n
     if (!cu(cudaMemsetAsync(rev, 0, sizeof(double) * (size_t)Cn * nT, s), "memset")) goto done;
     for (int n = 0; n < nT; n++) {
@@ -1127,18 +1142,9 @@ int march_dn_device(const MeshData& m, const double* dV, int LV, const double* d
             if (!cu(cudaGetLastError(), "mass apply")) goto done;
         }
         const int M = std::min(n + 1, LK) - 1;          // K_1 .. K_M
-        if (M > 0 && (rc = launch_hist_gemv(dK + (size_t)R * Cn, R, (long long)Cn * M, un + Cn, y, sms, s))) goto done;
-        if (cusolverDnDormqr(hs, CUBLAS_SIDE_LEFT, CUBLAS_OP_T, R, 1, Cn, A, R, tau, y, R, work, lwork, info) !=
-            CUSOLVER_STATUS_SUCCESS) {
-            rc = fail(EBEM_ERR_CUDA, "Q^T application failed");
+        if (M > 0 && (rc = launch_hist_gemv(dK + RC, R, (long long)Cn * M, un + Cn, y, sms, s))) goto done;
+        if (!blas_ok(cublasDgemv(hb, CUBLAS_OP_N, Cn, R, &one, X, Cn, y, 1, &zero, un, 1), "least-squares product"))
             goto done;
-        }
-        if (cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, Cn, 1, &one, A, R,
-                        y, R) != CUBLAS_STATUS_SUCCESS) {
-            rc = fail(EBEM_ERR_CUDA, "triangular solve failed");
-            goto done;
-        }
-        if (!cu(cudaMemcpyAsync(un, y, sizeof(double) * Cn, cudaMemcpyDeviceToDevice, s), "copy")) goto done;
     }
     {
         const long long tot = (long long)Cn * nT;
@@ -1147,9 +1153,8 @@ int march_dn_device(const MeshData& m, const double* dV, int LV, const double* d
     }
     cu(cudaStreamSynchronize(s), "direct time marching");
 done:
-    if (hs) cusolverDnDestroy(hs);
-    if (hb) cublasDestroy(hb);
-    ws_free(A, s); ws_free(tau, s); ws_free(work, s); ws_free(beta, s); ws_free(rev, s); ws_free(y, s); ws_free(info, s);
+    ws_free(A, s); ws_free(Q, s); ws_free(X, s); ws_free(tau, s); ws_free(work, s); ws_free(beta, s); ws_free(rev, s);
+    ws_free(y, s); ws_free(info, s);
     return rc;
 }
 
@@ -1164,13 +1169,9 @@ int march_dd_device(const MeshData& m, const double* dV, int LV, const double* d
     double* b = nullptr;
     cublasHandle_t hb = nullptr;
     int rc = EBEM_OK;
+    if (int e = blas_handle(s, &hb)) return e;
     if (ws_malloc(&b, sizeof(double) * (size_t)R * nT, s) != cudaSuccess)
         return fail(EBEM_ERR_NOMEM, "right-hand side allocation failed");
-    if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) {
-        ws_free(b, s);
-        return fail(EBEM_ERR_CUDA, "cuBLAS handle creation failed");
-    }
-    cublasSetStream(hb, s);
     // b = rhs / 2 + beta_K, beta_K,n = sum_j K_{n-j} gK_j
     if (cudaMemsetAsync(b, 0, sizeof(double) * (size_t)R * nT, s) != cudaSuccess) rc = fail(EBEM_ERR_CUDA, "memset failed");
     if (!rc) rc = beta_gemm(hb, dK, LK, R, Cn, d_gK, nT, b);
@@ -1181,7 +1182,6 @@ int march_dd_device(const MeshData& m, const double* dV, int LV, const double* d
     }
     if (!rc) rc = march_device(dV, R, LV, b, nT, d_phi, s);
     cudaStreamSynchronize(s);
-    cublasDestroy(hb);
     ws_free(b, s);
     return rc;
 }

@@ -10,6 +10,7 @@
 #include "sa_device.cuh"
 
 struct cusolverDnContext;   // cuSOLVER dense handle (cusolverDnHandle_t)
+struct cublasContext;       // cuBLAS handle (cublasHandle_t)
 
 namespace ebem { struct NodeW; }
 
@@ -110,14 +111,22 @@ int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_
 
 int launch_rhs(const MeshData& m, const PhysParams& P, int n_gh, int datum, double* d_rhs, cudaStream_t s);
 int march_device(const double* dE, int n3, int L, const double* drhs, int nT, double* dphi, cudaStream_t s);
-// Device LU factors of one n x n matrix (cuSOLVER getrf once, getrs per solve).
+// A square system solved many times: A^{-1} formed once from the LU factors
+// (partial pivoting), so that each solve is one matrix-vector (or matrix)
+// product instead of a row-interchange pass and two triangular solves, which
+// for one right-hand side are latency-bound.  `pooled` plans (the marching's
+// own) keep the inverse in the workspace pool, released on `st`.
 struct LuPlan {
     int n = 0;
-    double* lu = nullptr;
-    int* ipiv = nullptr;
-    int* info = nullptr;
-    ::cusolverDnContext* h = nullptr;
+    double* inv = nullptr;      // A^{-1}, column-major n x n
+    bool pooled = false;
+    cudaStream_t st = nullptr;
 };
+// cuSOLVER / cuBLAS handles of the calling host thread on the current device,
+// created on first use and kept for the life of the thread (creating one costs
+// milliseconds and allocates device memory), bound to stream s on return.
+int solver_handle(cudaStream_t s, ::cusolverDnContext** h);
+int blas_handle(cudaStream_t s, ::cublasContext** h);
 // Banded Toeplitz blocks (csrc/banded.cu): pair p = i N + j owns the blocks
 // [off[p], off[p+1]) of Eb, one per lag of its band starting at lo[p], the 6
 // symmetric entries (11,12,13,22,23,33) of each.
@@ -134,7 +143,7 @@ int band_to_dense(const BandOp& op, int lag0, int nlag, double* d_E, cudaStream_
 int band_march(const BandOp& op, const double* d_rhs, int nT, double* d_phi, cudaStream_t s);
 int launch_sa_assemble_banded(const MeshData& m, const PhysParams& P, int n_gh, int L, double* d_Eb,
                               const long long* d_boff, const int* d_blo, int mixed, cudaStream_t s);
-int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan);
+int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan, bool pooled = false);
 int lu_plan_solve(LuPlan* plan, double* db, int nrhs, cudaStream_t s);
 void lu_plan_destroy(LuPlan* plan);
 int launch_pp_sa(const MeshData& m, const PhysParams& P, const double* d_phi, const double* d_pts, int npts,

@@ -11,6 +11,7 @@
 #include "ebem_internal.h"
 #include "sa_pair.cuh"
 
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
@@ -316,128 +317,185 @@ __global__ void copy_reverse_kernel(const double* __restrict__ src, double* __re
         }                                                                                         \
     } while (0)
 
+// ---------------------------------------------------------------------------
+// Library handles per host thread and device.  A thread-local table of plain
+// pointers: nothing is destroyed at thread or process exit (the driver
+// reclaims the handles with the context), so no handle outlives its CUDA
+// context in a destructor.
+namespace {
+constexpr int kHandleDevices = 64;
+struct ThreadHandles {
+    cusolverDnHandle_t sol[kHandleDevices];
+    cublasHandle_t blas[kHandleDevices];
+};
+thread_local ThreadHandles t_handles = {};
+
+int handle_device(int* dev) {
+    if (cudaGetDevice(dev) != cudaSuccess || *dev < 0 || *dev >= kHandleDevices) {
+        cudaGetLastError();
+        return fail(EBEM_ERR_CUDA, "no usable current device for a library handle");
+    }
+    return EBEM_OK;
+}
+}  // namespace
+
+int solver_handle(cudaStream_t s, cusolverDnHandle_t* h) {
+    int dev = 0;
+    if (int rc = handle_device(&dev)) return rc;
+    cusolverDnHandle_t& c = t_handles.sol[dev];
+    if (!c && cusolverDnCreate(&c) != CUSOLVER_STATUS_SUCCESS) {
+        c = nullptr;
+        return fail(EBEM_ERR_CUDA, "cuSOLVER handle creation failed");
+    }
+    if (cusolverDnSetStream(c, s) != CUSOLVER_STATUS_SUCCESS) return fail(EBEM_ERR_CUDA, "cuSOLVER stream binding failed");
+    *h = c;
+    return EBEM_OK;
+}
+
+int blas_handle(cudaStream_t s, cublasHandle_t* h) {
+    int dev = 0;
+    if (int rc = handle_device(&dev)) return rc;
+    cublasHandle_t& c = t_handles.blas[dev];
+    if (!c && cublasCreate(&c) != CUBLAS_STATUS_SUCCESS) {
+        c = nullptr;
+        return fail(EBEM_ERR_CUDA, "cuBLAS handle creation failed");
+    }
+    if (cublasSetStream(c, s) != CUBLAS_STATUS_SUCCESS) return fail(EBEM_ERR_CUDA, "cuBLAS stream binding failed");
+    *h = c;
+    return EBEM_OK;
+}
+
 // phi (device, column-major n3 x nT) from E (device, n3 x n3 x L) and rhs
-// (device, n3 x nT).
+// (device, n3 x nT): E_0^{-1} once, then per step the history product and
+// one product with E_0^{-1}.
 int march_device(const double* dE, int n3, int L, const double* drhs, int nT, double* dphi, cudaStream_t s) {
-    int rc = EBEM_OK;
-    cusolverDnHandle_t h = nullptr;
-    double *lu = nullptr, *work = nullptr, *rev = nullptr;
-    int *ipiv = nullptr, *info = nullptr;
-    int lwork = 0, hinfo = 0, dev = 0, sms = 148;
+    int rc = EBEM_OK, dev = 0, sms = 148;
+    double* rev = nullptr;
+    LuPlan lu;
     const size_t nn = (size_t)n3 * n3;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (ws_malloc(&lu, nn * sizeof(double), s) != cudaSuccess || ws_malloc(&ipiv, n3 * sizeof(int), s) != cudaSuccess ||
-        ws_malloc(&info, sizeof(int), s) != cudaSuccess ||
-        ws_malloc(&rev, (size_t)n3 * nT * sizeof(double), s) != cudaSuccess) {
-        rc = fail(EBEM_ERR_NOMEM, "time-marching workspace allocation failed");
+    if (ws_malloc(&rev, (size_t)n3 * nT * sizeof(double), s) != cudaSuccess)
+        return fail(EBEM_ERR_NOMEM, "time-marching workspace allocation failed");
+    rc = lu_plan_create(dE, n3, s, &lu, true);
+    if (!rc) {
+        // density in reversed time order: phi_n at column nT-1-n, so that
+        // phi_{n-1}, phi_{n-2}, ... are contiguous for the history product
+        const long long tot = (long long)n3 * nT;
+        copy_reverse_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(drhs, rev, n3, nT, 1);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(EBEM_ERR_CUDA, "rhs copy failed");
+        for (int n = 0; n < nT && !rc; n++) {
+            double* y = rev + (size_t)(nT - 1 - n) * n3;
+            const int M = (n < L - 1) ? n : L - 1;
+            if (M > 0) rc = launch_hist_gemv(dE + nn, n3, (long long)n3 * M, rev + (size_t)(nT - n) * n3, y, sms, s);
+            if (!rc) rc = lu_plan_solve(&lu, y, 1, s);
+        }
+        if (!rc) {
+            copy_reverse_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rev, dphi, n3, nT, 0);
+            if (cudaGetLastError() != cudaSuccess) rc = fail(EBEM_ERR_CUDA, "density copy failed");
+        }
+        if (!rc && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(EBEM_ERR_CUDA, "time marching failed");
+    }
+    lu_plan_destroy(&lu);
+    ws_free(rev, s);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// A^{-1} of one matrix kept on the device (the E_0 solve of the marching,
+// also for callers that drive the steps themselves): LU with partial
+// pivoting (getrf), then getrs on the identity, whose n right-hand sides run
+// as matrix-matrix triangular solves.
+__global__ void set_identity_kernel(double* __restrict__ a, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[(size_t)i * n + i] = 1.0;
+}
+
+int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan, bool pooled) {
+    int rc = EBEM_OK;
+    int lwork = 0, hinfo = 0;
+    double *lu = nullptr, *work = nullptr;
+    int *ipiv = nullptr, *info = nullptr;
+    const size_t nn = (size_t)n * n;
+    cusolverDnHandle_t h = nullptr;
+    plan->n = n;
+    plan->pooled = pooled;
+    plan->st = s;
+    if ((rc = solver_handle(s, &h))) return rc;
+    cudaError_t e = pooled ? ws_malloc(&plan->inv, nn * sizeof(double), s) : cudaMalloc(&plan->inv, nn * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        plan->inv = nullptr;
+        return fail(EBEM_ERR_NOMEM, "inverse allocation failed");
+    }
+    if (ws_malloc(&lu, nn * sizeof(double), s) != cudaSuccess || ws_malloc(&ipiv, n * sizeof(int), s) != cudaSuccess ||
+        ws_malloc(&info, sizeof(int), s) != cudaSuccess) {
+        rc = fail(EBEM_ERR_NOMEM, "LU workspace allocation failed");
         goto done;
     }
-    CUSOLVER_TRY(cusolverDnCreate(&h));
-    CUSOLVER_TRY(cusolverDnSetStream(h, s));
-    if (cudaMemcpyAsync(lu, dE, nn * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
-        rc = fail(EBEM_ERR_CUDA, "E_0 copy failed");
+    if (cudaMemcpyAsync(lu, dA, nn * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        rc = fail(EBEM_ERR_CUDA, "matrix copy failed");
         goto done;
     }
-    CUSOLVER_TRY(cusolverDnDgetrf_bufferSize(h, n3, n3, lu, n3, &lwork));
+    CUSOLVER_TRY(cusolverDnDgetrf_bufferSize(h, n, n, lu, n, &lwork));
     if (ws_malloc(&work, (size_t)(lwork > 0 ? lwork : 1) * sizeof(double), s) != cudaSuccess) {
         rc = fail(EBEM_ERR_NOMEM, "LU workspace allocation failed");
         goto done;
     }
-    CUSOLVER_TRY(cusolverDnDgetrf(h, n3, n3, lu, n3, work, ipiv, info));
+    CUSOLVER_TRY(cusolverDnDgetrf(h, n, n, lu, n, work, ipiv, info));
     if (cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) {
         rc = fail(EBEM_ERR_CUDA, "LU factorisation failed");
         goto done;
     }
     if (hinfo != 0) {
-        rc = fail(EBEM_ERR_SINGULAR, "E_0 is singular (zero pivot " + std::to_string(hinfo) + ")");
+        rc = fail(EBEM_ERR_SINGULAR, "matrix is singular (zero pivot " + std::to_string(hinfo) + ")");
         goto done;
     }
-    {
-        // density in reversed time order: phi_n at column nT-1-n, so that
-        // phi_{n-1}, phi_{n-2}, ... are contiguous for the history product
-        long long tot = (long long)n3 * nT;
-        copy_reverse_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(drhs, rev, n3, nT, 1);
-        if (cudaGetLastError() != cudaSuccess) { rc = fail(EBEM_ERR_CUDA, "rhs copy failed"); goto done; }
-        for (int n = 0; n < nT; n++) {
-            double* y = rev + (size_t)(nT - 1 - n) * n3;
-            int M = (n < L - 1) ? n : L - 1;
-            if (M > 0) {
-                rc = launch_hist_gemv(dE + nn, n3, (long long)n3 * M, rev + (size_t)(nT - n) * n3, y, sms, s);
-                if (rc) goto done;
-            }
-            CUSOLVER_TRY(cusolverDnDgetrs(h, CUBLAS_OP_N, n3, 1, lu, n3, ipiv, y, n3, info));
-        }
-        copy_reverse_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rev, dphi, n3, nT, 0);
-        if (cudaGetLastError() != cudaSuccess) { rc = fail(EBEM_ERR_CUDA, "density copy failed"); goto done; }
-        if (cudaStreamSynchronize(s) != cudaSuccess) { rc = fail(EBEM_ERR_CUDA, "time marching failed"); goto done; }
+    if (cudaMemsetAsync(plan->inv, 0, nn * sizeof(double), s) != cudaSuccess) {
+        rc = fail(EBEM_ERR_CUDA, "inverse initialisation failed");
+        goto done;
     }
+    set_identity_kernel<<<(n + 255) / 256, 256, 0, s>>>(plan->inv, n);
+    if (cudaGetLastError() != cudaSuccess) {
+        rc = fail(EBEM_ERR_CUDA, "inverse initialisation failed");
+        goto done;
+    }
+    CUSOLVER_TRY(cusolverDnDgetrs(h, CUBLAS_OP_N, n, n, lu, n, ipiv, plan->inv, n, info));
 done:
-    if (h) cusolverDnDestroy(h);
     ws_free(lu, s);
     ws_free(work, s);
-    ws_free(rev, s);
     ws_free(ipiv, s);
     ws_free(info, s);
     return rc;
 }
 
-// ---------------------------------------------------------------------------
-// LU factors of one matrix kept on the device (the E_0 factorisation of the
-// marching, for callers that drive the steps themselves).
-int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan) {
-    int rc = EBEM_OK;
-    int lwork = 0, hinfo = 0;
-    double* work = nullptr;
-    const size_t nn = (size_t)n * n;
-    plan->n = n;
-    if (cudaMalloc(&plan->lu, nn * sizeof(double)) != cudaSuccess || cudaMalloc(&plan->ipiv, n * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&plan->info, sizeof(int)) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(EBEM_ERR_NOMEM, "LU allocation failed");
-    }
-    CUSOLVER_TRY(cusolverDnCreate(&plan->h));
-    CUSOLVER_TRY(cusolverDnSetStream(plan->h, s));
-    if (cudaMemcpyAsync(plan->lu, dA, nn * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
-        rc = fail(EBEM_ERR_CUDA, "matrix copy failed");
-        goto done;
-    }
-    CUSOLVER_TRY(cusolverDnDgetrf_bufferSize(plan->h, n, n, plan->lu, n, &lwork));
-    if (cudaMalloc(&work, (size_t)(lwork > 0 ? lwork : 1) * sizeof(double)) != cudaSuccess) {
-        cudaGetLastError();
-        rc = fail(EBEM_ERR_NOMEM, "LU workspace allocation failed");
-        goto done;
-    }
-    CUSOLVER_TRY(cusolverDnDgetrf(plan->h, n, n, plan->lu, n, work, plan->ipiv, plan->info));
-    if (cudaMemcpyAsync(&hinfo, plan->info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
-        rc = fail(EBEM_ERR_CUDA, "LU factorisation failed");
-        goto done;
-    }
-    if (hinfo != 0) rc = fail(EBEM_ERR_SINGULAR, "matrix is singular (zero pivot " + std::to_string(hinfo) + ")");
-done:
-    if (work) cudaFree(work);
-    return rc;
-}
-
+// b (n x nrhs, device, overwritten) = A^{-1} b.
 int lu_plan_solve(LuPlan* plan, double* db, int nrhs, cudaStream_t s) {
-    int rc = EBEM_OK;
-    CUSOLVER_TRY(cusolverDnSetStream(plan->h, s));
-    CUSOLVER_TRY(cusolverDnDgetrs(plan->h, CUBLAS_OP_N, plan->n, nrhs, plan->lu, plan->n, plan->ipiv, db, plan->n,
-                                  plan->info));
-done:
-    return rc;
+    cublasHandle_t hb = nullptr;
+    if (int rc = blas_handle(s, &hb)) return rc;
+    const int n = plan->n;
+    const size_t cnt = (size_t)n * nrhs;
+    double* tmp = nullptr;
+    if (ws_malloc(&tmp, cnt * sizeof(double), s) != cudaSuccess) return fail(EBEM_ERR_NOMEM, "solve workspace allocation failed");
+    const double one = 1.0, zero = 0.0;
+    const cublasStatus_t st =
+        nrhs == 1 ? cublasDgemv(hb, CUBLAS_OP_N, n, n, &one, plan->inv, n, db, 1, &zero, tmp, 1)
+                  : cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &one, plan->inv, n, db, n, &zero, tmp, n);
+    cudaError_t e = st == CUBLAS_STATUS_SUCCESS ? cudaMemcpyAsync(db, tmp, cnt * sizeof(double), cudaMemcpyDeviceToDevice, s)
+                                                : cudaSuccess;
+    ws_free(tmp, s);
+    if (st != CUBLAS_STATUS_SUCCESS) return fail(EBEM_ERR_CUDA, "product with the inverse failed (cuBLAS status " + std::to_string((int)st) + ")");
+    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("solve copy: ") + cudaGetErrorString(e));
+    return EBEM_OK;
 }
 
 void lu_plan_destroy(LuPlan* plan) {
-    if (plan->h) cusolverDnDestroy(plan->h);
-    if (plan->lu) cudaFree(plan->lu);
-    if (plan->ipiv) cudaFree(plan->ipiv);
-    if (plan->info) cudaFree(plan->info);
-    plan->h = nullptr;
-    plan->lu = nullptr;
-    plan->ipiv = plan->info = nullptr;
+    if (plan->inv) {
+        if (plan->pooled) ws_free(plan->inv, plan->st);
+        else cudaFree(plan->inv);
+    }
+    plan->inv = nullptr;
 }
 
 // ---------------------------------------------------------------------------

@@ -246,8 +246,9 @@ int ebem_assemble_ghc(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh,
  * rhs: 3N x nT column-major, host or device. */
 int ebem_rhs(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int datum, double* rhs, void* stream);
 
-/* Time marching: LU of E_0 once, then phi_n = E_0^{-1}(b_n -
- * sum_{l=1}^{min(n,L-1)} E_l phi_{n-l}).  Replaces the marching loop of
+/* Time marching: LU of E_0 once (and from it E_0^{-1}, as ebem_lu_create
+ * does), then phi_n = E_0^{-1}(b_n - sum_{l=1}^{min(n,L-1)} E_l phi_{n-l}).
+ * Replaces the marching loop of
  * f/BEMenerg_indir/BEMenerg_core/BEMenerg_coreGPU/BEMenerg_coreGPU_timeMarching.m:151-169
  * (and of BEMenerg_coreSA_timeMarching.m:46-113).  E: n3 x n3 x L (the
  * layout of ebem_assemble_sa), rhs and phi: n3 x nT; host or device.
@@ -259,13 +260,16 @@ int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double
  * [r0, r0 + rows) of every E_l and one all-gather per step assembles the
  * right-hand side).
  *
- * ebem_lu_create: LU factors (partial pivoting) of the device matrix A
- * (column-major n x n), kept on the device; replaces
- * [L, U, P] = lu(sparse(matrix)) of
+ * ebem_lu_create: the factorisation of the device matrix A (column-major
+ * n x n) for repeated solves; replaces [L, U, P] = lu(sparse(matrix)) of
  * f/BEMenerg_indir/BEMenerg_core/BEMenerg_coreSA/BEMenerg_coreSA_timeMarching.m:46
- * (BEMenerg_coreGPU_timeMarching.m:153).  Returns EBEM_ERR_SINGULAR on a
- * zero pivot.  ebem_lu_solve overwrites the device columns b (n x nrhs) with
- * A^{-1} b (U\(L\(P*b)), :59).  ebem_lu_destroy frees the factors.
+ * (BEMenerg_coreGPU_timeMarching.m:153).  LU with partial pivoting, from
+ * which A^{-1} is formed once and kept on the device (n^2 doubles), so that
+ * a solve is one matrix-vector product rather than two triangular solves of
+ * one right-hand side.  Returns EBEM_ERR_SINGULAR on a zero pivot.
+ * ebem_lu_solve overwrites the device columns b (n x nrhs) with A^{-1} b
+ * (U\(L\(P*b)) of :59, equal to rounding: the two differ by about
+ * cond(A) times the unit roundoff).  ebem_lu_destroy frees the inverse.
  *
  * ebem_history_gemv: y -= A x for device A (rows x K, column-major, leading
  * dimension rows), x (K) and y (rows): the history sum
