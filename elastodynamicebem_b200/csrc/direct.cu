@@ -843,19 +843,23 @@ __device__ __forceinline__ void warp_add3(double* dst, double v0, double v1, dou
 }
 
 // G part: sum over slices n of clamp(G(t - (n-1) dt) - G(t - n dt)) / (4 pi rho) a_n.
-__global__ void __launch_bounds__(128) pp_g_kernel(PPArgs A) {
+// Block (x-tile, evaluation, chunk c) takes the slices n in
+// [c kchunk + 1, (c + 1) kchunk] and evaluates G at the levels n_lo - 1 .. n_hi
+// (one level more than its slices), so that short meshes still fill the GPU.
+__global__ void __launch_bounds__(128) pp_g_kernel(PPArgs A, int kchunk) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int ev = blockIdx.y;                          // evaluation index q * npts + ip
     const int q = ev / A.npts, ip = ev % A.npts;
     const double t = A.times[q];
     const double* src = A.pts + 3 * ip;
     const int nhat = (t > 0) ? (int)ceil(t / A.dt) : 0;
+    const int n_lo = blockIdx.z * kchunk + 1, n_hi = min((int)(blockIdx.z + 1) * kchunk, nhat);
     double u0 = 0.0, u1 = 0.0, u2 = 0.0;
-    if (x < A.N && nhat > 0) {
+    if (x < A.N && n_lo <= n_hi) {
         const DirTri& X = A.tri[x];
         double Gp[9] = {0}, Gk[9];
         const double c4 = 4 * kPi * A.p.rho;
-        for (int k = 0; k <= nhat; k++) {
+        for (int k = n_lo - 1; k <= n_hi; k++) {
             const double tk = t - k * A.dt;
 #pragma unroll
             for (int e = 0; e < 9; e++) Gk[e] = 0.0;
@@ -872,7 +876,7 @@ __global__ void __launch_bounds__(128) pp_g_kernel(PPArgs A) {
                         for (int e = 0; e < 9; e++) Gk[e] += w * nu[e];
                     }
             }
-            if (k >= 1) {
+            if (k >= n_lo) {
                 const int n = k;                        // slice n uses instants t - (n-1) dt and t - n dt
                 double S[9];
 #pragma unroll
@@ -901,19 +905,22 @@ __global__ void __launch_bounds__(128) pp_g_kernel(PPArgs A) {
 }
 
 // P part: minus the sum over slices n of clamp(P_{n-1} - 2 P_n + P_{n+1}) / (4 pi rho dt) b_n.
-__global__ void __launch_bounds__(128) pp_p_kernel(PPArgs A) {
+// Chunked over the slices as pp_g_kernel; a chunk evaluates P at the levels
+// n_lo - 1 .. n_hi + 1.
+__global__ void __launch_bounds__(128) pp_p_kernel(PPArgs A, int kchunk) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int ev = blockIdx.y;
     const int q = ev / A.npts, ip = ev % A.npts;
     const double t = A.times[q];
     const double* src = A.pts + 3 * ip;
     const int nhat = (t > 0) ? (int)ceil(t / A.dt) : 0;
+    const int n_lo = blockIdx.z * kchunk + 1, n_hi = min((int)(blockIdx.z + 1) * kchunk, nhat);
     double u0 = 0.0, u1 = 0.0, u2 = 0.0;
-    if (s < A.Nv && nhat > 0) {
+    if (s < A.Nv && n_lo <= n_hi) {
         double Pm2[9] = {0}, Pm1[9] = {0}, Pk[9];
         const double c4 = 4 * kPi * A.p.rho * A.dt;
         const int e0 = A.vt_off[s], e1 = A.vt_off[s + 1];
-        for (int k = 0; k <= nhat + 1; k++) {
+        for (int k = n_lo - 1; k <= n_hi + 1; k++) {
             const double tk = t - k * A.dt;
 #pragma unroll
             for (int e = 0; e < 9; e++) Pk[e] = 0.0;
@@ -937,7 +944,7 @@ __global__ void __launch_bounds__(128) pp_p_kernel(PPArgs A) {
                         }
                 }
             }
-            if (k >= 2) {
+            if (k >= n_lo + 1) {
                 const int n = k - 1;                    // slice n: P_{n-1} - 2 P_n + P_{n+1}
                 double S[9];
 #pragma unroll
@@ -973,6 +980,8 @@ int launch_pp_dir(const MeshData& m, const PhysParams& P, int n_sub, int n_sing,
     const int gstride = fix ? n_sing : 3;
     if (3 * (n_sub - 1) + n_sing > n_sub * n_sing && !fix)
         return fail(EBEM_ERR_INVALID, "the reference's node stride 3 needs n_sing >= 3 (or the fixed stride)");
+    if ((long long)npts * ntimes > 65535)
+        return fail(EBEM_ERR_INVALID, "at most 65535 (point, time) evaluations per call");
     Tables T;
     if (int rc = upload_tables(T, 0, n_sub, n_sing, 0, s)) return rc;
     double* d_times = nullptr;
@@ -1004,11 +1013,28 @@ int launch_pp_dir(const MeshData& m, const PhysParams& P, int n_sub, int n_sing,
     A.Pm = d_P;
     A.mode = mode;
     if (e == cudaSuccess) {
-        dim3 gg((m.nt + 127) / 128, npts * ntimes), gp((m.nv + 127) / 128, npts * ntimes);
+        // slices split into chunks over grid z so that about 8 blocks per SM
+        // run (a chunk re-evaluates 1 (G) or 2 (P) boundary levels: at least
+        // 4 and 8 slices per chunk keep that under a quarter)
+        int nhat_max = 0;
+        for (int q = 0; q < ntimes; q++)
+            if (h_times[q] > 0) nhat_max = std::max(nhat_max, (int)std::ceil(h_times[q] / P.dt));
+        nhat_max = std::max(nhat_max, 1);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
+        const long long evs = (long long)npts * ntimes, target = 8LL * sms;
+        auto chunk_of = [&](long long bxy, int kmin) {
+            const long long want = (nhat_max * bxy + target - 1) / target;
+            return (int)std::min<long long>(nhat_max, std::max<long long>(kmin, want));
+        };
+        const long long bg = (m.nt + 127) / 128, bp = (m.nv + 127) / 128;
+        const int kg = chunk_of(bg * evs, 4), kp = chunk_of(bp * evs, 8);
+        dim3 gg((unsigned)bg, (unsigned)evs, (unsigned)((nhat_max + kg - 1) / kg));
+        dim3 gp((unsigned)bp, (unsigned)evs, (unsigned)((nhat_max + kp - 1) / kp));
         if (mode == 0) e = cudaMemsetAsync(d_u, 0, sizeof(double) * 3 * (size_t)npts * ntimes, s);
         if (e == cudaSuccess) {
-            pp_g_kernel<<<gg, 128, 0, s>>>(A);
-            pp_p_kernel<<<gp, 128, 0, s>>>(A);
+            pp_g_kernel<<<gg, 128, 0, s>>>(A, kg);
+            pp_p_kernel<<<gp, 128, 0, s>>>(A, kp);
             e = cudaGetLastError();
         }
     }
