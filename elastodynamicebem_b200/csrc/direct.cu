@@ -534,11 +534,34 @@ __global__ void __launch_bounds__(128) k_assemble_warp_kernel(KArgs A) {
         if (llo < 0) continue;
         const int e0 = A.vt_off[s], e1 = A.vt_off[s + 1];
         const int NP = (e1 - e0) * per_tri;
+        // the node pairs' exact distance range (warp min/max): lags in which
+        // every node pair would be skipped below add nothing and are skipped
+        // by the whole warp (the null test above bounds them by vertex
+        // distances and triangle sizes only)
+        double r2min = 1e300, r2max = 0.0;
+        for (int np = lane; np < NP; np += 32) {
+            const int ee = e0 + np / per_tri, rem = np - (np / per_tri) * per_tri;
+            const int m = A.vt_tri[ee];
+            if (m == x) continue;
+            const int qi = rem / A.n_gh, o = rem - qi * A.n_gh;
+            double y[3], xo[3];
+            bary_point(y, A.inner + 3 * qi, A.tri[m].V);
+            bary_point(xo, A.outer + 3 * o, X.V);
+            const double pt[3] = {xo[0] - y[0], xo[1] - y[1], xo[2] - y[2]};
+            const double r2 = pt[0] * pt[0] + pt[1] * pt[1] + pt[2] * pt[2];
+            r2min = fmin(r2min, r2);
+            r2max = fmax(r2max, r2);
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            r2min = fmin(r2min, __shfl_xor_sync(0xffffffffu, r2min, off));
+            r2max = fmax(r2max, __shfl_xor_sync(0xffffffffu, r2max, off));
+        }
         for (int l = llo; l <= lhi; l++) {
             const bool lin = !A.fix && l < 3;
             const double thi = (l + 1) * dt, tlo = (l - 2) * dt;
             const double skipP2 = lin ? 1e300 : (cP * thi) * (cP * thi) * (1 + 1e-12);
             const double skipS2 = (l >= 3) ? (cS * tlo) * (cS * tlo) * (1 - 1e-12) : -1.0;
+            if (r2min > skipP2 || r2max < skipS2) continue;
             double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             for (int np = lane; np < NP; np += 32) {
                 const int ee = e0 + np / per_tri, rem = np - (np / per_tri) * per_tri;

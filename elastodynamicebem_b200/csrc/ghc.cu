@@ -204,10 +204,32 @@ __global__ void __launch_bounds__(128) ghc_assemble_warp_kernel(GHCArgs A) {
         while (lhi >= A.lag0 && (lhi - 1) * A.velS * A.dt > distMax) lhi--;
         if (lhi < A.lag0) continue;
         const double aS = A.geo[i].area, aF = A.geo[j].area;
+        // the node pairs' exact distance range (warp min/max): lags whose
+        // window lies before the P front or after the S front for every node
+        // pair add nothing and are skipped by the whole warp
+        double r2min = 1e300, r2max = 0.0;
+        for (int np = lane; np < NP; np += 32) {
+            const int q = np / A.n_out, o = np - q * A.n_out;
+            const double* bq = A.inner + 3 * q;
+            const double* bl = A.outer + 3 * o;
+            double r2 = 0.0;
+            for (int c = 0; c < 3; c++) {
+                const double xc = (bq[0] * VF[0][c] + bq[1] * VF[1][c] + bq[2] * VF[2][c]) -
+                                  (bl[0] * VS[0][c] + bl[1] * VS[1][c] + bl[2] * VS[2][c]);
+                r2 += xc * xc;
+            }
+            r2min = fmin(r2min, r2);
+            r2max = fmax(r2max, r2);
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            r2min = fmin(r2min, __shfl_xor_sync(0xffffffffu, r2min, off));
+            r2max = fmax(r2max, __shfl_xor_sync(0xffffffffu, r2max, off));
+        }
         for (int l = A.lag0; l <= lhi; l++) {
             const double thi = (l + 1) * dt, tlo = (l - 1) * dt;
             const double skipP2 = (cP * thi) * (cP * thi) * (1 + 1e-12);
             const double skipS2 = (l >= 1) ? (cS * tlo) * (cS * tlo) * (1 - 1e-12) : -1.0;
+            if (r2min > skipP2 || r2max < skipS2) continue;
             double K[6] = {0, 0, 0, 0, 0, 0};
             for (int np = lane; np < NP; np += 32) {
                 const int q = np / A.n_out, o = np - q * A.n_out;
