@@ -34,6 +34,15 @@
 #include <cmath>
 #include <vector>
 
+// Dispatch between the warp-per-pair and thread-per-pair K kernels
+// (compile-time knobs for measuring other thresholds).
+#ifndef EBEM_K_WARP_MIN_NODE_PAIRS
+#define EBEM_K_WARP_MIN_NODE_PAIRS 32
+#endif
+#ifndef EBEM_K_WARP_MAX_PAIRS_PER_SM
+#define EBEM_K_WARP_MAX_PAIRS_PER_SM 4096
+#endif
+
 namespace ebem {
 
 // ---------------------------------------------------------------------------
@@ -662,60 +671,73 @@ __global__ void __launch_bounds__(128) k_sing_kernel(KArgs A, const double* __re
     }
 }
 
-// Diagonal blocks of V_l on the DIAG rule: one thread per triangle.
-__global__ void __launch_bounds__(128) v_diag_kernel(const DirTri* __restrict__ tri, int N, const double* __restrict__ outer,
-                                                     const double* __restrict__ wout, int n_gh, const double* __restrict__ dn,
-                                                     const double* __restrict__ dw, int n_diag, double cP, double cS,
-                                                     double dt, double c4pirho, int lag0, int nlag, double* V, size_t ld,
-                                                     size_t ld_lag) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= N) return;
+// Diagonal blocks of V_l on the DIAG rule, in two passes.  Levels: one warp
+// per (triangle x, time level k), the lanes over the (outer node, child, DIAG
+// node) evaluations of the level integral T_k (9 entries), reduced over the
+// warp into Tb[x][k - kmin].  Combine: one thread per (triangle, lag, entry),
+// V_l = (T_{l+1} - 2 T_l + T_{l-1}) / (4 pi rho) with T_0 taken as zero.
+// (One thread per triangle walking every level left all but a few SMs idle
+// on meshes of a few hundred triangles.)
+__global__ void __launch_bounds__(128) v_diag_level_kernel(const DirTri* __restrict__ tri, int N,
+                                                           const double* __restrict__ outer,
+                                                           const double* __restrict__ wout, int n_gh,
+                                                           const double* __restrict__ dn, const double* __restrict__ dw,
+                                                           int n_diag, double cP, double cS, double dt, int kmin, int nk,
+                                                           double* __restrict__ Tb) {
+    const int lane = threadIdx.x & 31;
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= (long long)N * nk) return;                 // uniform across the warp
+    const int x = (int)(w / nk), kk = (int)(w - (long long)x * nk);
+    const double t = (kmin + kk) * dt;
     const DirTri& X = tri[x];
-    double Tm2[9] = {0}, Tm1[9] = {0}, T[9];
-    const int klo = max(1, lag0 - 1), khi = lag0 + nlag;
-    for (int k = klo; k <= khi; k++) {
-        const double t = k * dt;
+    const int per_o = 3 * n_diag, total = n_gh * per_o;
+    double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = lane; c < total; c += 32) {
+        const int o = c / per_o, rem = c - o * per_o, ch = rem / n_diag, d = rem - ch * n_diag;
+        double xo[3];
+        bary_point(xo, outer + 3 * o, X.V);
+        const int a = ch, b = (ch + 2) % 3;
+        const double ea[3] = {X.V[a][0] - xo[0], X.V[a][1] - xo[1], X.V[a][2] - xo[2]};
+        const double eb[3] = {X.V[b][0] - xo[0], X.V[b][1] - xo[1], X.V[b][2] - xo[2]};
+        const double cr[3] = {ea[1] * eb[2] - ea[2] * eb[1], ea[2] * eb[0] - ea[0] * eb[2], ea[0] * eb[1] - ea[1] * eb[0]};
+        const double ac = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) / 2;
+        const double* bd = dn + 3 * d;
+        double X3[3];
 #pragma unroll
-        for (int e = 0; e < 9; e++) T[e] = 0.0;
-        for (int o = 0; o < n_gh; o++) {
-            double xo[3];
-            bary_point(xo, outer + 3 * o, X.V);
-            double in[9] = {0};
-            for (int ch = 0; ch < 3; ch++) {
-                const int a = ch, b = (ch + 2) % 3;
-                const double ea[3] = {X.V[a][0] - xo[0], X.V[a][1] - xo[1], X.V[a][2] - xo[2]};
-                const double eb[3] = {X.V[b][0] - xo[0], X.V[b][1] - xo[1], X.V[b][2] - xo[2]};
-                const double cr[3] = {ea[1] * eb[2] - ea[2] * eb[1], ea[2] * eb[0] - ea[0] * eb[2], ea[0] * eb[1] - ea[1] * eb[0]};
-                const double ac = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) / 2;
-                for (int d = 0; d < n_diag; d++) {
-                    const double* bd = dn + 3 * d;
-                    double X3[3];
+        for (int q = 0; q < 3; q++) X3[q] = (bd[0] * X.V[a][q] + bd[1] * X.V[b][q] + bd[2] * xo[q]) - xo[q];
+        double nu[9];
+        kern_v(nu, X3, sqrt(X3[0] * X3[0] + X3[1] * X3[1] + X3[2] * X3[2]), t, cP, cS);
+        const double wgt = (X.area * wout[o]) * (dw[d] * ac);
 #pragma unroll
-                    for (int c = 0; c < 3; c++) X3[c] = (bd[0] * X.V[a][c] + bd[1] * X.V[b][c] + bd[2] * xo[c]) - xo[c];
-                    double nu[9];
-                    kern_v(nu, X3, sqrt(X3[0] * X3[0] + X3[1] * X3[1] + X3[2] * X3[2]), t, cP, cS);
-#pragma unroll
-                    for (int e = 0; e < 9; e++) in[e] += dw[d] * ac * nu[e];
-                }
-            }
-#pragma unroll
-            for (int e = 0; e < 9; e++) T[e] += X.area * wout[o] * in[e];
-        }
-        const int l = k - 1;
-        if (l >= lag0 && l < lag0 + nlag) {
-            double* base = V + (size_t)(l - lag0) * ld_lag + (3 * (size_t)x) * ld + 3 * (size_t)x;
-#pragma unroll
-            for (int i = 0; i < 3; i++)
-#pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    const int e = 3 * i + j;
-                    const double prev = (l - 1 >= 1) ? Tm2[e] : 0.0;
-                    base[(size_t)j * ld + i] = ((T[e] - 2 * Tm1[e]) + prev) / c4pirho;
-                }
-        }
-#pragma unroll
-        for (int e = 0; e < 9; e++) { Tm2[e] = Tm1[e]; Tm1[e] = T[e]; }
+        for (int e = 0; e < 9; e++) T[e] += wgt * nu[e];
     }
+#pragma unroll
+    for (int e = 0; e < 9; e++)
+        for (int off = 16; off > 0; off >>= 1) T[e] += __shfl_xor_sync(0xffffffffu, T[e], off);
+    if (lane < 9) {
+        double v = 0.0;
+#pragma unroll
+        for (int e = 0; e < 9; e++)
+            if (e == lane) v = T[e];
+        Tb[((size_t)x * nk + kk) * 9 + lane] = v;
+    }
+}
+
+__global__ void __launch_bounds__(128) v_diag_combine_kernel(const double* __restrict__ Tb, int N, int kmin, int nk,
+                                                             int lag0, int nlag, double c4pirho, double* __restrict__ V,
+                                                             size_t ld, size_t ld_lag) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)N * nlag * 9) return;
+    const int e = (int)(idx % 9);
+    const long long r = idx / 9;
+    const int q = (int)(r % nlag), x = (int)(r / nlag);
+    const int l = lag0 + q, k = l + 1;
+    auto level = [&](int kk) {
+        return (kk >= kmin && kk < kmin + nk) ? Tb[((size_t)x * nk + (kk - kmin)) * 9 + e] : 0.0;
+    };
+    const double prev = (l - 1 >= 1) ? level(k - 2) : 0.0;
+    const int i = e / 3, j = e - 3 * i;
+    V[(size_t)q * ld_lag + (3 * (size_t)x + j) * ld + 3 * (size_t)x + i] = ((level(k) - 2 * level(k - 1)) + prev) / c4pirho;
 }
 
 // Rule tables in one device buffer.
@@ -798,7 +820,7 @@ int launch_k_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_su
     // 1.08x faster, bar of 2800 triangles 1.37x slower)
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
-    if (n_sub * n_sing * n_gh >= 32 && pairs < (long long)sms * 4096) {
+    if (n_sub * n_sing * n_gh >= EBEM_K_WARP_MIN_NODE_PAIRS && pairs < (long long)sms * EBEM_K_WARP_MAX_PAIRS_PER_SM) {
         const long long want = (pairs + 3) / 4, cap = (long long)sms * 64;
         k_assemble_warp_kernel<<<(unsigned)(want < cap ? want : cap), 128, 0, s>>>(A);
     } else {
@@ -818,11 +840,20 @@ int launch_v_diag(const MeshData& m, const PhysParams& P, int n_gh, int n_diag, 
     Tables T;
     if (int rc = upload_tables(T, n_gh, 0, 0, n_diag, s)) return rc;
     const size_t ld = 3 * (size_t)m.nt;
-    v_diag_kernel<<<(m.nt + 127) / 128, 128, 0, s>>>(m.d_dir, m.nt, T.d + T.outer, T.d + T.wout, n_gh, T.d + T.dn,
-                                                      T.d + T.dw, n_diag, P.velP, P.velS, P.dt, 4 * kPi * P.rho, lag0,
-                                                      nlag, d_V, ld, ld * ld);
-    EBEM_CUDA_TRY(cudaGetLastError());
-    EBEM_CUDA_TRY(cudaStreamSynchronize(s));
+    // levels k = kmin .. lag0 + nlag (t = k dt; t = 0 contributes nothing)
+    const int kmin = std::max(1, lag0 - 1), nk = lag0 + nlag - kmin + 1;
+    double* Tb = nullptr;
+    EBEM_CUDA_TRY(ws_malloc(&Tb, sizeof(double) * 9 * (size_t)m.nt * nk, s));
+    const long long lv_threads = 32LL * m.nt * nk, cb_threads = 9LL * m.nt * nlag;
+    v_diag_level_kernel<<<(unsigned)((lv_threads + 127) / 128), 128, 0, s>>>(
+        m.d_dir, m.nt, T.d + T.outer, T.d + T.wout, n_gh, T.d + T.dn, T.d + T.dw, n_diag, P.velP, P.velS, P.dt, kmin,
+        nk, Tb);
+    v_diag_combine_kernel<<<(unsigned)((cb_threads + 127) / 128), 128, 0, s>>>(Tb, m.nt, kmin, nk, lag0, nlag,
+                                                                               4 * kPi * P.rho, d_V, ld, ld * ld);
+    cudaError_t e = cudaGetLastError();
+    ws_free(Tb, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("V diagonal blocks: ") + cudaGetErrorString(e));
     return EBEM_OK;
 }
 

@@ -24,6 +24,20 @@
 #include "ebem_internal.h"
 #include "sa_pair.cuh"
 
+// Dispatch between the warp-per-pair and thread-per-pair kernels (compile-time
+// knobs for measuring other thresholds).  Measured with the exact lag skip in
+// both kernels: the warp kernel wins up to about 16k pairs per SM at 84 node
+// pairs and more (sphere of 320 triangles, rule 7/4/3: 5.5 -> 3.3 ms; sphere
+// of 1280, 1.6 M pairs, rule 7/16/3: 166 -> 97 ms); on the 2800-triangle bar
+// (7.8 M pairs, most of them done after the skip test) the thread kernel is
+// 1.4x faster at rule 7/4/3 and even at 7/16/3.
+#ifndef EBEM_GHC_WARP_MIN_NODE_PAIRS
+#define EBEM_GHC_WARP_MIN_NODE_PAIRS 64
+#endif
+#ifndef EBEM_GHC_WARP_MAX_PAIRS_PER_SM
+#define EBEM_GHC_WARP_MAX_PAIRS_PER_SM 16384
+#endif
+
 namespace ebem {
 
 struct GHCArgs {
@@ -308,13 +322,11 @@ int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_
     A.ld_lag = ld_lag;
     long long NN = (long long)m.nt * m.nt;
     int threads = 128;
-    // warp per pair when the thread kernel would not fill the GPU (fewer
-    // pairs than two waves of threads) and a pair has 160+ node pairs
-    // (measured: sphere of 320 triangles, 336 node pairs, 1.57x faster; 84 node
-    // pairs 1.2x slower; bar of 2800 triangles, 7.8 M pairs, 1.2x slower)
+    // warp per pair below the thresholds at the top of this file
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
-    if ((long long)n_gh * n_sub * n_sing >= 160 && NN < (long long)sms * 4096) {
+    if ((long long)n_gh * n_sub * n_sing >= EBEM_GHC_WARP_MIN_NODE_PAIRS &&
+        NN < (long long)sms * EBEM_GHC_WARP_MAX_PAIRS_PER_SM) {
         const long long want = (NN + 3) / 4, cap = (long long)sms * 64;
         ghc_assemble_warp_kernel<<<(unsigned)(want < cap ? want : cap), threads, 0, s>>>(A);
     } else {
