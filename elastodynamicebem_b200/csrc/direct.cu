@@ -616,59 +616,94 @@ __global__ void __launch_bounds__(128) k_assemble_warp_kernel(KArgs A) {
     }
 }
 
-// Same-triangle parts of K_l: one thread per (triangle x, local vertex kv).
-__global__ void __launch_bounds__(128) k_sing_kernel(KArgs A, const double* __restrict__ dn, const double* __restrict__ dw,
-                                                     int n_diag) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= 3 * A.N) return;
+// Same-triangle parts of K_l, in two passes.  Levels: one warp per (triangle
+// x, local vertex kv, level k) over the call's levels kmin..kmin+nk-1, the
+// lanes over the (outer node, child, DIAG node) evaluations, reduced over the
+// warp into Tb[3x + kv - 1][k - kmin]; a level outside the triangle's own
+// range klo..khi (its parts vanish from lag lmax on) is left unwritten and
+// never read.  Emission: one thread per (x, kv, lag) adds the third
+// difference (k_emit), levels below klo read as zero.  (One thread per
+// (x, kv) walking all levels left most SMs idle on small meshes.)
+struct KSingRange {
+    int llo, lhi, klo, khi;
+};
+__device__ __forceinline__ KSingRange k_sing_range(const KArgs& A, const DirTri& X) {
+    KSingRange r;
+    const int lmax = (int)ceil(X.maxL / (A.p.cS * A.dt)) + 2;      // lags >= lmax are zero
+    r.llo = A.lag0;
+    r.lhi = min(A.lag0 + A.nlag - 1, lmax - 1);
+    r.klo = max(1, r.llo - 2);
+    r.khi = r.lhi + 1;
+    return r;
+}
+
+__global__ void __launch_bounds__(128) k_sing_level_kernel(KArgs A, const double* __restrict__ dn,
+                                                           const double* __restrict__ dw, int n_diag, int kmin, int nk,
+                                                           double* __restrict__ Tb) {
+    const int lane = threadIdx.x & 31;
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= 3LL * A.N * nk) return;                    // uniform across the warp
+    const int p = (int)(w / nk), kk = (int)(w - (long long)p * nk);
     const int x = p / 3, kv = p % 3 + 1;
     const DirTri& X = A.tri[x];
-    const int lmax = (int)ceil(X.maxL / (A.p.cS * A.dt)) + 2;      // lags >= lmax are zero
-    const int llo = A.lag0, lhi = min(A.lag0 + A.nlag - 1, lmax - 1);
-    if (lhi < llo) return;
-    const int s = A.tris[3 * x + kv - 1];
+    const KSingRange rg = k_sing_range(A, X);
+    const int k = kmin + kk;
+    if (rg.lhi < rg.llo || k < rg.klo || k > rg.khi) return;
+    const double t = k * A.dt;
     const double g[3] = {X.M[3 * (kv - 1)], X.M[3 * (kv - 1) + 1], X.M[3 * (kv - 1) + 2]};
     const double vms[3] = {X.n[1] * g[2] - X.n[2] * g[1], X.n[2] * g[0] - X.n[0] * g[2], X.n[0] * g[1] - X.n[1] * g[0]};
-    double Tm3[9] = {0}, Tm2[9] = {0}, Tm1[9] = {0}, T[9];
-    const int klo = max(1, llo - 2), khi = lhi + 1;
-    for (int k = klo; k <= khi; k++) {
-        const double t = k * A.dt;
+    const int per_o = 3 * n_diag, total = A.n_gh * per_o;
+    double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = lane; c < total; c += 32) {
+        const int o = c / per_o, rem = c - o * per_o, ch = rem / n_diag, d = rem - ch * n_diag;
+        double xo[3];
+        bary_point(xo, A.outer + 3 * o, X.V);
+        const int a = ch, b = (ch + 2) % 3;               // children (V1,V3,x), (V2,V1,x), (V3,V2,x)
+        const double ea[3] = {X.V[a][0] - xo[0], X.V[a][1] - xo[1], X.V[a][2] - xo[2]};
+        const double eb[3] = {X.V[b][0] - xo[0], X.V[b][1] - xo[1], X.V[b][2] - xo[2]};
+        const double cr[3] = {ea[1] * eb[2] - ea[2] * eb[1], ea[2] * eb[0] - ea[0] * eb[2], ea[0] * eb[1] - ea[1] * eb[0]};
+        const double ac = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) / 2;
+        const double* bd = dn + 3 * d;
+        double y[3];
 #pragma unroll
-        for (int e = 0; e < 9; e++) T[e] = 0.0;
-        for (int o = 0; o < A.n_gh; o++) {
-            double xo[3];
-            bary_point(xo, A.outer + 3 * o, X.V);
-            double in[9] = {0};
-            for (int ch = 0; ch < 3; ch++) {
-                const int a = ch, b = (ch + 2) % 3;           // children (V1,V3,x), (V2,V1,x), (V3,V2,x)
-                const double ea[3] = {X.V[a][0] - xo[0], X.V[a][1] - xo[1], X.V[a][2] - xo[2]};
-                const double eb[3] = {X.V[b][0] - xo[0], X.V[b][1] - xo[1], X.V[b][2] - xo[2]};
-                const double cr[3] = {ea[1] * eb[2] - ea[2] * eb[1], ea[2] * eb[0] - ea[0] * eb[2], ea[0] * eb[1] - ea[1] * eb[0]};
-                const double ac = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) / 2;
-                for (int d = 0; d < n_diag; d++) {
-                    const double* bd = dn + 3 * d;
-                    double y[3];
+        for (int q = 0; q < 3; q++) y[q] = bd[0] * X.V[a][q] + bd[1] * X.V[b][q] + bd[2] * xo[q];
+        const double R[3] = {xo[0] - y[0], xo[1] - y[1], xo[2] - y[2]};
+        const double r = sqrt(R[0] * R[0] + R[1] * R[1] + R[2] * R[2]);
+        const double phik = X.v[kv - 1] + g[0] * y[0] + g[1] * y[1] + g[2] * y[2];
+        double v[9];
+        kern_k(v, R, r, X.n, t, vms, phik, A.p, false, false);
+        const double wgt = (X.area * A.wout[o]) * (dw[d] * ac);
 #pragma unroll
-                    for (int c = 0; c < 3; c++) y[c] = bd[0] * X.V[a][c] + bd[1] * X.V[b][c] + bd[2] * xo[c];
-                    const double R[3] = {xo[0] - y[0], xo[1] - y[1], xo[2] - y[2]};
-                    const double r = sqrt(R[0] * R[0] + R[1] * R[1] + R[2] * R[2]);
-                    const double phik = X.v[kv - 1] + g[0] * y[0] + g[1] * y[1] + g[2] * y[2];
-                    double v[9];
-                    kern_k(v, R, r, X.n, t, vms, phik, A.p, false, false);
-                    const double w = dw[d] * ac;
-#pragma unroll
-                    for (int e = 0; e < 9; e++) in[e] += w * v[e];
-                }
-            }
-            const double wo = X.area * A.wout[o];
-#pragma unroll
-            for (int e = 0; e < 9; e++) T[e] += wo * in[e];
-        }
-        const int l = k - 1;
-        if (l >= llo && l <= lhi) k_emit(A, l, x, s, Tm3, Tm2, Tm1, T, false);
-#pragma unroll
-        for (int e = 0; e < 9; e++) { Tm3[e] = Tm2[e]; Tm2[e] = Tm1[e]; Tm1[e] = T[e]; }
+        for (int e = 0; e < 9; e++) T[e] += wgt * v[e];
     }
+#pragma unroll
+    for (int e = 0; e < 9; e++)
+        for (int off = 16; off > 0; off >>= 1) T[e] += __shfl_xor_sync(0xffffffffu, T[e], off);
+    if (lane < 9) {
+        double v = 0.0;
+#pragma unroll
+        for (int e = 0; e < 9; e++)
+            if (e == lane) v = T[e];
+        Tb[((size_t)p * nk + kk) * 9 + lane] = v;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_sing_emit_kernel(KArgs A, int kmin, int nk, const double* __restrict__ Tb) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 3LL * A.N * A.nlag) return;
+    const int p = (int)(idx / A.nlag), q = (int)(idx - (long long)p * A.nlag);
+    const int x = p / 3, kv = p % 3 + 1;
+    const KSingRange rg = k_sing_range(A, A.tri[x]);
+    const int l = A.lag0 + q;
+    if (l > rg.lhi) return;
+    double Tl[4][9];                                    // levels l-2, l-1, l, l+1
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+        const int k = l - 2 + h;
+#pragma unroll
+        for (int e = 0; e < 9; e++) Tl[h][e] = (k >= rg.klo) ? Tb[((size_t)p * nk + (k - kmin)) * 9 + e] : 0.0;
+    }
+    k_emit(A, l, x, A.tris[3 * x + kv - 1], Tl[0], Tl[1], Tl[2], Tl[3], false);
 }
 
 // Diagonal blocks of V_l on the DIAG rule, in two passes.  Levels: one warp
@@ -828,8 +863,16 @@ int launch_k_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_su
     }
     EBEM_CUDA_TRY(cudaGetLastError());
     if (n_diag > 0) {
-        k_sing_kernel<<<(3 * m.nt + 127) / 128, 128, 0, s>>>(A, T.d + T.dn, T.d + T.dw, n_diag);
-        EBEM_CUDA_TRY(cudaGetLastError());
+        const int kmin = std::max(1, lag0 - 2), nk = lag0 + nlag - kmin + 1;
+        double* Tb = nullptr;
+        EBEM_CUDA_TRY(ws_malloc(&Tb, sizeof(double) * 27 * (size_t)m.nt * nk, s));
+        const long long lv_threads = 32LL * 3 * m.nt * nk, em_threads = 3LL * m.nt * nlag;
+        k_sing_level_kernel<<<(unsigned)((lv_threads + 127) / 128), 128, 0, s>>>(A, T.d + T.dn, T.d + T.dw, n_diag, kmin,
+                                                                                  nk, Tb);
+        k_sing_emit_kernel<<<(unsigned)((em_threads + 127) / 128), 128, 0, s>>>(A, kmin, nk, Tb);
+        cudaError_t e = cudaGetLastError();
+        ws_free(Tb, s);
+        if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("K same-triangle parts: ") + cudaGetErrorString(e));
     }
     EBEM_CUDA_TRY(cudaStreamSynchronize(s));
     return EBEM_OK;
