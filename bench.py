@@ -38,11 +38,13 @@ UNIT = "pair-integrals/s"
 FLOPS_PER_PAIR_INTEGRAL = 19_232.0
 FLOPS_PER_PAIR_INTEGRAL_REF_SCHEDULE = 53_560.0
 
-# DRAM bytes (read + write) per launch of the assembly kernel: ncu on the
-# sphere N=320 case measured 30.7 MB + 339.8 MB; the traffic is the N^2 L output
-# (written in 24-byte column pieces), so it is scaled to N=1280 by the output
-# size, x16.
+# DRAM bytes (read + write) of the assembly kernel over the whole workload
+# written in place in one launch: ncu on the sphere N=320 case measured
+# 30.7 MB + 339.8 MB; the traffic is the N^2 L output (written in 24-byte
+# column pieces), so it is scaled to N=1280 by the output size, x16.
 NCU_TRAFFIC_PER_LAUNCH = (30.733056e6 + 339.811584e6) * 16
+
+
 KERNEL = "sa_assemble_warp_kernel"
 
 
@@ -324,7 +326,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
     value = total_pairs * args.steps / t_max
-    kernel_s = my_s / args.steps          # one assembly kernel launch per step
+    launches = 1                        # a device output is assembled in place: one launch per step
+    kernel_s = my_s / (args.steps * launches)
 
     # end to end through the C ABI with host buffers: mesh upload, assembly,
     # copy of E to pinned host memory, every step
@@ -365,7 +368,7 @@ def main():
 
     if rank == 0:
         peak = float("nan") if args.no_peak else fp64_peak_tflops(torch)
-        achieved = FLOPS_PER_PAIR_INTEGRAL * my_pairs / kernel_s / 1e12
+        achieved = FLOPS_PER_PAIR_INTEGRAL * (my_pairs / launches) / kernel_s / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
@@ -374,13 +377,13 @@ def main():
                        "rho": prm.rho, "mu": prm.mu, "lambda": prm.lam, "dt": prm.dt, "nT": prm.nT,
                        "pair_integrals_per_step": total_pairs, "parallelism": f"source-row panels x{world}",
                        "l2": "output 4.7 GB per step written to HBM, far larger than L2"},
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * launches,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
-                         "traffic": NCU_TRAFFIC_PER_LAUNCH,
+                         "traffic": NCU_TRAFFIC_PER_LAUNCH / launches,
                          "peak_source": "measured: cuBLAS DGEMM 8192^3 via torch.matmul float64, best of 5",
                          "flops_per_unit": FLOPS_PER_PAIR_INTEGRAL,
-                         "units_per_launch": my_pairs,
+                         "units_per_launch": my_pairs / launches, "launches_per_step": launches,
                          "kernel": KERNEL, "kernel_ms": kernel_s * 1e3},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "path": "ebem_mesh_create + ebem_assemble_sa_panel into pinned host memory + ebem_mesh_destroy",

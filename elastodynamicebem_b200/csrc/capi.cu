@@ -11,6 +11,10 @@
 #include <initializer_list>
 #include <mutex>
 
+#ifndef EBEM_STAGE_DEVICE_OUTPUT
+#define EBEM_STAGE_DEVICE_OUTPUT 0
+#endif
+
 struct ebem_mesh {
     ebem::MeshData d;
     double lo[3], hi[3];    // bounding box of the vertices (host side)
@@ -356,46 +360,76 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
         }
     }
     int rc = EBEM_OK;
-    if (is_device_ptr(E)) {
+    const bool dev_out = is_device_ptr(E);
+    // Host outputs are assembled in source-row sub-panels into two compact
+    // device buffers (leading dimension 3 x rows) in turn; each is copied into
+    // place (a 2D copy into the strided output) on a second stream while the
+    // next one is assembled.  Device outputs are written in place unless the
+    // library is built with EBEM_STAGE_DEVICE_OUTPUT=1, which stages those of
+    // 1 GiB or more the same way: the assembly alone is faster into compact
+    // sub-panels (sphere of 1280 triangles, L = 40: 196 ms against 204.5 ms),
+    // but with the device-to-device copies running beside it a step took
+    // 195 ms in one run and 217 ms in another, against a steady 204-206 ms in
+    // place.
+    const bool stage = !dev_out || (EBEM_STAGE_DEVICE_OUTPUT && nsrc >= 16 &&
+                                    (size_t)ld * n3 * nlag * sizeof(double) >= ((size_t)1 << 30));
+    if (!stage) {
         rc = launch_sa_assemble(md, P, n_gh, lag0, nlag, src0, nsrc, E, (size_t)ld, lag_elems, accumulate, d_count, s, 0,
                                 prec == EBEM_PREC_MIXED);
     } else {
-        if (ld != 3LL * nsrc) {
+        if (!dev_out && ld != 3LL * nsrc) {
             ws_free(d_count, s);
             return fail(EBEM_ERR_INVALID, "host output needs ld == 3 nsrc");
         }
-        // host output: source-row sub-panels are assembled into two device
-        // buffers in turn; each is copied back (a 2D copy into the strided
-        // host panel) on a second stream while the next one is assembled
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
         const size_t cols = n3 * (size_t)nlag;                     // columns of all lags
         const size_t per_row = 3 * cols * sizeof(double);          // one source triangle, all lags
-        const size_t budget = std::min<size_t>(free_b / 2, (size_t)16 << 30) / 2;   // per buffer
+        size_t budget = std::min<size_t>(free_b / 2, (size_t)16 << 30) / 2;   // per buffer
+        if (dev_out) budget = std::min<size_t>(budget, (size_t)1 << 30);
         int rows = (int)std::max<size_t>(1, std::min<size_t>(budget / per_row, (size_t)(nsrc + 7) / 8));
         rows = std::min(rows, nsrc);
+        // sub-panels of `rows` source rows, the remainder halved down to about
+        // rows / 8: the copy of the last sub-panel overlaps nothing, so it is
+        // kept short (1280 sources: 7 x 160, then 80, 40, 20, 20)
+        std::vector<std::pair<int, int>> parts;             // (first row, rows)
+        {
+            int r0 = 0;
+            while (nsrc - r0 > rows) { parts.push_back({r0, rows}); r0 += rows; }
+            int rest = nsrc - r0;
+            const int tail = std::max(1, rows / 8);
+            while (rest > tail) {
+                const int nr = (rest + 1) / 2;
+                parts.push_back({r0, nr});
+                r0 += nr;
+                rest -= nr;
+            }
+            if (rest > 0) parts.push_back({r0, rest});
+        }
         double* buf[2] = {nullptr, nullptr};
         cudaStream_t cs = nullptr;
         cudaEvent_t done[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+        // every part has at most `rows` rows; a second buffer exactly when there
+        // is a second part
         bool ok = ws_malloc(&buf[0], per_row * rows, s) == cudaSuccess &&
-                  (rows >= nsrc || ws_malloc(&buf[1], per_row * rows, s) == cudaSuccess) &&
+                  (parts.size() < 2 || ws_malloc(&buf[1], per_row * rows, s) == cudaSuccess) &&
                   cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess;
         for (int b = 0; ok && b < 2; b++)
             ok = cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming) == cudaSuccess &&
                  cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming) == cudaSuccess;
         if (!ok) {
             cudaGetLastError();
-            rc = fail(EBEM_ERR_NOMEM, "device staging buffer allocation failed");
+            if (!dev_out) rc = fail(EBEM_ERR_NOMEM, "device staging buffer allocation failed");
         }
-        for (int k = 0, r0 = 0; rc == EBEM_OK && r0 < nsrc; k++, r0 += rows) {
-            const int nr = std::min(rows, nsrc - r0), b = k & 1;
+        for (int k = 0; ok && rc == EBEM_OK && k < (int)parts.size(); k++) {
+            const int r0 = parts[k].first, nr = parts[k].second, b = k & 1;
             const size_t ldb = 3 * (size_t)nr;
             double* hE = E + 3 * (size_t)r0;
             cudaError_t e = cudaSuccess;
             if (k >= 2) e = cudaStreamWaitEvent(s, copied[b], 0);
             if (e == cudaSuccess && accumulate)
                 e = cudaMemcpy2DAsync(buf[b], ldb * sizeof(double), hE, (size_t)ld * sizeof(double), ldb * sizeof(double),
-                                      cols, cudaMemcpyHostToDevice, s);
+                                      cols, cudaMemcpyDefault, s);
             if (e != cudaSuccess) { rc = fail(EBEM_ERR_CUDA, "upload failed"); break; }
             rc = launch_sa_assemble(md, P, n_gh, lag0, nlag, src0 + r0, nr, buf[b], ldb, ldb * n3, accumulate, d_count,
                                     s, 0, prec == EBEM_PREC_MIXED);
@@ -404,7 +438,7 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
             if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, done[b], 0);
             if (e == cudaSuccess)
                 e = cudaMemcpy2DAsync(hE, (size_t)ld * sizeof(double), buf[b], ldb * sizeof(double), ldb * sizeof(double),
-                                      cols, cudaMemcpyDeviceToHost, cs);
+                                      cols, cudaMemcpyDefault, cs);
             if (e == cudaSuccess) e = cudaEventRecord(copied[b], cs);
             if (e != cudaSuccess) { rc = fail(EBEM_ERR_CUDA, "download failed"); break; }
         }
@@ -418,6 +452,10 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
         }
         if (cs) cudaStreamDestroy(cs);
         if (rc == EBEM_OK && e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, cudaGetErrorString(e));
+        // a device output without room for the staging buffers: written in place
+        if (!ok && dev_out && rc == EBEM_OK)
+            rc = launch_sa_assemble(md, P, n_gh, lag0, nlag, src0, nsrc, E, (size_t)ld, lag_elems, accumulate, d_count, s,
+                                    0, prec == EBEM_PREC_MIXED);
     }
     if (d_count) {
         unsigned long long c = 0;

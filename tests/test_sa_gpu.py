@@ -167,3 +167,27 @@ def test_sphere1280_sampled_blocks(ebem, oracle):
     assert np.abs(got - ref).max() <= TOL_F64 * scale
     assert rel(got, ref) <= TOL_F64
     assert np.isfinite(Ec).all()
+
+
+def test_large_device_output_lag_windows(ebem):
+    """The full 4.7 GB device output of the sphere of 1280 triangles (L = 40)
+    equals, bit for bit, its 4-lag windows assembled separately, their
+    non-null counts add up to the full count, and accumulating into a copy of
+    the blocks doubles them exactly."""
+    import torch
+    from elastodynamicebem_b200 import problem
+    w = problem.sphere_workload(7)
+    dm = ebem.DeviceMesh(w.mesh)
+    L = ebem.num_blocks(dm, w.params)
+    E, cnt = ebem.assemble_sa(dm, w.params, 7, 0, L, count=True)
+    total = 0
+    for l0 in range(0, L, 4):
+        nl = min(4, L - l0)
+        Ew, c = ebem.assemble_sa(dm, w.params, 7, l0, nl, count=True)
+        assert torch.equal(Ew, E[l0:l0 + nl])
+        total += c
+        del Ew
+    assert total == cnt
+    buf = E.transpose(1, 2).clone()                         # a copy in the library's column-major storage
+    acc = ebem.assemble_sa(dm, w.params, 7, 0, L, out=buf, accumulate=True)
+    assert torch.equal(acc, 2 * E)
