@@ -88,4 +88,3 @@ def test_mesh_validation(lib):
     h = C.c_void_p()
     rc = lib.ebem_mesh_create(coords.ctypes.data, 3, tris.ctypes.data, 1, C.byref(h))
     assert rc == -1 and b"out of range" in lib.ebem_last_error()
-
