@@ -4,7 +4,8 @@
 Workload: unit icosphere subdivided 3x (1280 triangles, 3840 unknowns per
 step), rho=1, mu=1, lambda=1, dt=0.025, T=1 (Nt=40, L=40 Toeplitz blocks),
 7-point outer Gauss-Hammer rule, plain FP64.  One step = assembly of
-E_0..E_39 (26.1 M non-null pair-lags, 4.7 GB of output, far larger than L2).
+E_0..E_39 (26.68 M non-null pair-lags on this generated icosphere, 26.14 M on
+the reference's sphereUniform_3 mesh; 4.7 GB of output, far larger than L2).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 

@@ -88,6 +88,21 @@ def test_reference_mesh_census():
     assert O.count_nonnull(m, prm, 20) == 257204
 
 
+def test_sphere_census():
+    """The benchmark's unit count: the generated icosphere of 1280 triangles
+    (L = 40) has 26,678,800 non-null pair-lags; the reference's own
+    sphereUniform_3 mesh, whose vertices lie elsewhere, has 26,137,900 (runs
+    only where the reference is mounted)."""
+    import oracle as O
+    from elastodynamicebem_b200 import mesh, problem
+    w = problem.sphere_workload(7)
+    assert O.num_blocks(w.mesh, w.params) == 40
+    assert O.count_nonnull(w.mesh, w.params, 40) == 26_678_800
+    path = "/root/reference/mesh/sphereUniform/sphereUniform_3.mesh"
+    if os.path.exists(path):
+        assert O.count_nonnull(mesh.read_space_mesh(path), w.params, 40) == 26_137_900
+
+
 def test_flop_census_frozen(oracle):
     """The frozen FP64 flops per pair-integral used by bench.py's roofline."""
     import importlib.util
