@@ -220,24 +220,41 @@ def forms(core, problem, torch, w, dm, L, plain_rate):
     return out
 
 
+def workload_config(w, L: int, pairs: int, world: int) -> dict:
+    """The `config` object of both arms' JSON lines."""
+    N, prm = w.mesh.numberTriangles, w.params
+    return {"workload": f"sphere_icosphere{3 if N == 1280 else 2}_N{N}_L{L}_GH7", "N": N, "L": L, "n_gh": w.n_gh,
+            "rho": prm.rho, "mu": prm.mu, "lambda": prm.lam, "dt": prm.dt, "nT": prm.nT,
+            "pair_integrals_per_step": pairs, "parallelism": f"source-row panels x{world}",
+            "l2": "output 4.7 GB per step written to HBM, far larger than L2"}
+
+
 def reference_arm(args, rank: int):
+    """The reference's path on the host cores: the oracle (C++ restatement of
+    its MATLAB SA assembly, three instants per lag) on bounded seeded samples
+    of the same workload, one sample per step; rank 0 only."""
     from elastodynamicebem_b200 import problem
     if rank != 0:
         return
-    w = problem.sphere_workload(7)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    w = problem.sphere_workload(7, subdivisions=3 if args.workload == "sphere1280" else 2)
+    L = O.num_blocks(w.mesh, w.params)
+    pairs = O.count_nonnull(w.mesh, w.params, L)
     vals = []
     info = None
     for _ in range(args.warmup):
-        cpu_baseline(w, target_s=2.0)
+        cpu_baseline(w, target_s=min(2.0, args.reference_sample_s))
     for _ in range(args.steps):
-        info = cpu_baseline(w, target_s=8.0)
+        info = cpu_baseline(w, target_s=args.reference_sample_s)
         vals.append(info["value"])
     v = statistics.median(vals)
     info["value"] = v
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "sphere_icosphere3_N1280_L40_GH7", "N": 1280, "L": 40, "n_gh": 7},
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": pairs / v * 1e3,           # a whole step of the workload at the sampled rate
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(w, L, pairs, 1),
             "cpu_baseline": info,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -254,6 +271,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak measurement")
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed-precision and batched measurements")
+    ap.add_argument("--reference-sample-s", type=float, default=8.0,
+                    help="seconds of host-core work per step of --impl reference")
     ap.add_argument("--workload", default="sphere1280", choices=["sphere1280", "sphere320"],
                     help="sphere1280 is the benchmark; sphere320 (icosphere 2) is the small profiling case")
     args = ap.parse_args()
@@ -374,10 +393,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"sphere_icosphere{3 if N == 1280 else 2}_N{N}_L{L}_GH7", "N": N, "L": L, "n_gh": w.n_gh,
-                       "rho": prm.rho, "mu": prm.mu, "lambda": prm.lam, "dt": prm.dt, "nT": prm.nT,
-                       "pair_integrals_per_step": total_pairs, "parallelism": f"source-row panels x{world}",
-                       "l2": "output 4.7 GB per step written to HBM, far larger than L2"},
+            "config": workload_config(w, L, total_pairs, world),
             "gpu_launches": args.steps * launches,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
