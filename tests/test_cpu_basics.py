@@ -88,3 +88,17 @@ def test_mesh_validation(lib):
     h = C.c_void_p()
     rc = lib.ebem_mesh_create(coords.ctypes.data, 3, tris.ctypes.data, 1, C.byref(h))
     assert rc == -1 and b"out of range" in lib.ebem_last_error()
+
+
+def test_argument_checks_before_any_device_use(lib):
+    """Calls with missing arguments fail with EBEM_ERR_INVALID and a message
+    before touching a device, and releasing the workspace when no pool was
+    ever created succeeds (all of it runs without a GPU)."""
+    out = C.c_void_p()
+    assert lib.ebem_release_workspace() == 0
+    assert lib.ebem_lu_create(None, 4, None, C.byref(out)) == -1 and not out.value
+    assert b"bad arguments" in lib.ebem_last_error()
+    assert lib.ebem_lu_solve(None, None, 1, None) == -1
+    assert lib.ebem_pp_sa(None, None, None, None, 1, None, 1, None, None) == -1
+    assert lib.ebem_march(None, 3, 1, None, 1, None, None) == -1
+    assert lib.ebem_batch_create(None, None, None, 0, 7, 0, C.byref(out)) == -1
