@@ -4,8 +4,10 @@
 // call with no visible CUDA device fails with EBEM_ERR_NODEVICE (there is no
 // CPU path).
 #include "ebem_internal.h"
+#include "ptr_kind.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <initializer_list>
@@ -35,6 +37,17 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_pool_mu;
 cudaMemPool_t g_pool[kMaxDevices] = {};
+// Bumped by ebem_device_release: state cached under an older generation
+// (per-thread library handles, the allocation-free scratch address) is
+// abandoned and rebuilt on next use.
+std::atomic<unsigned> g_generation[kMaxDevices] = {};
+}  // namespace
+
+unsigned device_generation(int dev) {
+    return (dev >= 0 && dev < kMaxDevices) ? g_generation[dev].load(std::memory_order_acquire) : 0u;
+}
+
+namespace {
 
 // The workspace pool of device dev, created on first use.
 cudaError_t workspace_pool(int dev, cudaMemPool_t* pool) {
@@ -119,13 +132,53 @@ int check_problem(const ebem_problem* p) {
     return EBEM_OK;
 }
 
-bool is_device_ptr(const void* p) {
+// Kind of a caller's buffer relative to the current device (the device the
+// call runs on).
+PtrKind ptr_kind(const void* p, int* owner = nullptr) {
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        return PtrKind::Host;
     }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (owner) *owner = at.device;
+    return classify_pointer((int)at.type, at.device, cur);
+}
+
+bool is_device_ptr(const void* p) { return ptr_kind(p) == PtrKind::Device; }
+
+int other_device_error(const void* p) {
+    int owner = -1, cur = -1;
+    ptr_kind(p, &owner);
+    cudaGetDevice(&cur);
+    return fail(EBEM_ERR_INVALID, "a buffer in the memory of device " + std::to_string(owner) +
+                                      " was passed to a call that runs on device " + std::to_string(cur) +
+                                      " (the mesh's device); pass a buffer of that device or a host buffer");
+}
+
+// EBEM_OK when p is device memory usable by the current device, else a
+// failure naming `what`.
+int need_device(const void* p, const char* what) {
+    const PtrKind k = ptr_kind(p);
+    if (k == PtrKind::Device) return EBEM_OK;
+    if (k == PtrKind::OtherDevice) return other_device_error(p);
+    return fail(EBEM_ERR_INVALID, std::string(what) + " must be in device memory");
+}
+
+// A non-null count is copied to the host and waited for, which a stream
+// under capture does not allow: such calls are refused before any work.
+int reject_count_under_capture(const long long* nonnull, cudaStream_t s) {
+    if (!nonnull) return EBEM_OK;
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(EBEM_ERR_INVALID, "the stream's capture status could not be read");
+    }
+    if (st != cudaStreamCaptureStatusNone)
+        return fail(EBEM_ERR_INVALID, "nonnull must be NULL while the stream is being captured (the count is read back "
+                                      "to the host and waited for)");
+    return EBEM_OK;
 }
 
 __global__ void max_vertex_dist_kernel(const double* __restrict__ c, int nv, unsigned long long* out) {
@@ -150,7 +203,9 @@ struct DevIn {
     double* owned = nullptr;
     cudaStream_t st = nullptr;
     int init(const double* p, size_t n, cudaStream_t s) {
-        if (is_device_ptr(p)) { d = p; return EBEM_OK; }
+        const PtrKind k = ptr_kind(p);
+        if (k == PtrKind::Device) { d = p; return EBEM_OK; }
+        if (k == PtrKind::OtherDevice) return other_device_error(p);
         st = s;
         if (ws_malloc(&owned, n * sizeof(double), s) != cudaSuccess)
             return fail(EBEM_ERR_NOMEM, "device staging allocation failed");
@@ -170,7 +225,9 @@ struct DevOut {
     cudaStream_t st = nullptr;
     int init(double* p, size_t count, cudaStream_t s) {
         n = count;
-        if (is_device_ptr(p)) { d = p; return EBEM_OK; }
+        const PtrKind k = ptr_kind(p);
+        if (k == PtrKind::Device) { d = p; return EBEM_OK; }
+        if (k == PtrKind::OtherDevice) return other_device_error(p);
         host = p;
         st = s;
         if (ws_malloc(&d, n * sizeof(double), s) != cudaSuccess)
@@ -213,6 +270,43 @@ int ebem_release_workspace(void) {
         }
     }
     if (prev >= 0) cudaSetDevice(prev);
+    return EBEM_OK;
+}
+
+int ebem_workspace_info(int device, unsigned long long* reserved, unsigned long long* used) {
+    if (device < 0 || device >= kMaxDevices) return fail(EBEM_ERR_INVALID, "device ordinal out of range");
+    unsigned long long r = 0, u = 0;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (g_pool[device]) {
+        cudaMemPoolGetAttribute(g_pool[device], cudaMemPoolAttrReservedMemCurrent, &r);
+        cudaMemPoolGetAttribute(g_pool[device], cudaMemPoolAttrUsedMemCurrent, &u);
+        cudaGetLastError();
+    }
+    if (reserved) *reserved = r;
+    if (used) *used = u;
+    return EBEM_OK;
+}
+
+int ebem_device_release(int device) {
+    if (device < 0 || device >= kMaxDevices) return fail(EBEM_ERR_INVALID, "device ordinal out of range");
+    // first: every cached handle and address of this device becomes stale
+    g_generation[device].fetch_add(1, std::memory_order_acq_rel);
+    cudaError_t e = cudaSuccess;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        if (g_pool[device]) {
+            DeviceGuard dg(device);
+            e = cudaDeviceSynchronize();
+            cudaError_t e2 = cudaMemPoolDestroy(g_pool[device]);
+            if (e == cudaSuccess) e = e2;
+            g_pool[device] = nullptr;
+        }
+    }
+    release_thread_handles(device);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(EBEM_ERR_CUDA, std::string("device release: ") + cudaGetErrorString(e));
+    }
     return EBEM_OK;
 }
 
@@ -309,6 +403,24 @@ int ebem_mesh_derived(const ebem_mesh* m, double* normal, double* area, double* 
     return EBEM_OK;
 }
 
+int ebem_mesh_cache_info(const ebem_mesh* m, int* rules_cached, long long* device_bytes) {
+    if (!m) return fail(EBEM_ERR_INVALID, "mesh is NULL");
+    static const int kSlotRule[MeshData::kNodeRules] = {1, 3, 7, 12, 19, 28};
+    const MeshData& d = m->d;
+    long long bytes = (long long)sizeof(double) * 3 * d.nv + (long long)sizeof(int32_t) * 3 * d.nt +
+                      (long long)sizeof(TriGeom) * d.nt;
+    int mask = 0;
+    for (int k = 0; k < MeshData::kNodeRules; k++)
+        if (d.d_node_tables[k]) {
+            mask |= 1 << k;
+            bytes += 32LL * d.nt * kSlotRule[k];
+        }
+    if (d.d_dir) bytes += (long long)sizeof(DirTri) * d.nt + (long long)sizeof(int32_t) * (d.nv + 1 + 3LL * d.nt);
+    if (rules_cached) *rules_cached = mask;
+    if (device_bytes) *device_bytes = bytes;
+    return EBEM_OK;
+}
+
 int ebem_num_blocks(const ebem_mesh* m, const ebem_problem* p, int* num_blocks) {
     if (!m || !num_blocks) return fail(EBEM_ERR_INVALID, "NULL argument");
     if (int rc = check_problem(p)) return rc;
@@ -345,6 +457,7 @@ static int assemble_impl(const ebem_mesh* m, const ebem_problem* p, int n_gh, in
     if (prec != EBEM_PREC_FP64 && prec != EBEM_PREC_MIXED) return fail(EBEM_ERR_INVALID, "unknown precision mode");
     DeviceGuard dg(m->d.device);
     cudaStream_t s = (cudaStream_t)stream;
+    if (int rc = reject_count_under_capture(nonnull, s)) return rc;
     MeshData& md = const_cast<MeshData&>(m->d);
     if (int rc = map_nodes(md, n_gh, s)) return rc;
     PhysParams P = phys_from(p);
@@ -619,7 +732,7 @@ int ebem_lu_create(const double* A, int n, void* stream, ebem_lu** out) {
     *out = nullptr;
     if (!A || n < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
     if (int rc = check_device()) return rc;
-    if (!is_device_ptr(A)) return fail(EBEM_ERR_INVALID, "the matrix must be in device memory");
+    if (int rc = need_device(A, "the matrix")) return rc;
     ebem_lu* lu = new ebem_lu();
     cudaGetDevice(&lu->device);
     if (int rc = lu_plan_create(A, n, (cudaStream_t)stream, &lu->plan)) {
@@ -634,7 +747,7 @@ int ebem_lu_create(const double* A, int n, void* stream, ebem_lu** out) {
 int ebem_lu_solve(ebem_lu* lu, double* b, int nrhs, void* stream) {
     if (!lu || !b || nrhs < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
     DeviceGuard dg(lu->device);
-    if (!is_device_ptr(b)) return fail(EBEM_ERR_INVALID, "the right-hand side must be in device memory");
+    if (int rc = need_device(b, "the right-hand side")) return rc;
     return lu_plan_solve(&lu->plan, b, nrhs, (cudaStream_t)stream);
 }
 
@@ -648,8 +761,8 @@ void ebem_lu_destroy(ebem_lu* lu) {
 int ebem_history_gemv(const double* A, int rows, long long K, const double* x, double* y, void* stream) {
     if (!A || !x || !y || rows < 1 || K < 0) return fail(EBEM_ERR_INVALID, "bad arguments");
     if (int rc = check_device()) return rc;
-    if (!is_device_ptr(A) || !is_device_ptr(x) || !is_device_ptr(y))
-        return fail(EBEM_ERR_INVALID, "A, x and y must be in device memory");
+    for (const void* q : {(const void*)A, (const void*)x, (const void*)y})
+        if (int rc = need_device(q, "A, x and y")) return rc;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -895,7 +1008,8 @@ int ebem_assemble_sa_noalloc(const ebem_mesh* m, const ebem_problem* p, int n_gh
         return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
     if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
     DeviceGuard dg(m->d.device);
-    if (!is_device_ptr(E)) return fail(EBEM_ERR_INVALID, "the allocation-free assembly needs a device output buffer");
+    if (int rc = need_device(E, "the output of the allocation-free assembly")) return rc;
+    if (int rc = reject_count_under_capture(nonnull, (cudaStream_t)stream)) return rc;
     PhysParams P = phys_from(p);
     unsigned long long c = 0;
     int rc = launch_sa_assemble_noalloc(m->d, P, n_gh, lag0, nlag, E, accumulate, nonnull != nullptr, &c,
@@ -1049,7 +1163,8 @@ int ebem_batch_assemble(ebem_batch* b, double* const* E, void* stream) {
     if (!b || !E) return fail(EBEM_ERR_INVALID, "NULL batch or outputs");
     DeviceGuard dg(b->device);
     for (int k = 0; k < b->n; k++) {
-        if (!E[k] || !is_device_ptr(E[k])) return fail(EBEM_ERR_INVALID, "batch outputs must be device buffers");
+        if (!E[k]) return fail(EBEM_ERR_INVALID, "batch outputs must be device buffers");
+        if (int rc = need_device(E[k], "every batch output")) return rc;
         b->h_insts[k].E = E[k];
     }
     cudaStream_t s = (cudaStream_t)stream;

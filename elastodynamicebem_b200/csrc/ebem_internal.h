@@ -20,6 +20,13 @@ namespace ebem {
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 
+// Generation of device dev's cached state, bumped by ebem_device_release:
+// per-thread library handles and the allocation-free scratch address cached
+// under an older generation are abandoned and rebuilt on next use.
+unsigned device_generation(int dev);
+// Destroys the calling thread's cuSOLVER / cuBLAS handles of device dev.
+void release_thread_handles(int dev);
+
 // Per-call device workspace, stream-ordered, from a memory pool the library
 // keeps for each device.  Up to kWorkspaceKeep bytes stay reserved in the pool
 // between calls, so a repeated call allocates without a driver call and

@@ -327,6 +327,7 @@ constexpr int kHandleDevices = 64;
 struct ThreadHandles {
     cusolverDnHandle_t sol[kHandleDevices];
     cublasHandle_t blas[kHandleDevices];
+    unsigned sol_gen[kHandleDevices], blas_gen[kHandleDevices];   // device generation at creation
 };
 thread_local ThreadHandles t_handles = {};
 
@@ -343,9 +344,14 @@ int solver_handle(cudaStream_t s, cusolverDnHandle_t* h) {
     int dev = 0;
     if (int rc = handle_device(&dev)) return rc;
     cusolverDnHandle_t& c = t_handles.sol[dev];
-    if (!c && cusolverDnCreate(&c) != CUSOLVER_STATUS_SUCCESS) {
-        c = nullptr;
-        return fail(EBEM_ERR_CUDA, "cuSOLVER handle creation failed");
+    const unsigned gen = device_generation(dev);
+    if (c && t_handles.sol_gen[dev] != gen) c = nullptr;      // released device state: abandoned
+    if (!c) {
+        if (cusolverDnCreate(&c) != CUSOLVER_STATUS_SUCCESS) {
+            c = nullptr;
+            return fail(EBEM_ERR_CUDA, "cuSOLVER handle creation failed");
+        }
+        t_handles.sol_gen[dev] = gen;
     }
     if (cusolverDnSetStream(c, s) != CUSOLVER_STATUS_SUCCESS) return fail(EBEM_ERR_CUDA, "cuSOLVER stream binding failed");
     *h = c;
@@ -356,13 +362,32 @@ int blas_handle(cudaStream_t s, cublasHandle_t* h) {
     int dev = 0;
     if (int rc = handle_device(&dev)) return rc;
     cublasHandle_t& c = t_handles.blas[dev];
-    if (!c && cublasCreate(&c) != CUBLAS_STATUS_SUCCESS) {
-        c = nullptr;
-        return fail(EBEM_ERR_CUDA, "cuBLAS handle creation failed");
+    const unsigned gen = device_generation(dev);
+    if (c && t_handles.blas_gen[dev] != gen) c = nullptr;     // released device state: abandoned
+    if (!c) {
+        if (cublasCreate(&c) != CUBLAS_STATUS_SUCCESS) {
+            c = nullptr;
+            return fail(EBEM_ERR_CUDA, "cuBLAS handle creation failed");
+        }
+        t_handles.blas_gen[dev] = gen;
     }
     if (cublasSetStream(c, s) != CUBLAS_STATUS_SUCCESS) return fail(EBEM_ERR_CUDA, "cuBLAS stream binding failed");
     *h = c;
     return EBEM_OK;
+}
+
+void release_thread_handles(int dev) {
+    if (dev < 0 || dev >= kHandleDevices) return;
+    if (!t_handles.sol[dev] && !t_handles.blas[dev]) return;
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaSetDevice(dev);
+    if (t_handles.sol[dev]) cusolverDnDestroy(t_handles.sol[dev]);
+    if (t_handles.blas[dev]) cublasDestroy(t_handles.blas[dev]);
+    t_handles.sol[dev] = nullptr;
+    t_handles.blas[dev] = nullptr;
+    if (prev >= 0) cudaSetDevice(prev);
+    cudaGetLastError();
 }
 
 // phi (device, column-major n3 x nT) from E (device, n3 x n3 x L) and rhs

@@ -669,19 +669,24 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 size_t noalloc_max_nodes() { return kNoAllocMaxNodes; }
 
 // Device address of the scratch array on the current device, looked up once
-// per device (the host-side name of the array is not a device address).
+// per device (the host-side name of the array is not a device address) and
+// again after ebem_device_release, whose caller may reset the device (a new
+// context may place the array elsewhere).
 static int noalloc_scratch(int device, unsigned char** out) {
     constexpr int kMaxDevices = 64;
     static unsigned char* addr[kMaxDevices] = {};
+    static unsigned gen[kMaxDevices] = {};
     static std::mutex mu;
     if (device < 0 || device >= kMaxDevices) return fail(EBEM_ERR_INVALID, "device ordinal beyond the supported range");
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[device]) {
+    const unsigned g = device_generation(device);
+    if (!addr[device] || gen[device] != g) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             return fail(EBEM_ERR_CUDA, std::string("scratch address lookup failed: ") + cudaGetErrorString(e));
         addr[device] = (unsigned char*)p;
+        gen[device] = g;
     }
     *out = addr[device];
     return EBEM_OK;

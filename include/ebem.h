@@ -71,6 +71,23 @@ const char* ebem_last_error(void);
  * that no call in flight uses (after the calls in flight have finished). */
 int ebem_release_workspace(void);
 
+/* Bytes the workspace pool of `device` holds reserved and in use (both 0
+ * when the library has not used that device).  No counterpart in the
+ * reference. */
+int ebem_workspace_info(int device, unsigned long long* reserved, unsigned long long* used);
+
+/* Release everything the library keeps for `device` between calls, before
+ * its CUDA context is reset (cudaDeviceReset, or the reset(gpuDevice) that
+ * f/BEMenerg_indir/BEMenerg_core/BEMenerg_coreGPU/BEMenerg_coreGPU_timeMarching.m:7,170
+ * runs at entry and exit): waits for the device, destroys the workspace pool
+ * and the calling thread's cuSOLVER / cuBLAS handles, and forgets the device
+ * address of the allocation-free assembly's scratch array.  Handles of other
+ * host threads are abandoned (not destroyed) at their next use.  Later calls
+ * rebuild all of it.  Objects the caller holds (meshes, batch plans, banded
+ * operators, LU plans) own device memory of that context: destroy them
+ * before the reset.  No counterpart in the reference. */
+int ebem_device_release(int device);
+
 /* Gauss-Hammer composite rule.  Replaces f/utility/quadRules/
  * GaussHammerComposite.m:1 (with the base tables of GaussHammer_base.m).
  * n_nodes in {1,3,7,12,19,28}; n_sub in {1,4,16,64,...} (a square);
@@ -90,6 +107,11 @@ int ebem_mesh_info(const ebem_mesh* mesh, int* n_vertices, int* n_triangles);
 /* Derived fields copied to host arrays (any may be NULL): normal (N x 3),
  * area (N), center (N x 3), maxl (N); readSpaceMesh.m:114-139. */
 int ebem_mesh_derived(const ebem_mesh* mesh, double* normal, double* area, double* center, double* maxl);
+/* Device data the mesh handle holds: rules_cached bit k set when the mapped
+ * outer-node table of rule k (1, 3, 7, 12, 19, 28 nodes) is cached, and the
+ * device bytes held (geometry, cached tables, direct-formulation data).
+ * No counterpart in the reference. */
+int ebem_mesh_cache_info(const ebem_mesh* mesh, int* rules_cached, long long* device_bytes);
 
 /* Number of non-zero Toeplitz blocks L = min(nT, ceil(maxDist/(c_S dt)) + 1).
  * Replaces .../BEMenerg_coreGPU/BEMenerg_coreGPU_calcNumBlocks.m:1-20. */
@@ -107,7 +129,10 @@ int ebem_num_blocks(const ebem_mesh* mesh, const ebem_problem* prob, int* num_bl
  * E: 9 N^2 nlag doubles, host or device.  accumulate = 0 overwrites every
  * entry (zeros included); 1 adds (E += block), as the reference kernels do.
  * nonnull (may be NULL): number of (source, field, lag) blocks that pass the
- * null test; requesting it synchronises the stream. */
+ * null test; requesting it synchronises the stream, so it must be NULL on a
+ * stream under capture (EBEM_ERR_INVALID otherwise).  A device E must belong
+ * to the mesh's device (EBEM_ERR_INVALID otherwise); so must every device
+ * buffer passed to a mesh-based entry point below. */
 int ebem_assemble_sa(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag,
                      double* E, int accumulate, void* stream, long long* nonnull);
 
@@ -149,11 +174,13 @@ int ebem_assemble_sa_panel(const ebem_mesh* mesh, const ebem_problem* prob, int 
  * buffer of 9 N^2 nlag doubles.
  *
  * The first call on a device looks up the device address of the array (a
- * one-time set-up); make that first call before any stream capture.  All
- * calls on a device share the array and each call rewrites it (the counter
- * is zeroed by every call that asks for nonnull): calls whose work can
- * overlap on the GPU (different streams, no ordering between them) race and
- * must be serialised by the caller. */
+ * one-time set-up, repeated once after ebem_device_release); make that first
+ * call before any stream capture.  nonnull must be NULL on a stream under
+ * capture (the count is read back and waited for).  All calls on a device
+ * share the array and each call rewrites it (the counter is zeroed by every
+ * call that asks for nonnull): calls whose work can overlap on the GPU
+ * (different streams, no ordering between them) race and must be serialised
+ * by the caller. */
 int ebem_assemble_sa_noalloc(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag,
                              double* E, int accumulate, void* stream, long long* nonnull);
 

@@ -26,6 +26,10 @@ def test_reference_arm_line():
     assert d["metric"].startswith("E_l assembly pair-integrals/s") and d["value"] > 0 and d["ms_per_step"] > 0
     cfg = d["config"]
     assert cfg["workload"] == "sphere_icosphere3_N1280_L40_GH7" and cfg["pair_integrals_per_step"] == 26_678_800
+    # the step time is the measured time of the sampled work, not an extrapolation to a full step
+    assert d["ms_per_step"] <= 1e3 * (cb_s := d["cpu_baseline"]["seconds"]) * 1.0001 + 1e-9
+    assert d["ms_per_step"] < 60_000 and "sample" in cfg["reference_step"]
+    assert cfg["l2"].startswith("output 4.72 GB per step")
     cb = d["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}

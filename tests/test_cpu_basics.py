@@ -102,3 +102,52 @@ def test_argument_checks_before_any_device_use(lib):
     assert lib.ebem_pp_sa(None, None, None, None, 1, None, 1, None, None) == -1
     assert lib.ebem_march(None, 3, 1, None, 1, None, None) == -1
     assert lib.ebem_batch_create(None, None, None, 0, 7, 0, C.byref(out)) == -1
+
+
+def test_device_state_release_without_device(lib):
+    """ebem_device_release and ebem_workspace_info on a device the library has
+    never used: nothing is cached, both succeed without touching a GPU; an
+    ordinal outside the supported range is refused."""
+    r, u = C.c_ulonglong(7), C.c_ulonglong(7)
+    assert lib.ebem_workspace_info(0, C.byref(r), C.byref(u)) == 0
+    assert (r.value, u.value) == (0, 0)
+    assert lib.ebem_device_release(0) == 0
+    assert lib.ebem_device_release(-1) == -1 and b"out of range" in lib.ebem_last_error()
+    assert lib.ebem_device_release(64) == -1
+    assert lib.ebem_workspace_info(64, None, None) == -1
+
+
+def test_pointer_classification(tmp_path):
+    """The C ABI's buffer classification (csrc/ptr_kind.h): device memory of
+    the call's device is used in place, device memory of another GPU is
+    refused, managed memory is usable from every device, host memory (pinned
+    or not) is staged.  Compiled with g++ and run on the CPU."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    src = tmp_path / "ptr_kind_check.cpp"
+    src.write_text(r'''
+#include "ptr_kind.h"
+#include <cstdio>
+using ebem::PtrKind;
+using ebem::classify_pointer;
+int main() {
+    int bad = 0;
+    // (cudaMemoryType, owning device, current device) -> kind
+    struct { int t, owner, cur; PtrKind want; } cases[] = {
+        {0, -2, 0, PtrKind::Host},  {1, 0, 0, PtrKind::Host},   {1, 1, 0, PtrKind::Host},
+        {2, 0, 0, PtrKind::Device}, {2, 3, 3, PtrKind::Device}, {2, 1, 0, PtrKind::OtherDevice},
+        {2, 0, 5, PtrKind::OtherDevice}, {3, 0, 0, PtrKind::Device}, {3, 2, 0, PtrKind::Device},
+    };
+    for (auto& c : cases)
+        if (classify_pointer(c.t, c.owner, c.cur) != c.want) { std::printf("case %d %d %d\n", c.t, c.owner, c.cur); bad++; }
+    return bad;
+}
+''')
+    exe = tmp_path / "ptr_kind_check"
+    subprocess.run([gxx, "-std=c++17", "-I", os.path.join(ROOT, "elastodynamicebem_b200", "csrc"), str(src), "-o",
+                    str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout

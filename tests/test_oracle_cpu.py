@@ -78,9 +78,8 @@ def test_null_census_screen():
 def test_reference_mesh_census():
     """On the reference's own screenUniform_2 mesh the census is 257,204
     (runs only where the reference is mounted)."""
-    path = "/root/reference/mesh/screenUniform/screenUniform_2.mesh"
-    if not os.path.exists(path):
-        pytest.skip("reference mesh not available")
+    from conftest import reference_file
+    path = reference_file("mesh", "screenUniform", "screenUniform_2.mesh")
     import oracle as O
     from elastodynamicebem_b200 import mesh, problem
     m = mesh.read_space_mesh(path)
@@ -98,7 +97,8 @@ def test_sphere_census():
     w = problem.sphere_workload(7)
     assert O.num_blocks(w.mesh, w.params) == 40
     assert O.count_nonnull(w.mesh, w.params, 40) == 26_678_800
-    path = "/root/reference/mesh/sphereUniform/sphereUniform_3.mesh"
+    from conftest import REFERENCE_ROOT
+    path = os.path.join(REFERENCE_ROOT, "mesh", "sphereUniform", "sphereUniform_3.mesh")
     if os.path.exists(path):
         assert O.count_nonnull(mesh.read_space_mesh(path), w.params, 40) == 26_137_900
 

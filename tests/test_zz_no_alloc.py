@@ -92,6 +92,71 @@ def test_rule_change_between_calls(env):
     assert _rel(a, ref3) <= TOL and _rel(b, ref7) <= TOL
 
 
+def test_allocates_nothing(env):
+    """What the entry point exists for: with the library's workspace pool
+    emptied and a fresh mesh handle (no cached outer-node table), two calls
+    in a row leave the pool empty, build no table in the mesh and take no
+    device memory (free bytes unchanged), and still match the ordinary
+    assembly, which does allocate (it builds and caches the table)."""
+    torch, core, lib, L = env
+    from elastodynamicebem_b200 import problem
+    w = problem.screen_workload()
+    dm = core.DeviceMesh(w.mesh)
+    nlag = core.num_blocks(dm, w.params)
+    n3 = 3 * dm.N
+    out = torch.empty(nlag * n3 * n3, dtype=torch.float64, device="cuda")
+    p = lib.problem_struct(w.params)
+    dev = torch.cuda.current_device()
+
+    def state():
+        mask, nbytes = C.c_int(-1), C.c_longlong(-1)
+        lib.check(L.ebem_mesh_cache_info(dm.handle, C.byref(mask), C.byref(nbytes)))
+        res, used = C.c_ulonglong(), C.c_ulonglong()
+        lib.check(L.ebem_workspace_info(dev, C.byref(res), C.byref(used)))
+        return mask.value, nbytes.value, res.value, used.value
+
+    lib.check(L.ebem_assemble_sa_noalloc(dm.handle, C.byref(p), 7, 0, nlag, C.c_void_p(out.data_ptr()), 0, None,
+                                         None))                     # first call: one-time address look-up
+    torch.cuda.synchronize()
+    lib.check(L.ebem_release_workspace())
+    before = state()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        lib.check(L.ebem_assemble_sa_noalloc(dm.handle, C.byref(p), 7, 0, nlag, C.c_void_p(out.data_ptr()), 0,
+                                             None, None))
+    torch.cuda.synchronize()
+    after = state()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert after == before
+    assert before[0] == 0 and before[2] == 0 and before[3] == 0    # no table cached, pool empty
+    got = out.clone()
+    ref, _ = _ordinary(env, dm, w.params, 7, nlag)
+    assert _rel(got, ref) <= TOL
+    mask, nbytes, _, _ = state()
+    assert mask == 1 << 2 and nbytes > after[1]          # the ordinary call cached the 7-node table
+
+
+def test_count_refused_under_capture(env):
+    """The non-null count is read back and waited for, which a stream under
+    capture does not allow: such a call is refused before it does any work."""
+    torch, core, lib, L = env
+    from elastodynamicebem_b200 import mesh, problem
+    m, prm = mesh.screen_uniform(2), problem.ProblemParams(1.0, 1.0, 2.0, 1.0, 4)
+    dm = core.DeviceMesh(m)
+    out = torch.zeros(9 * m.numberTriangles ** 2, dtype=torch.float64, device="cuda")
+    p = lib.problem_struct(prm)
+    cnt = C.c_longlong(-1)
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        g.capture_begin()
+        rc = L.ebem_assemble_sa_noalloc(dm.handle, C.byref(p), 7, 0, 1, C.c_void_p(out.data_ptr()), 0,
+                                        C.c_void_p(s.cuda_stream), C.byref(cnt))
+        msg = L.ebem_last_error()
+        g.capture_end()
+    assert rc == -1 and b"capture" in msg and cnt.value == -1
+
+
 def test_rejects_mesh_beyond_scratch(env):
     torch, core, lib, L = env
     from elastodynamicebem_b200 import mesh, problem
