@@ -500,6 +500,60 @@ int or_march(const double* E, int n3, int L, const double* rhs, int nT, double* 
     return 0;
 }
 
+// The same marching with the LU factorisation, the history sums and the
+// solves carried out in `real` (binary128 in the quad build; identical to
+// or_march's arithmetic order otherwise), the inputs being the double
+// blocks and right-hand side: the exact marching of the given data, used to
+// pin the time-marched density of the benchmark configurations.
+int or_march_exact(const double* E, int n3, int L, const double* rhs, int nT, double* phi) {
+    std::vector<real> A(E, E + (size_t)n3 * n3);
+    std::vector<int> piv(n3);
+    for (int k = 0; k < n3; k++) {                       // column-major, partial pivoting
+        int p = k;
+        real best = oracle::fabs(A[(size_t)k * n3 + k]);
+        for (int i = k + 1; i < n3; i++) {
+            real v = oracle::fabs(A[(size_t)k * n3 + i]);
+            if (v > best) { best = v; p = i; }
+        }
+        if (best == 0) return -1;
+        piv[k] = p;
+        if (p != k)
+            for (int j = 0; j < n3; j++) std::swap(A[(size_t)j * n3 + k], A[(size_t)j * n3 + p]);
+        const real d = A[(size_t)k * n3 + k];
+        for (int i = k + 1; i < n3; i++) A[(size_t)k * n3 + i] /= d;
+        for (int j = k + 1; j < n3; j++) {
+            const real f = A[(size_t)j * n3 + k];
+            if (f == 0) continue;
+            for (int i = k + 1; i < n3; i++) A[(size_t)j * n3 + i] -= A[(size_t)k * n3 + i] * f;
+        }
+    }
+    std::vector<real> ph((size_t)n3 * nT), b(n3);
+    for (int n = 0; n < nT; n++) {
+        for (int i = 0; i < n3; i++) b[i] = rhs[(size_t)n * n3 + i];
+        const int endInd = std::min(n + 1, L);
+        for (int mm = 1; mm < endInd; mm++) {
+            const double* Em = E + (size_t)mm * n3 * n3;
+            const real* pp = ph.data() + (size_t)(n - mm) * n3;
+            for (int j = 0; j < n3; j++) {
+                const real pj = pp[j];
+                if (pj == 0) continue;
+                const double* col = Em + (size_t)j * n3;
+                for (int i = 0; i < n3; i++) b[i] -= real(col[i]) * pj;
+            }
+        }
+        for (int k = 0; k < n3; k++) std::swap(b[k], b[piv[k]]);
+        for (int k = 0; k < n3; k++)                     // L y = P b (unit lower)
+            for (int i = k + 1; i < n3; i++) b[i] -= A[(size_t)k * n3 + i] * b[k];
+        for (int k = n3 - 1; k >= 0; k--) {              // U x = y
+            b[k] /= A[(size_t)k * n3 + k];
+            for (int i = 0; i < k; i++) b[i] -= A[(size_t)k * n3 + i] * b[k];
+        }
+        for (int i = 0; i < n3; i++) ph[(size_t)n * n3 + i] = b[i];
+    }
+    for (size_t i = 0; i < ph.size(); i++) phi[i] = (double)ph[i];
+    return 0;
+}
+
 // Closed-form single-instant block of BEMenerg_postProcA_calcMatrixBlock.m.
 static M3 pp_block(const Params& p, const TriConst& F, const double x[3], double tau) {
     M3 ris;
@@ -534,7 +588,7 @@ int or_pp_sa(const double* coords, int nv, const int* tris, int nt,
         int ix = (int)(q % npts), it = (int)(q / npts);
         double t = times[it];
         const double* x = pts + 3 * ix;
-        double uu[3] = {0, 0, 0};
+        real uu[3] = {0, 0, 0};
         if (t > 0) {
             int nHat = (int)std::ceil(t / p.dt) - 1;
             std::vector<M3> cur(nt), nxt(nt);
@@ -558,7 +612,7 @@ int or_pp_sa(const double* coords, int nv, const int* tris, int nt,
             for (int j = 0; j < nt; j++)
                 for (int a = 0; a < 3; a++) for (int b = 0; b < 3; b++) uu[a] += cur[j].m[a][b] * al[3 * j + b];
         }
-        for (int a = 0; a < 3; a++) u[3 * (size_t)q + a] = uu[a];
+        for (int a = 0; a < 3; a++) u[3 * (size_t)q + a] = (double)uu[a];
     }
     return 0;
 }

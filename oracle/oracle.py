@@ -49,6 +49,7 @@ def lib(variant: str = "f64"):
         L.or_rhs.argtypes = mesh_args + par + [C.c_int, C.c_int, _dp]
         L.or_tn_test.argtypes = [C.c_double] * 7 + [C.c_int] * 3 + [_dp]
         L.or_march.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, _dp]
+        L.or_march_exact.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, _dp]
         L.or_pp_sa.argtypes = mesh_args + par + [_dp, _dp, C.c_int, _dp, C.c_int, _dp, C.c_int]
         L.or_assemble_ghc.argtypes = mesh_args + par + [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_int]
         L.or_count_nonnull.argtypes = mesh_args + par + [C.c_int]
@@ -135,6 +136,19 @@ def march(E, b):
     phi = np.zeros(n3 * nT)
     rc = lib().or_march(Ecm, n3, L, bcm, nT, phi)
     if rc:
+        raise ValueError("singular E_0")
+    return phi.reshape(nT, n3).T.copy()
+
+
+def march_exact(E, b, variant: str = "q"):
+    """The marching of `march` with the factorisation, history sums and
+    solves in binary128 (variant "q") on the given double data."""
+    L, n3, _ = E.shape
+    nT = b.shape[1]
+    Ecm = np.ascontiguousarray(E.transpose(0, 2, 1)).ravel()
+    bcm = np.ascontiguousarray(b.T).ravel()
+    phi = np.zeros(n3 * nT)
+    if lib(variant).or_march_exact(Ecm, n3, L, bcm, nT, phi):
         raise ValueError("singular E_0")
     return phi.reshape(nT, n3).T.copy()
 
@@ -244,6 +258,42 @@ def ref_ghc(mesh, prm, n_gh: int, n_sub: int, n_sing: int, nlag: int):
                    verts.ravel(), np.ascontiguousarray(mesh.area), 0, nlag)
     if rc:
         raise RuntimeError(f"reference kernelGHC launch failed ({rc})")
+    n3 = 3 * N
+    return E.reshape(nlag, n3, n3).transpose(0, 2, 1)
+
+
+def ref_ghc_composite(mesh, prm, n_gh: int, n_sub: int, n_sing: int, nlag: int, max_threads: int = 1024):
+    """The reference's kernelGHC with an inner composite rule of any size.
+
+    The kernel runs one thread per inner node in a block of (n_sub, n_sing)
+    threads, so a single launch is limited to n_sub * n_sing <= 1024.  The
+    composite rule is a sum over its sub-triangles, so a larger rule is run as
+    consecutive launches over chunks of its sub-triangles (nodes sub * n_sing
+    + sing, GaussHammerComposite.m's order) with the full rule's weights; the
+    launcher accumulates into the same matrix (E += block, kernelGHC.cu:165).
+    Chunks hold a power of two of sub-triangles, as the kernel's shared-memory
+    tree reduction over x requires."""
+    L = C.CDLL(os.path.join(_HERE, "_ref", "libref_ghc.so"))
+    L.ref_ghc.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp,
+                          C.c_int, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_int, C.c_int]
+    N = mesh.numberTriangles
+    gn, gw = gauss_hammer(n_gh, 1)
+    cn, cw = gauss_hammer(n_sing, n_sub)
+    chunk = n_sub
+    while chunk * n_sing > max_threads:
+        chunk //= 2
+    if chunk < 1 or n_sub % chunk:
+        raise ValueError("composite rule cannot be split into power-of-two chunks")
+    P = mesh.coordinates[mesh.triangles]
+    verts = np.ascontiguousarray(P.transpose(0, 2, 1).reshape(N, 9)).ravel()
+    E = np.zeros(9 * N * N * nlag)
+    for c0 in range(0, n_sub, chunk):
+        nodes = np.ascontiguousarray(cn[c0 * n_sing:(c0 + chunk) * n_sing])
+        rc = L.ref_ghc(E, N, nlag, prm.dt, prm.velP, prm.velS, 4 * np.pi * prm.rho, np.ascontiguousarray(gw),
+                       np.ascontiguousarray(gn), n_gh, np.ascontiguousarray(cw), nodes, chunk, n_sing, verts,
+                       np.ascontiguousarray(mesh.area), 0, nlag)
+        if rc:
+            raise RuntimeError(f"reference kernelGHC launch failed ({rc})")
     n3 = 3 * N
     return E.reshape(nlag, n3, n3).transpose(0, 2, 1)
 
