@@ -276,6 +276,25 @@ def pp_sa(dmesh: DeviceMesh, prm: ProblemParams, phi: torch.Tensor, points, time
     return u
 
 
+PP_POINT = 0     # kernelSP semantics: u(x, :) of one point over its times
+PP_LAYER = 1     # kernelLayer semantics: u(:, t) of many points at one time
+
+
+def pp_gpu(dmesh: DeviceMesh, prm: ProblemParams, phi: torch.Tensor, points, times, n_sub: int, n_sing: int,
+           variant: int = PP_LAYER, fix_defects: bool = False, stream=None):
+    """Numerical post-processing (the reference's method "GPU n_sub n_sing"):
+    displacement u (ntimes, npts, 3) from the density phi (nT, 3N)."""
+    pts = torch.as_tensor(np.ascontiguousarray(points, np.float64)).to(phi.device)
+    tms = np.ascontiguousarray(times, np.float64)
+    u = torch.empty((len(tms), pts.shape[0], 3), dtype=torch.float64, device=phi.device)
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_pp_gpu(dmesh.handle, C.byref(p), int(n_sub), int(n_sing), int(variant),
+                                       1 if fix_defects else 0, _ptr(phi.contiguous()), _ptr(pts),
+                                       int(pts.shape[0]), tms.ctypes.data, len(tms), _ptr(u),
+                                       _stream_ptr(stream) if u.is_cuda else None))
+    return u
+
+
 def assemble_ghc(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, n_sub: int, n_sing: int, lag0: int = 0,
                  nlag: int | None = None, out: torch.Tensor | None = None, sa_diagonal: bool = True, stream=None):
     """Numerical-inner E_lag0.. (the reference's GPU method): returns E[l][row, col]

@@ -851,6 +851,32 @@ static int check_rules(int n_gh, int n_sub, int n_sing, int n_diag) {
     return EBEM_OK;
 }
 
+int ebem_pp_gpu(const ebem_mesh* m, const ebem_problem* p, int n_sub, int n_sing, int variant, int flags,
+                const double* phi, const double* pts, int npts, const double* times, int ntimes, double* u,
+                void* stream) {
+    if (!m || !phi || !pts || !times || !u || npts < 1 || ntimes < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
+    if (int rc = check_problem(p)) return rc;
+    if (int rc = check_rules(3, n_sub, n_sing, 0)) return rc;
+    if (variant != EBEM_PP_POINT && variant != EBEM_PP_LAYER)
+        return fail(EBEM_ERR_INVALID, "variant must be EBEM_PP_POINT or EBEM_PP_LAYER");
+    if (is_device_ptr(times)) return fail(EBEM_ERR_INVALID, "times must be a host array");
+    // the sums read density column ceil(t / dt) (BEMenerg_postProcGPU_calcSP.m:85), which exists for t <= tfin
+    for (int q = 0; q < ntimes; q++)
+        if (!(times[q] <= p->tfin * (1 + 1e-12))) return fail(EBEM_ERR_INVALID, "evaluation time beyond tfin");
+    DeviceGuard dg(m->d.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    PhysParams P = phys_from(p);
+    DevIn dphi, dpts;
+    if (int rc = dphi.init(phi, 3 * (size_t)m->d.nt * P.nT, s)) return rc;
+    if (int rc = dpts.init(pts, 3 * (size_t)npts, s)) return rc;
+    DevOut out;
+    if (int rc = out.init(u, 3 * (size_t)npts * ntimes, s)) return rc;
+    if (int rc = launch_pp_num(m->d, P, n_sub, n_sing, variant == EBEM_PP_LAYER, flags & EBEM_FIX_REFERENCE_DEFECTS,
+                               dphi.d, dpts.d, npts, times, ntimes, out.d, s))
+        return rc;
+    return out.finish(s);
+}
+
 int ebem_num_blocks_dir(const ebem_mesh* m, const ebem_problem* p, int* lv, int* lk) {
     int L = 0;
     if (int rc = ebem_num_blocks(m, p, &L)) return rc;

@@ -155,6 +155,12 @@ int lu_plan_solve(LuPlan* plan, double* db, int nrhs, cudaStream_t s);
 void lu_plan_destroy(LuPlan* plan);
 int launch_pp_sa(const MeshData& m, const PhysParams& P, const double* d_phi, const double* d_pts, int npts,
                  const double* h_times, int ntimes, double* d_u, cudaStream_t s);
+// Numerical post-processing (pp_num.cu): composite rule (n_sub, n_sing) per
+// triangle, kernelLayer's semantics when layer != 0, else kernelSP's (node
+// stride 3 unless fix); u (ntimes x npts x 3) fully written.
+int launch_pp_num(const MeshData& m, const PhysParams& P, int n_sub, int n_sing, int layer, int fix,
+                  const double* d_phi, const double* d_pts, int npts, const double* h_times, int ntimes, double* d_u,
+                  cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // direct formulation (direct.cu)

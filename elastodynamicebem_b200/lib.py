@@ -86,6 +86,8 @@ PROTOTYPES = {
                                       C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_longlong)]),
     "ebem_timemarch_sa_ex": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_int, C.c_void_p,
                                        C.POINTER(C.c_int), C.c_void_p]),
+    "ebem_pp_gpu": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                              C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "ebem_num_blocks_dir": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "ebem_assemble_k": (C.c_int, [C.c_void_p, C.POINTER(ProblemC)] + [C.c_int] * 7 + [C.c_void_p, C.c_int, C.c_void_p]),
     "ebem_assemble_v": (C.c_int, [C.c_void_p, C.POINTER(ProblemC)] + [C.c_int] * 6 + [C.c_void_p, C.c_void_p]),

@@ -361,6 +361,32 @@ int ebem_timemarch_sa_ex(const ebem_mesh* mesh, const ebem_problem* prob, int n_
 int ebem_pp_sa(const ebem_mesh* mesh, const ebem_problem* prob, const double* phi, const double* pts, int npts,
                const double* times, int ntimes, double* u, void* stream);
 
+/* Numerical post-processing of the indirect formulation, the reference's
+ * method "GPU yy z" (composite Gauss-Hammer rule of n_sub sub-triangles x
+ * n_sing nodes on every triangle, n_sub in {1,4,16,64}, n_sing in
+ * {1,3,7,12,19}; f/utility/setup/BEMenerg_setupPost.m:15-27), at npts points
+ * and ntimes times, arguments and output as ebem_pp_sa.  variant:
+ *   EBEM_PP_POINT  kernelSP (f/BEMenerg_indir/BEMenerg_postProc/
+ *                  BEMenerg_postProcGPU/CUDAkernels/kernelSP.cu:5-105 with the
+ *                  host sum of BEMenerg_postProcGPU_calcSP.m:78-85): entries
+ *                  kept when |sum| > 1e-14 before the division by 4 pi rho,
+ *                  u = sum_{k<nHat} (M_k - M_{k+1}) phi_k + M_nHat phi_nHat;
+ *                  replaces BEMenerg_postProcGPU_setupSP.m:1 (main.m:167).
+ *   EBEM_PP_LAYER  kernelLayer (.../CUDAkernels/kernelLayer.cu:5-175):
+ *                  entries below 1e-14 after the division zeroed,
+ *                  u = sum_{k<=nHat} M_k (phi_k - phi_{k-1});
+ *                  replaces BEMenerg_postProcGPU_setupLayer.m:1 (main.m:165).
+ * nHat = ceil(t / dt) - 1; u = 0 for t <= 0; times <= tfin.  flags:
+ * EBEM_FIX_REFERENCE_DEFECTS reads kernelSP's nodes with stride n_sing; by
+ * default it keeps the reference's stride 3 (kernelSP.cu:41), and rules where
+ * that read would pass the end of the node table (n_sing = 1, n_sub > 1) are
+ * refused with EBEM_ERR_INVALID. */
+#define EBEM_PP_POINT 0
+#define EBEM_PP_LAYER 1
+int ebem_pp_gpu(const ebem_mesh* mesh, const ebem_problem* prob, int n_sub, int n_sing, int variant, int flags,
+                const double* phi, const double* pts, int npts, const double* times, int ntimes, double* u,
+                void* stream);
+
 /* ------------------------------------------------------------------------
  * Direct formulation (f/BEMenerg_dir, f/BEMenerg_dirPP).
  * Rules: outer Gauss-Hammer n_gh in {3,7,12,19}; inner composite rule

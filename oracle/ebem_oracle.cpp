@@ -694,6 +694,84 @@ int or_assemble_ghc(const double* coords, int nv, const int* tris, int nt,
     return 0;
 }
 
+// The reference's numerical post-processing "GPU yy z" restated on the CPU:
+// kernelSP.cu:5-121 with the host sum of BEMenerg_postProcGPU_calcSP.m:21-85
+// (variant 0) and kernelLayer.cu:5-170 with BEMenerg_postProcGPU_calcLayer.m
+// (variant 1), per (point, time).  stride: node index stride*subregion + l
+// (kernelSP.cu:41 has 3; kernelLayer n_sing).  phi column-major 3N x nT;
+// u is 3 x npts x ntimes (column-major).
+int or_pp_gpu(const double* coords, int nv, const int* tris, int nt, double rho, double mu, double lambda, double dt,
+              int nT, const double* phi, const double* pts, int npts, const double* times, int ntimes, int nSub,
+              int nSing, int variant, int stride, double* u, int nthreads) {
+    std::vector<double> gcn(3 * (size_t)nSub * nSing), gcw(nSing);
+    if (or_gh(nSing, nSub, gcn.data(), gcw.data()) != 0) return -1;
+    if ((nSub - 1) * stride + nSing > nSub * nSing) return -2;
+    Mesh m = make_mesh(coords, nv, tris, nt);
+    Params p = make_params(rho, mu, lambda, dt, nT);
+    set_threads(nthreads);
+    const double c4 = 4 * PI * rho;
+    const size_t n3 = 3 * (size_t)nt;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (long long q = 0; q < (long long)npts * ntimes; q++) {
+        const int ix = (int)(q % npts), it = (int)(q / npts);
+        const double t = times[it];
+        const double* x = pts + 3 * ix;
+        double uu[3] = {0, 0, 0};
+        if (t > 0) {
+            int nHat = (int)std::ceil(t / dt) - 1;
+            const int numIst = nHat + 1;
+            // matrixTotal [3 numIst x 3N] (variant 0) or the per-instant blocks (variant 1)
+            std::vector<double> Mt((size_t)3 * numIst * n3, 0.0);
+            for (int k = 0; k < numIst; k++) {
+                volatile double kd = k * dt;
+                const double tau = t - kd;
+                for (int mm = 0; mm < nt; mm++) {
+                    double dv[3] = {x[0] - m.center[3 * mm], x[1] - m.center[3 * mm + 1], x[2] - m.center[3 * mm + 2]};
+                    double distMin = std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]) - m.maxL[mm];
+                    if (tau * p.velP < distMin) continue;
+                    double V[3][3]; m.vert(mm, V);
+                    double blk[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+                    for (int sub = 0; sub < nSub; sub++) for (int l = 0; l < nSing; l++) {
+                        const double* nd = &gcn[3 * (size_t)(stride * sub + l)];
+                        double y[3];
+                        for (int c = 0; c < 3; c++) y[c] = nd[0] * V[0][c] + nd[1] * V[1][c] + nd[2] * V[2][c];
+                        double pt[3] = {y[0] - x[0], y[1] - x[1], y[2] - x[2]};
+                        double pn = std::sqrt(pt[0] * pt[0] + pt[1] * pt[1] + pt[2] * pt[2]);
+                        double nu[3][3];
+                        nucleo(nu, pt, pn, tau, p.velP, p.velS);
+                        double wt = gcw[l] * m.area[mm];
+                        for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) blk[i][j] += wt * nu[i][j];
+                    }
+                    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) {
+                        double v;
+                        if (variant == 0) v = (std::fabs(blk[i][j]) > 1.0e-14) ? blk[i][j] / c4 : 0.0;
+                        else { v = blk[i][j] / c4; if (std::fabs(v) < 1.0e-14) v = 0.0; }
+                        Mt[(3 * (size_t)mm + j) * 3 * numIst + 3 * k + i] = v;     // row 3k+i, column 3mm+j
+                    }
+                }
+            }
+            auto M = [&](int k, int i, size_t col) { return Mt[col * 3 * numIst + 3 * k + i]; };
+            if (variant == 0) {
+                for (int k = 0; k < nHat; k++)
+                    for (size_t col = 0; col < n3; col++) {
+                        double d = phi[(size_t)k * n3 + col];
+                        for (int i = 0; i < 3; i++) uu[i] += (M(k, i, col) - M(k + 1, i, col)) * d;
+                    }
+                for (size_t col = 0; col < n3; col++)
+                    for (int i = 0; i < 3; i++) uu[i] += M(nHat, i, col) * phi[(size_t)nHat * n3 + col];
+            } else {
+                for (int k = 0; k < numIst; k++)
+                    for (size_t col = 0; col < n3; col++) {
+                        double d = phi[(size_t)k * n3 + col] - (k > 0 ? phi[(size_t)(k - 1) * n3 + col] : 0.0);
+                        for (int i = 0; i < 3; i++) uu[i] += M(k, i, col) * d;
+                    }
+            }
+        }
+        for (int a = 0; a < 3; a++) u[3 * (size_t)q + a] = uu[a];
+    }
+    return 0;
+}
+
 // Null-test census: number of non-null pair-lags over lags [0, L).
 long long or_count_nonnull(const double* coords, int nv, const int* tris, int nt,
                            double rho, double mu, double lambda, double dt, int nT, int L) {

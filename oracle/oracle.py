@@ -52,6 +52,7 @@ def lib(variant: str = "f64"):
         L.or_march_exact.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, _dp]
         L.or_pp_sa.argtypes = mesh_args + par + [_dp, _dp, C.c_int, _dp, C.c_int, _dp, C.c_int]
         L.or_assemble_ghc.argtypes = mesh_args + par + [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_int]
+        L.or_pp_gpu.argtypes = mesh_args + par + [_dp, _dp, C.c_int, _dp, C.c_int] + [C.c_int] * 4 + [_dp, C.c_int]
         L.or_count_nonnull.argtypes = mesh_args + par + [C.c_int]
         L.or_count_nonnull.restype = C.c_longlong
         L.or_field_integrals.argtypes = [_dp, C.c_int, _ip, C.c_int, C.c_double, C.c_double, C.c_int, _dp,
@@ -164,6 +165,24 @@ def pp_sa(mesh, prm, phi, points, times, nthreads: int = 0, variant: str = "f64"
     return u.reshape(len(tms), len(pts), 3).transpose(2, 1, 0).copy()
 
 
+def pp_gpu(mesh, prm, phi, points, times, n_sub: int, n_sing: int, variant: int, stride: int | None = None,
+           nthreads: int = 0):
+    """The reference's numerical post-processing restated (variant 0:
+    kernelSP with its host sum, node stride 3 unless given; 1: kernelLayer):
+    u (3, npts, ntimes)."""
+    if stride is None:
+        stride = 3 if variant == 0 else n_sing
+    phicm = np.ascontiguousarray(np.asarray(phi).T).ravel()
+    pts = np.ascontiguousarray(points, np.float64)
+    tms = np.ascontiguousarray(times, np.float64)
+    u = np.zeros(3 * len(pts) * len(tms))
+    rc = lib().or_pp_gpu(*_m(mesh), *_p(prm), phicm, pts, len(pts), tms, len(tms), n_sub, n_sing, variant, stride, u,
+                         nthreads)
+    if rc:
+        raise ValueError(f"invalid post-processing rule ({rc})")
+    return u.reshape(len(tms), len(pts), 3).transpose(2, 1, 0).copy()
+
+
 def assemble_ghc(mesh, prm, n_gh: int, n_sub: int, n_sing: int, lag0: int, nlag: int, nthreads: int = 0):
     n3 = 3 * mesh.numberTriangles
     E = np.zeros(n3 * n3 * nlag)
@@ -260,6 +279,68 @@ def ref_ghc(mesh, prm, n_gh: int, n_sub: int, n_sing: int, nlag: int):
         raise RuntimeError(f"reference kernelGHC launch failed ({rc})")
     n3 = 3 * N
     return E.reshape(nlag, n3, n3).transpose(0, 2, 1)
+
+
+def ref_pp_available() -> bool:
+    return all(os.path.exists(os.path.join(_HERE, "_ref", f)) for f in ("libref_sp.so", "libref_layer.so"))
+
+
+def _pp_inputs(mesh, prm, t, n_sub, n_sing):
+    N = mesh.numberTriangles
+    nhat = int(np.ceil(t / prm.dt)) - 1
+    diff = t - np.arange(nhat + 1) * prm.dt                       # diffTemp of calcSP.m:35 / calcLayer.m:33
+    nodes, w = gauss_hammer(n_sing, n_sub)
+    P = mesh.coordinates[mesh.triangles]
+    verts = np.ascontiguousarray(P.transpose(0, 2, 1).reshape(N, 9)).ravel()
+    return (N, nhat, np.ascontiguousarray(diff), np.ascontiguousarray(w), np.ascontiguousarray(nodes), verts,
+            np.ascontiguousarray(mesh.area), np.ascontiguousarray(mesh.center).ravel(),
+            np.ascontiguousarray(mesh.maxL))
+
+
+def ref_pp_sp(mesh, prm, phi, x, t: float, n_sub: int, n_sing: int):
+    """The reference's kernelSP (compiled from its source into oracle/_ref) for
+    one point x and time t, with the host sum of
+    BEMenerg_postProcGPU_calcSP.m:78-85 done here: (u (3,), kernel ms)."""
+    if t <= 0:
+        return np.zeros(3), 0.0
+    L = C.CDLL(os.path.join(_HERE, "_ref", "libref_sp.so"))
+    L.ref_sp.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp, C.c_int,
+                         C.c_int, _dp, _dp, _dp, _dp]
+    L.ref_last_kernel_ms.restype = C.c_float
+    N, nhat, diff, w, nodes, verts, area, ctr, maxl = _pp_inputs(mesh, prm, t, n_sub, n_sing)
+    numIst = nhat + 1
+    M = np.zeros(9 * numIst * N)
+    rc = L.ref_sp(M, N, numIst, prm.velP, prm.velS, 4 * np.pi * prm.rho, np.ascontiguousarray(x, np.float64), diff,
+                  w, nodes.ravel(), n_sub, n_sing, verts, area, ctr, maxl)
+    if rc:
+        raise RuntimeError(f"reference kernelSP launch failed ({rc})")
+    M = M.reshape(3 * N, 3 * numIst).T                             # [3 numIst x 3N]
+    u = np.zeros(3)
+    for k in range(nhat):
+        u += (M[3 * k:3 * k + 3] - M[3 * k + 3:3 * k + 6]) @ phi[:, k]
+    u += M[3 * nhat:3 * nhat + 3] @ phi[:, nhat]
+    return u, float(L.ref_last_kernel_ms())
+
+
+def ref_pp_layer(mesh, prm, phi, pts, t: float, n_sub: int, n_sing: int):
+    """The reference's kernelLayer (compiled from its source into oracle/_ref)
+    for all points at one time t: (u (3, npts), kernel ms)."""
+    pts = np.ascontiguousarray(pts, np.float64)
+    if t <= 0:
+        return np.zeros((3, len(pts))), 0.0
+    L = C.CDLL(os.path.join(_HERE, "_ref", "libref_layer.so"))
+    L.ref_layer.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp,
+                            C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
+    L.ref_last_kernel_ms.restype = C.c_float
+    N, nhat, diff, w, nodes, verts, area, ctr, maxl = _pp_inputs(mesh, prm, t, n_sub, n_sing)
+    numIst = nhat + 1
+    dens = np.ascontiguousarray(np.asarray(phi)[:, :numIst]).ravel()   # reshape(density(:,1:numIst)', ...)
+    u = np.zeros(3 * len(pts))
+    rc = L.ref_layer(u, N, len(pts), numIst, prm.velP, prm.velS, 4 * np.pi * prm.rho, pts.ravel(), diff, w,
+                     nodes.ravel(), n_sub, n_sing, verts, area, ctr, maxl, dens)
+    if rc:
+        raise RuntimeError(f"reference kernelLayer launch failed ({rc})")
+    return u.reshape(len(pts), 3).T.copy(), float(L.ref_last_kernel_ms())
 
 
 def ref_ghc_composite(mesh, prm, n_gh: int, n_sub: int, n_sing: int, nlag: int, max_threads: int = 1024):

@@ -140,6 +140,38 @@ def test_row_pp_sa(ebem, sphere):
     assert err <= 1e-10
 
 
+def test_row_pp_numerical(ebem, sphere):
+    """a17's numerical half: kernelLayer (many points at one time, the density
+    contraction in the kernel) and kernelSP (one point, its times) against
+    the reference's kernels on this GPU, rule 16 x 3 (main.m:135-141 "GPU 16 3")."""
+    w, dm, L = sphere
+    if not O.ref_pp_available():
+        pytest.skip("reference kernels not built")
+    phi, _ = ebem.timemarch_sa(dm, w.params, w.n_gh, w.datum)
+    ph = phi.cpu().numpy().T
+    pts = w.points[:64]
+    t = w.times[-1]
+    ours = dev_ms(lambda: ebem.pp_gpu(dm, w.params, phi, pts, [t], 16, 3, 1))
+    ul = ebem.pp_gpu(dm, w.params, phi, pts, [t], 16, 3, 1).cpu().numpy()[0].T
+    ulr, ref = O.ref_pp_layer(w.mesh, w.params, ph, pts, t, 16, 3)
+    err = rel(ul, ulr)
+    record("a17 numerical post-processing (kernelLayer)", f"sphere N={dm.N}, {len(pts)} points at t={t:g}", ours, ref,
+           "reference kernelLayer on this GPU", err)
+    assert err <= 1e-12
+    x, tms = w.points[5], w.times
+    ours = dev_ms(lambda: ebem.pp_gpu(dm, w.params, phi, x[None], tms, 16, 3, 0))
+    us = ebem.pp_gpu(dm, w.params, phi, x[None], tms, 16, 3, 0).cpu().numpy()[:, 0]
+    ref, urs = 0.0, []
+    for tt in tms:
+        uu, ms = O.ref_pp_sp(w.mesh, w.params, ph, x, tt, 16, 3)
+        urs.append(uu)
+        ref += ms
+    err = rel(us, np.stack(urs))
+    record("a17 numerical post-processing (kernelSP)", f"sphere N={dm.N}, 1 point x {len(tms)} times", ours, ref,
+           "reference kernelSP on this GPU, one launch per (x, t), host sums excluded", err)
+    assert err <= 1e-12
+
+
 def test_row_kernel_k(ebem, bar):
     m, prm, dm, (LV, LK) = bar
     if not O.ref_dir_available():
