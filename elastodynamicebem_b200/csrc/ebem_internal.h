@@ -95,6 +95,12 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
                        cudaStream_t s, int diag_only = 0, int mixed = 0, const int2* pairs = nullptr,
                        long long npairs = 0);
+// The same assembly in two passes (sa_level.cu): F(t_k) of every (pair,
+// level) into a workspace, then the second difference written column by
+// column.  Dense outputs only (no pair list, no diagonal-only mode).
+int launch_sa_levels(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
+                     double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count, int mixed,
+                     cudaStream_t s);
 // Allocation-free variant of the full assembly (device E, ld = 3N): mapped
 // nodes and the counter live in a static device array (sa_assemble.cu).
 int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, double* d_E,

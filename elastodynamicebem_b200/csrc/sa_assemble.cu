@@ -30,6 +30,9 @@
 #ifndef EBEM_SA_KERNEL
 #define EBEM_SA_KERNEL 0    // 0: warp per pair when 3 n_gh <= 32, 1: always thread per pair
 #endif
+#ifndef EBEM_SA_LEVELS
+#define EBEM_SA_LEVELS 1    // 1: dense assemblies run the two-pass level kernel of sa_level.cu
+#endif
 
 namespace ebem {
 
@@ -575,6 +578,8 @@ static int launch_warp(const SAArgs& A, long long NN, int device, cudaStream_t s
 int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
                        cudaStream_t s, int diag_only, int mixed, const int2* pairs, long long npairs) {
+    if (EBEM_SA_LEVELS && EBEM_SA_KERNEL == 0 && !diag_only && !pairs)
+        return launch_sa_levels(m, P, n_gh, lag0, nlag, src0, nsrc, d_E, ld, ld_lag, accumulate, d_count, mixed, s);
     SAArgs A;
     A.geo = m.d_geo;
     A.nodes = m.d_nodes;

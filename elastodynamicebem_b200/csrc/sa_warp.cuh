@@ -207,10 +207,34 @@ struct LaneChild {
     bool live;
 };
 
-// Decision phase of one child at one level: closed-form circle pieces and
-// lo-subtractions into A (child frame), whole-range pieces from the moments
-// (or flagged in need_mom when they are not computed yet), partial edge
-// pieces returned in pc[0..np).  Mirrors child_level_e piece by piece.
+// Level data of one projected outer node, shared by its three children: the
+// case (BEMenerg_coreSA_calcMatrixSubBlock.m:58-81), the in-plane front radii
+// and the radial weights of the circle-bounded pieces: wPc (P terms between
+// the S circle, or the projection, and the P circle), wPlo (minus the P terms
+// at the lower limit) and wSc (P&S terms of the S circle minus the origin).
+struct NodeLevel {
+    W4 wPc, wPlo, wSc;
+    double rhoP, rhoS;
+    int type;
+};
+
+EBEM_DI void node_level(NodeLevel& n, double zeta, double dMIN, const LevelCtx& L, const W4& w0) {
+    n.type = classify(zeta, L.RP, L.RS, dMIN, n.rhoP, n.rhoS);
+    if (n.type == T_NONE) return;
+    const bool isP = (n.type == T_P);
+    const double rhoSe = isP ? 0.0 : n.rhoS;
+    Rad VSe = radial_at(rhoSe, isP ? zeta : L.RS, zeta);
+    Rad VP = radial_at(n.rhoP, L.RP, zeta);
+    n.wPc = weigh(rad_sub(VP, VSe), true, L);
+    n.wPlo = neg(weigh(VSe, true, L));
+    if (n.type == T_SP_SP) n.wSc = wsub(weigh(VSe, false, L), w0);
+}
+
+// Decision phase of one child at one level from its node's level data:
+// closed-form circle pieces and lo-subtractions into A (child frame),
+// whole-range pieces flagged in full_mask (the caller applies the moments),
+// partial edge pieces returned in pc[0..np).  Mirrors child_level_e piece by
+// piece.
 #ifndef EBEM_NOINLINE_DECIDE
 #define EBEM_NOINLINE_DECIDE 0     // 1: one out-of-line copy of the decision phase
 #endif
@@ -219,24 +243,21 @@ static __device__ __noinline__
 #else
 EBEM_DI
 #endif
-void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const LaneChild& C, const LevelCtx& L,
-                          double rhoP, double rhoS, int type, const W4& w0, double amax) {
-    const ChildE& g = C.g;
+void child_decide_n(AccE& A, Piece pc[3], int& np, int& full_mask, const ChildE& g, double cg, double sgm, double zs,
+                    const NodeLevel& n, const W4& w0, double amax) {
+    const int type = n.type;
+    const double rhoP = n.rhoP, rhoS = n.rhoS;
     const bool isP = (type == T_P), spsp = (type == T_SP_SP);
-    const double zeta = C.zeta, zs = C.zeta * C.sigma;
     np = 0;
     full_mask = 0;                          // bit 0: full P piece, bit 1: full S piece
     double DeltaP = g.bm * g.bm - (g.a * g.a - rhoP * rhoP);
     double DeltaS = isP ? 0.0 : g.bm * g.bm - (g.a * g.a - rhoS * rhoS);
     const bool xP = DeltaP > 1.0e-6, xS = xP && DeltaS > 1.0e-6;
-    double rhoSe = isP ? 0.0 : rhoS;
-    Rad VSe = radial_at(rhoSe, isP ? zeta : L.RS, zeta);
-    Rad VP = radial_at(rhoP, L.RP, zeta);
-    W4 wPc = weigh(rad_sub(VP, VSe), true, L);
-    W4 wPlo = neg(weigh(VSe, true, L));
+    const W4& wPc = n.wPc;
+    const W4& wPlo = n.wPlo;
     const double smax = g.s0, smin = g.s1;
     const double th0 = 0.0, c0 = 1.0, sn0 = 0.0;
-    const double thg = g.gamma, cg = C.cg, sgm = C.sg;
+    const double thg = g.gamma;
     // S crossing data (used by the P pieces when the S front crosses, and by the S terms)
     double sS = 0.0, thAS = 0.0, cAS = 1.0, sAS = 0.0, thBS = 0.0, cBS = 1.0, sBS = 0.0;
     // a front whose radius reaches both edge ends covers the whole edge: both
@@ -286,7 +307,7 @@ void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const LaneChild
     }
     if (spsp) {
         // P&S terms, radial range [0, min(rhoS, R)]: V_S is VSe (not isP here)
-        W4 wSc = wsub(weigh(VSe, false, L), w0);
+        const W4& wSc = n.wSc;
         if (!xS) {
             add_circle(A, wSc, th0, c0, sn0, thg, cg, sgm, zs);
         } else {
@@ -300,6 +321,36 @@ void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const LaneChild
             }
         }
     }
+}
+
+// The same decision with the node's level data computed here (one child).
+EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const LaneChild& C, const LevelCtx& L,
+                          double rhoP, double rhoS, int type, const W4& w0, double amax) {
+    NodeLevel n;
+    n.type = type;
+    n.rhoP = rhoP;
+    n.rhoS = rhoS;
+    const bool isP = (type == T_P);
+    const double zeta = C.zeta;
+    const double rhoSe = isP ? 0.0 : rhoS;
+    Rad VSe = radial_at(rhoSe, isP ? zeta : L.RS, zeta);
+    Rad VP = radial_at(rhoP, L.RP, zeta);
+    n.wPc = weigh(rad_sub(VP, VSe), true, L);
+    n.wPlo = neg(weigh(VSe, true, L));
+    if (type == T_SP_SP) n.wSc = wsub(weigh(VSe, false, L), w0);
+    child_decide_n(A, pc, np, full_mask, C.g, C.cg, C.sg, C.zeta * C.sigma, n, w0, amax);
+}
+
+// A child is static from the level at which it lies inside the S front with
+// its whole edge (rho_S >= the distance to both edge ends, both fronts
+// crossing the edge line): its piece is then the full S piece alone, whose
+// value no longer depends on the level (fixed weights k5, k6, the origin
+// weights and the whole-edge moments), and it stays so at every later level.
+EBEM_DI bool child_static(const ChildE& g, const NodeLevel& n) {
+    if (n.type != T_SP_SP) return false;
+    const double DeltaP = g.bm * g.bm - (g.a * g.a - n.rhoP * n.rhoP);
+    const double DeltaS = g.bm * g.bm - (g.a * g.a - n.rhoS * n.rhoS);
+    return DeltaP > 1.0e-6 && DeltaS > 1.0e-6 && n.rhoS >= g.amax;
 }
 
 // Child frame -> plane frame (rotation by the direction of V1), times the
