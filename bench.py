@@ -39,14 +39,17 @@ UNIT = "pair-integrals/s"
 FLOPS_PER_PAIR_INTEGRAL = 19_232.0
 FLOPS_PER_PAIR_INTEGRAL_REF_SCHEDULE = 53_560.0
 
-# DRAM bytes (read + write) of the assembly kernel over the whole workload
-# written in place in one launch: ncu on the sphere N=320 case measured
-# 30.7 MB + 339.8 MB; the traffic is the N^2 L output (written in 24-byte
-# column pieces), so it is scaled to N=1280 by the output size, x16.
-NCU_TRAFFIC_PER_LAUNCH = (30.733056e6 + 339.811584e6) * 16
+# DRAM bytes (read + write) of the dominant kernel, the level pass of the
+# two-pass assembly (sa_assemble_warp_kernel storing F(t_k) of every pair and
+# level): ncu on the sphere N=320 case (2,478,740 pair-integrals, one launch)
+# measured 13.16 MB read + 131.14 MB written; the writes are the stored levels,
+# which grow with the pair-integrals, so a launch's traffic is scaled by the
+# pair-integrals it processes.
+NCU_LEVEL_PASS_BYTES_N320 = 13.158656e6 + 131.140096e6
+NCU_LEVEL_PASS_UNITS_N320 = 2_478_740
 
 
-KERNEL = "sa_assemble_warp_kernel"
+KERNEL = "sa_assemble_warp_kernel (level pass)"
 
 
 def log(*a):
@@ -224,7 +227,7 @@ def workload_config(w, L: int, pairs: int, world: int) -> dict:
     """The `config` object of both arms' JSON lines."""
     N, prm = w.mesh.numberTriangles, w.params
     out_gb = 9 * N * N * L * 8 / 1e9          # dense E_0..E_{L-1}, FP64
-    rel = "far larger than" if out_gb > 4 * 0.126 else "not larger than"
+    rel = "far larger than" if out_gb > 4 * 0.126 else ("larger than" if out_gb > 0.126 else "not larger than")
     return {"workload": f"sphere_icosphere{3 if N == 1280 else 2}_N{N}_L{L}_GH7", "N": N, "L": L, "n_gh": w.n_gh,
             "rho": prm.rho, "mu": prm.mu, "lambda": prm.lam, "dt": prm.dt, "nT": prm.nT,
             "pair_integrals_per_step": pairs, "parallelism": f"source-row panels x{world}",
@@ -338,6 +341,15 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    # per-pass device times of the library's own launches (CUDA events on the
+    # assembly stream), read after the timed steps
+    from elastodynamicebem_b200 import lib as _lib
+    import ctypes as _C
+    L_ = _lib.load()
+    prof_ms = (_C.c_double * 2)()
+    prof_n = (_C.c_longlong * 2)()
+    L_.ebem_profile_read(prof_ms, prof_n, 1)
+    L_.ebem_profile_enable(1)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
@@ -345,6 +357,8 @@ def main():
         step()
     ev1.record(stream)
     torch.cuda.synchronize()
+    L_.ebem_profile_enable(0)
+    L_.ebem_profile_read(prof_ms, prof_n, 1)
     if world > 1:
         dist.barrier()
     clocks = sampler.stop()
@@ -355,8 +369,12 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
     value = total_pairs * args.steps / t_max
-    launches = 1                        # a device output is assembled in place: one launch per step
-    kernel_s = my_s / (args.steps * launches)
+    # launches per step of the dominant kernel (the level pass, one per chunk
+    # of field columns) and its average launch time; the emission pass is the
+    # other launch of each chunk
+    launches = max(1, int(prof_n[0]) // args.steps)
+    kernel_s = prof_ms[0] / 1e3 / max(1, int(prof_n[0]))
+    emit_ms = prof_ms[1] / max(1, args.steps)
 
     # end to end through the C ABI with host buffers: mesh upload, assembly,
     # copy of E to pinned host memory, every step
@@ -403,14 +421,15 @@ def main():
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(w, L, total_pairs, world),
-            "gpu_launches": args.steps * launches,
+            "gpu_launches": int(prof_n[0] + prof_n[1]),
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
-                         "traffic": NCU_TRAFFIC_PER_LAUNCH / launches,
+                         "traffic": NCU_LEVEL_PASS_BYTES_N320 * (my_pairs / launches) / NCU_LEVEL_PASS_UNITS_N320,
                          "peak_source": "measured: cuBLAS DGEMM 8192^3 via torch.matmul float64, best of 5",
                          "flops_per_unit": FLOPS_PER_PAIR_INTEGRAL,
                          "units_per_launch": my_pairs / launches, "launches_per_step": launches,
-                         "kernel": KERNEL, "kernel_ms": kernel_s * 1e3},
+                         "kernel": KERNEL, "kernel_ms": kernel_s * 1e3,
+                         "emission_ms_per_step": emit_ms},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "path": "ebem_mesh_create + ebem_assemble_sa_panel into pinned host memory + ebem_mesh_destroy",
                     "host_link_d2h_gbs": link_gbs,

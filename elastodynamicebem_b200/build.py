@@ -15,7 +15,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libebem.so")
 
-SOURCES = ["capi.cu", "quadrature.cu", "sa_assemble.cu", "march.cu", "ghc.cu", "direct.cu", "selector.cu", "banded.cu", "pp_num.cu", "sa_level.cu"]
+SOURCES = ["capi.cu", "quadrature.cu", "sa_assemble.cu", "march.cu", "ghc.cu", "direct.cu", "selector.cu", "banded.cu", "pp_num.cu", "sa_twopass.cu"]
 HEADERS = ["sa_device.cuh", "sa_edge.cuh", "sa_pair.cuh", "sa_warp.cuh", "ebem_internal.h", "ptr_kind.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

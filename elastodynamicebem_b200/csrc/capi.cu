@@ -287,6 +287,17 @@ int ebem_workspace_info(int device, unsigned long long* reserved, unsigned long 
     return EBEM_OK;
 }
 
+int ebem_profile_enable(int on) {
+    profile_enable(on);
+    return EBEM_OK;
+}
+
+int ebem_profile_read(double* ms, long long* launches, int reset) {
+    if (!ms || !launches) return fail(EBEM_ERR_INVALID, "NULL output");
+    profile_read(ms, launches, reset);
+    return EBEM_OK;
+}
+
 int ebem_device_release(int device) {
     if (device < 0 || device >= kMaxDevices) return fail(EBEM_ERR_INVALID, "device ordinal out of range");
     // first: every cached handle and address of this device becomes stale

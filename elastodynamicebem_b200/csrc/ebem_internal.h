@@ -95,12 +95,20 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
                        cudaStream_t s, int diag_only = 0, int mixed = 0, const int2* pairs = nullptr,
                        long long npairs = 0);
-// The same assembly in two passes (sa_level.cu): F(t_k) of every (pair,
+// The same assembly in two passes (sa_twopass.cu): F(t_k) of every (pair,
 // level) into a workspace, then the second difference written column by
 // column.  Dense outputs only (no pair list, no diagonal-only mode).
-int launch_sa_levels(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
+int launch_sa_twopass(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                      double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count, int mixed,
                      cudaStream_t s);
+// Per-pass device times of the two-pass assembly (ebem_profile_enable / _read).
+void profile_enable(int on);
+void profile_read(double ms[2], long long n[2], int reset);
+// Pass 1 of that assembly by the one-warp-per-pair kernel (sa_assemble.cu):
+// F(t_k) and the non-null lags of the pairs of field columns [j0, j0 + nj).
+int launch_sa_fwarp(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc, int j0,
+                    int nj, int kbase, int KL, double* d_F, int2* d_band, unsigned long long* d_count, int mixed,
+                    cudaStream_t s);
 // Allocation-free variant of the full assembly (device E, ld = 3N): mapped
 // nodes and the counter live in a static device array (sa_assemble.cu).
 int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, double* d_E,

@@ -30,8 +30,8 @@
 #ifndef EBEM_SA_KERNEL
 #define EBEM_SA_KERNEL 0    // 0: warp per pair when 3 n_gh <= 32, 1: always thread per pair
 #endif
-#ifndef EBEM_SA_LEVELS
-#define EBEM_SA_LEVELS 1    // 1: dense assemblies run the two-pass level kernel of sa_level.cu
+#ifndef EBEM_SA_TWOPASS
+#define EBEM_SA_TWOPASS 1   // 1: dense assemblies store F(t_k) and emit the blocks in a second pass (sa_twopass.cu)
 #endif
 
 namespace ebem {
@@ -149,6 +149,12 @@ struct SAArgs {
     double* Eb = nullptr;
     const long long* boff = nullptr;
     const int* blo = nullptr;
+    // level output (instead of E): field columns [j0, j0 + nj) of the panel;
+    // F(t_k) of pair (i, j) at Fout[(((j - j0) KL + k - kbase) nsrc + i - src0) 6 + e]
+    // for every level it needs, its non-null lags (llo, lhi) at band[(j - j0) nsrc + i - src0]
+    double* Fout = nullptr;
+    int2* band = nullptr;
+    int j0 = 0, nj = 0, kbase = 0, KL = 0;
 };
 
 __device__ __forceinline__ void store_block(const SAArgs& A, int q, int i, int j, const double b[6]) {
@@ -255,7 +261,8 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
         pair_band(F, Sg, A.velP, A.velS, A.dt, A.lag0, A.nlag, &llo, &lhi);
     }
     if (lane == 0 && llo >= 0) my_count += (unsigned long long)(lhi - llo + 1);
-    if (!A.accumulate && !A.Eb) {
+    if (A.Fout && lane == 0) A.band[(long long)(j - A.j0) * A.nsrc + (i - A.src0)] = make_int2(llo, lhi);
+    if (!A.accumulate && !A.Eb && !A.Fout) {
         for (int idx = lane; idx < A.nlag * 9; idx += 32) {
             const int q = idx / 9, e = idx - 9 * q, l = A.lag0 + q;
             if (llo < 0 || l < llo || l > lhi) store_entry(A, q, i, j, e, 0.0);
@@ -498,7 +505,10 @@ __device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W,
             Fk[5] = 0.5 * (S + Rm[2][2]);
         }
         const int l = k - 1;
-        if (A.Eb) {
+        if (A.Fout) {
+            if (lane < 6)
+                A.Fout[(((long long)(j - A.j0) * A.KL + (k - A.kbase)) * A.nsrc + (i - A.src0)) * 6 + lane] = Fk[lane];
+        } else if (A.Eb) {
             if (l >= llo && l <= lhi && lane < 6) {
                 double prev = (l - 1 >= 1) ? Fm2[lane] : 0.0;
                 double v = ((Fk[lane] + (-2.0) * Fm1[lane]) + prev) / A.c4pirho;
@@ -540,7 +550,9 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs
     }
     if (threadIdx.x == 0) blk_count = 0;
     __syncthreads();
-    const long long NP = A.pairs ? A.npairs : A.diag_only ? (long long)A.nsrc : (long long)A.nsrc * A.N;
+    const long long NP = A.pairs      ? A.npairs
+                         : A.diag_only ? (long long)A.nsrc
+                                       : (long long)A.nsrc * (A.Fout ? A.nj : A.N);
     const long long nwarps = (long long)gridDim.x * WPB;
     unsigned long long my_count = 0;
     for (long long p = (long long)blockIdx.x * WPB + wib; p < NP; p += nwarps) {
@@ -551,7 +563,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs
             j = pj.y;
         } else {
             i = A.src0 + (int)(p % A.nsrc);
-            j = A.diag_only ? i : (int)(p / A.nsrc);
+            j = A.diag_only ? i : A.j0 + (int)(p / A.nsrc);
         }
         assemble_pair<R, MIXED>(A, W, glx, glw, i, j, lane, my_count);
     }
@@ -578,8 +590,8 @@ static int launch_warp(const SAArgs& A, long long NN, int device, cudaStream_t s
 int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
                        cudaStream_t s, int diag_only, int mixed, const int2* pairs, long long npairs) {
-    if (EBEM_SA_LEVELS && EBEM_SA_KERNEL == 0 && !diag_only && !pairs)
-        return launch_sa_levels(m, P, n_gh, lag0, nlag, src0, nsrc, d_E, ld, ld_lag, accumulate, d_count, mixed, s);
+    if (EBEM_SA_TWOPASS && EBEM_SA_KERNEL == 0 && 3 * n_gh <= 64 && !diag_only && !pairs)
+        return launch_sa_twopass(m, P, n_gh, lag0, nlag, src0, nsrc, d_E, ld, ld_lag, accumulate, d_count, mixed, s);
     SAArgs A;
     A.geo = m.d_geo;
     A.nodes = m.d_nodes;
@@ -615,6 +627,49 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
     sa_assemble_kernel<<<(unsigned)blocks, threads, 0, s>>>(A);
     EBEM_CUDA_TRY(cudaGetLastError());
     return EBEM_OK;
+}
+
+// Level output for the two-pass assembly (sa_twopass.cu): F(t_k) of the pairs
+// (sources [src0, src0 + nsrc), fields [j0, j0 + nj)) at every level their
+// non-null lags in [lag0, lag0 + nlag) need, and those lags.
+int launch_sa_fwarp(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc, int j0,
+                    int nj, int kbase, int KL, double* d_F, int2* d_band, unsigned long long* d_count, int mixed,
+                    cudaStream_t s) {
+    SAArgs A;
+    A.geo = m.d_geo;
+    A.nodes = m.d_nodes;
+    A.N = m.nt;
+    A.n_gh = n_gh;
+    A.velP = P.velP;
+    A.velS = P.velS;
+    A.dt = P.dt;
+    A.c4pirho = 4 * kPi * P.rho;
+    A.lag0 = lag0;
+    A.nlag = nlag;
+    A.src0 = src0;
+    A.nsrc = nsrc;
+    A.diag_only = 0;
+    A.E = nullptr;
+    A.ld = 0;
+    A.ld_lag = 0;
+    A.accumulate = 0;
+    A.count = d_count;
+    A.pairs = nullptr;
+    A.npairs = 0;
+    A.Fout = d_F;
+    A.band = d_band;
+    A.j0 = j0;
+    A.nj = nj;
+    A.kbase = kbase;
+    A.KL = KL;
+    const long long NN = (long long)nsrc * nj;
+    if (3 * n_gh <= 32)
+        return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
+                     : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
+    if (3 * n_gh <= 64)
+        return mixed ? launch_warp<2, 2, EBEM_WARP2_MINB, true>(A, NN, m.device, s)
+                     : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
+    return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
 }
 
 // Banded output: all lags [0, L) of every pair, written into the band

@@ -218,18 +218,6 @@ struct NodeLevel {
     int type;
 };
 
-EBEM_DI void node_level(NodeLevel& n, double zeta, double dMIN, const LevelCtx& L, const W4& w0) {
-    n.type = classify(zeta, L.RP, L.RS, dMIN, n.rhoP, n.rhoS);
-    if (n.type == T_NONE) return;
-    const bool isP = (n.type == T_P);
-    const double rhoSe = isP ? 0.0 : n.rhoS;
-    Rad VSe = radial_at(rhoSe, isP ? zeta : L.RS, zeta);
-    Rad VP = radial_at(n.rhoP, L.RP, zeta);
-    n.wPc = weigh(rad_sub(VP, VSe), true, L);
-    n.wPlo = neg(weigh(VSe, true, L));
-    if (n.type == T_SP_SP) n.wSc = wsub(weigh(VSe, false, L), w0);
-}
-
 // Decision phase of one child at one level from its node's level data:
 // closed-form circle pieces and lo-subtractions into A (child frame),
 // whole-range pieces flagged in full_mask (the caller applies the moments),
@@ -339,18 +327,6 @@ EBEM_DI void child_decide(AccE& A, Piece pc[3], int& np, int& full_mask, const L
     n.wPlo = neg(weigh(VSe, true, L));
     if (type == T_SP_SP) n.wSc = wsub(weigh(VSe, false, L), w0);
     child_decide_n(A, pc, np, full_mask, C.g, C.cg, C.sg, C.zeta * C.sigma, n, w0, amax);
-}
-
-// A child is static from the level at which it lies inside the S front with
-// its whole edge (rho_S >= the distance to both edge ends, both fronts
-// crossing the edge line): its piece is then the full S piece alone, whose
-// value no longer depends on the level (fixed weights k5, k6, the origin
-// weights and the whole-edge moments), and it stays so at every later level.
-EBEM_DI bool child_static(const ChildE& g, const NodeLevel& n) {
-    if (n.type != T_SP_SP) return false;
-    const double DeltaP = g.bm * g.bm - (g.a * g.a - n.rhoP * n.rhoP);
-    const double DeltaS = g.bm * g.bm - (g.a * g.a - n.rhoS * n.rhoS);
-    return DeltaP > 1.0e-6 && DeltaS > 1.0e-6 && n.rhoS >= g.amax;
 }
 
 // Child frame -> plane frame (rotation by the direction of V1), times the

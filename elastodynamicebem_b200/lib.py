@@ -32,6 +32,8 @@ PROTOTYPES = {
     "ebem_release_workspace": (C.c_int, []),
     "ebem_workspace_info": (C.c_int, [C.c_int, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
     "ebem_device_release": (C.c_int, [C.c_int]),
+    "ebem_profile_enable": (C.c_int, [C.c_int]),
+    "ebem_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "ebem_mesh_cache_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
     "ebem_quad_gh": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ebem_mesh_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),

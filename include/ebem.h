@@ -76,6 +76,18 @@ int ebem_release_workspace(void);
  * reference. */
 int ebem_workspace_info(int device, unsigned long long* reserved, unsigned long long* used);
 
+/* Device-time profile of the semi-analytic assembly of dense outputs, which
+ * runs in two passes (per chunk of field columns: the level kernel that stores
+ * F(t_k) of every pair and level, then the emission kernel that writes the
+ * blocks).  While enabled, each such call records CUDA events around its
+ * launches on its stream and waits for them at its end; ebem_profile_read
+ * returns the summed milliseconds and launch counts of both passes since the
+ * last reset (ms[0], launches[0]: levels; ms[1], launches[1]: emission) and
+ * resets them when reset != 0.  No counterpart in the reference (it has no
+ * timing code). */
+int ebem_profile_enable(int on);
+int ebem_profile_read(double* ms, long long* launches, int reset);
+
 /* Release everything the library keeps for `device` between calls, before
  * its CUDA context is reset (cudaDeviceReset, or the reset(gpuDevice) that
  * f/BEMenerg_indir/BEMenerg_core/BEMenerg_coreGPU/BEMenerg_coreGPU_timeMarching.m:7,170

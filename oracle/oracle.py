@@ -343,11 +343,12 @@ def ref_pp_layer(mesh, prm, phi, pts, t: float, n_sub: int, n_sing: int):
     return u.reshape(len(pts), 3).T.copy(), float(L.ref_last_kernel_ms())
 
 
-def ref_ghc_composite(mesh, prm, n_gh: int, n_sub: int, n_sing: int, nlag: int, max_threads: int = 1024):
+def ref_ghc_composite(mesh, prm, n_gh: int, n_sub: int, n_sing: int, nlag: int, max_threads: int = 256):
     """The reference's kernelGHC with an inner composite rule of any size.
 
     The kernel runs one thread per inner node in a block of (n_sub, n_sing)
-    threads, so a single launch is limited to n_sub * n_sing <= 1024.  The
+    threads with 72 bytes of shared memory each, so a launch holds a few
+    hundred nodes at most (registers and the 48 KB shared-memory default).  The
     composite rule is a sum over its sub-triangles, so a larger rule is run as
     consecutive launches over chunks of its sub-triangles (nodes sub * n_sing
     + sing, GaussHammerComposite.m's order) with the full rule's weights; the

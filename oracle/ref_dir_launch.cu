@@ -97,7 +97,8 @@ extern "C" int ref_k(double* matrix, int N, int Nv, int nlag, double deltaT, dou
                                                                 ccx, ccy, ccz, v, a, nr, ism, mc, vc, offsetZ,
                                                                 numBlocks, nm3, maxLen);
     timer.stop();
-    cudaError_t e = cudaDeviceSynchronize();
+    cudaError_t e = cudaGetLastError();               // a launch the block shape does not allow fails here
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(matrix, d_m, nm * sizeof(double), cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? 0 : -2;
 }
@@ -127,7 +128,8 @@ extern "C" int ref_g(double* matrix, int N, int nHat, double velP, double velS, 
     kernelPPNEWG<<<grid, block, nSub * 9 * sizeof(double)>>>(d_m, velP, velS, 4 * 3.141592653589793 * rho, sp, dtm, w,
                                                              x, y, z, nSing, v, a, c, ml);
     timer.stop();
-    cudaError_t e = cudaDeviceSynchronize();
+    cudaError_t e = cudaGetLastError();               // a launch the block shape does not allow fails here
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(matrix, d_m, nm * sizeof(double), cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? 0 : -2;
 }
@@ -157,7 +159,8 @@ extern "C" int ref_p(double* matrix, int N, int Nv, int nHat, double velP, doubl
                                                              4 * 3.141592653589793 * rho * deltaT, (double)N, sp, dtm,
                                                              w, x, y, z, nSing, v, a, nr, ism, mc, vc);
     timer.stop();
-    cudaError_t e = cudaDeviceSynchronize();
+    cudaError_t e = cudaGetLastError();               // a launch the block shape does not allow fails here
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(matrix, d_m, nm * sizeof(double), cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? 0 : -2;
 }

@@ -48,7 +48,8 @@ extern "C" int ref_ghc(double* matrix_host, int N, int nlag, double deltaT, doub
                                                                   d_z, nGH, d_cw, d_cx, d_cy, d_cz, d_v, d_a,
                                                                   offsetZ, numBlocks);
     cudaEventRecord(e1);
-    cudaError_t e = cudaDeviceSynchronize();
+    cudaError_t e = cudaGetLastError();               // a launch the block shape does not allow fails here
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     cudaEventElapsedTime(&g_last_ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -65,7 +65,8 @@ extern "C" int ref_sp(double* matrix_host /* 9 numIst N, column-major [3 numIst 
     kernelPP<<<dim3(N, numIst), dim3(nSub), nSub * 9 * sizeof(double)>>>(dm, velP, velS, const4PiRho, dx, dt, dw, dnx,
                                                                           dny, dnz, nSing, dv, da, dc, dl);
     cudaEventRecord(e1);
-    cudaError_t e = cudaDeviceSynchronize();
+    cudaError_t e = cudaGetLastError();               // a launch the block shape does not allow fails here
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     cudaEventElapsedTime(&g_last_ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -98,7 +99,8 @@ extern "C" int ref_layer(double* u_host /* 3 npts */, int N, int npts, int numIs
     kernelPP<<<dim3(npts), dim3(numIst), numIst * 3 * sizeof(double)>>>(du, velP, velS, const4PiRho, dp, dt, N, nSub,
                                                                         nSing, dw, dnx, dny, dnz, dv, da, dc, dl, dd);
     cudaEventRecord(e1);
-    cudaError_t e = cudaDeviceSynchronize();
+    cudaError_t e = cudaGetLastError();               // a launch the block shape does not allow fails here
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     cudaEventElapsedTime(&g_last_ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -44,8 +44,11 @@ def test_gpu_method_diagonal_is_sa(ebem):
     E = ebem.assemble_ghc(dm, prm, 7, 16, 3, 0, L, sa_diagonal=True).cpu().numpy()
     S = ebem.assemble_sa(dm, prm, 7, 0, L).cpu().numpy()
     N = m.numberTriangles
+    # the diagonal blocks come from the diagonal-only semi-analytic kernel:
+    # equal to the full assembly's to rounding (the same terms in another order)
     for i in range(N):
-        assert np.array_equal(E[:, 3 * i:3 * i + 3, 3 * i:3 * i + 3], S[:, 3 * i:3 * i + 3, 3 * i:3 * i + 3])
+        d, s = E[:, 3 * i:3 * i + 3, 3 * i:3 * i + 3], S[:, 3 * i:3 * i + 3, 3 * i:3 * i + 3]
+        assert np.abs(d - s).max() <= 1e-14 * np.abs(s).max()
     # off-diagonal numerical blocks approach the semi-analytic ones as the inner rule refines
     mask = np.ones((3 * N, 3 * N), bool)
     for i in range(N):

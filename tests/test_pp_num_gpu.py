@@ -23,8 +23,11 @@ TOL = 1e-12
 
 
 def rel(a, b):
+    """Relative Frobenius difference; the absolute one where b is zero (before
+    the P front reaches any point both are exactly zero)."""
     a, b = np.asarray(a), np.asarray(b)
-    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / nb) if nb > 0 else float(np.linalg.norm(a))
 
 
 @pytest.fixture(scope="module")
