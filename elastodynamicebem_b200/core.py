@@ -148,16 +148,21 @@ def rhs(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, datum: int, out: torch
     return out
 
 
-def march(E: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None, stream=None):
+FACTOR_LU = 0
+FACTOR_CHOLESKY = 1
+
+
+def march(E: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None, stream=None, factor: int = FACTOR_LU):
     """Density phi (nT, 3N) from the blocks E (L, 3N, 3N storage of
-    assemble_sa, i.e. E[l] transposed view) and the right-hand side b (nT, 3N)."""
+    assemble_sa, i.e. E[l] transposed view) and the right-hand side b (nT, 3N);
+    E_0 factored by LU (the reference's) or Cholesky of its symmetric part."""
     Eraw = E.transpose(1, 2).contiguous()      # column-major blocks of the C ABI (no copy for assemble_sa's view)
     L, n3 = Eraw.shape[0], Eraw.shape[1]
     nT = b.shape[0]
     if out is None:
         out = torch.empty((nT, n3), dtype=torch.float64, device=b.device)
-    _lib.check(_lib.load().ebem_march(_ptr(Eraw), int(n3), int(L), _ptr(b.contiguous()), int(nT), _ptr(out),
-                                      _stream_ptr(stream) if out.is_cuda else None))
+    _lib.check(_lib.load().ebem_march_ex(_ptr(Eraw), int(n3), int(L), _ptr(b.contiguous()), int(nT), _ptr(out),
+                                         int(factor), _stream_ptr(stream) if out.is_cuda else None))
     return out
 
 

@@ -654,6 +654,21 @@ int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double
     return out.finish(s);
 }
 
+int ebem_march_ex(const double* E, int n3, int L, const double* rhs, int nT, double* phi, int factor, void* stream) {
+    if (!E || !rhs || !phi || n3 < 1 || L < 1 || nT < 1) return fail(EBEM_ERR_INVALID, "bad arguments");
+    if (factor != EBEM_FACTOR_LU && factor != EBEM_FACTOR_CHOLESKY)
+        return fail(EBEM_ERR_INVALID, "factor must be EBEM_FACTOR_LU or EBEM_FACTOR_CHOLESKY");
+    if (int rc = check_device()) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevIn dE, dr;
+    if (int rc = dE.init(E, (size_t)n3 * n3 * L, s)) return rc;
+    if (int rc = dr.init(rhs, (size_t)n3 * nT, s)) return rc;
+    DevOut out;
+    if (int rc = out.init(phi, (size_t)n3 * nT, s)) return rc;
+    if (int rc = march_device(dE.d, n3, L, dr.d, nT, out.d, s, factor)) return rc;
+    return out.finish(s);
+}
+
 struct ebem_banded {
     BandOp op;
     int device = 0;

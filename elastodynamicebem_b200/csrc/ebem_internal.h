@@ -131,7 +131,10 @@ int launch_ghc_assemble(const MeshData& m, const PhysParams& P, int n_gh, int n_
                         double* d_E, size_t ld, size_t ld_lag, cudaStream_t s);
 
 int launch_rhs(const MeshData& m, const PhysParams& P, int n_gh, int datum, double* d_rhs, cudaStream_t s);
-int march_device(const double* dE, int n3, int L, const double* drhs, int nT, double* dphi, cudaStream_t s);
+// factor: EBEM_FACTOR_LU (partial pivoting, the reference's lu) or
+// EBEM_FACTOR_CHOLESKY (of the symmetric part (E_0 + E_0^T) / 2).
+int march_device(const double* dE, int n3, int L, const double* drhs, int nT, double* dphi, cudaStream_t s,
+                 int factor = EBEM_FACTOR_LU);
 // A square system solved many times: A^{-1} formed once from the LU factors
 // (partial pivoting), so that each solve is one matrix-vector (or matrix)
 // product instead of a row-interchange pass and two triangular solves, which
@@ -164,7 +167,7 @@ int band_to_dense(const BandOp& op, int lag0, int nlag, double* d_E, cudaStream_
 int band_march(const BandOp& op, const double* d_rhs, int nT, double* d_phi, cudaStream_t s);
 int launch_sa_assemble_banded(const MeshData& m, const PhysParams& P, int n_gh, int L, double* d_Eb,
                               const long long* d_boff, const int* d_blo, int mixed, cudaStream_t s);
-int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan, bool pooled = false);
+int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan, bool pooled = false, bool cholesky = false);
 int lu_plan_solve(LuPlan* plan, double* db, int nrhs, cudaStream_t s);
 void lu_plan_destroy(LuPlan* plan);
 int launch_pp_sa(const MeshData& m, const PhysParams& P, const double* d_phi, const double* d_pts, int npts,

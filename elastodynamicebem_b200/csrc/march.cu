@@ -393,7 +393,8 @@ void release_thread_handles(int dev) {
 // phi (device, column-major n3 x nT) from E (device, n3 x n3 x L) and rhs
 // (device, n3 x nT): E_0^{-1} once, then per step the history product and
 // one product with E_0^{-1}.
-int march_device(const double* dE, int n3, int L, const double* drhs, int nT, double* dphi, cudaStream_t s) {
+int march_device(const double* dE, int n3, int L, const double* drhs, int nT, double* dphi, cudaStream_t s,
+                 int factor) {
     int rc = EBEM_OK, dev = 0, sms = 148;
     double* rev = nullptr;
     LuPlan lu;
@@ -402,7 +403,7 @@ int march_device(const double* dE, int n3, int L, const double* drhs, int nT, do
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (ws_malloc(&rev, (size_t)n3 * nT * sizeof(double), s) != cudaSuccess)
         return fail(EBEM_ERR_NOMEM, "time-marching workspace allocation failed");
-    rc = lu_plan_create(dE, n3, s, &lu, true);
+    rc = lu_plan_create(dE, n3, s, &lu, true, factor == EBEM_FACTOR_CHOLESKY);
     if (!rc) {
         // density in reversed time order: phi_n at column nT-1-n, so that
         // phi_{n-1}, phi_{n-2}, ... are contiguous for the history product
@@ -436,7 +437,17 @@ __global__ void set_identity_kernel(double* __restrict__ a, int n) {
     if (i < n) a[(size_t)i * n + i] = 1.0;
 }
 
-int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan, bool pooled) {
+// (A + A^T) / 2 in place (column-major n x n).
+__global__ void symmetrize_kernel(double* __restrict__ a, int n) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(idx % n), j = (int)(idx / n);
+    if (idx >= (long long)n * n || i >= j) return;
+    const double v = 0.5 * (a[(size_t)j * n + i] + a[(size_t)i * n + j]);
+    a[(size_t)j * n + i] = v;
+    a[(size_t)i * n + j] = v;
+}
+
+int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan, bool pooled, bool cholesky) {
     int rc = EBEM_OK;
     int lwork = 0, hinfo = 0;
     double *lu = nullptr, *work = nullptr;
@@ -462,19 +473,27 @@ int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan, bool p
         rc = fail(EBEM_ERR_CUDA, "matrix copy failed");
         goto done;
     }
-    CUSOLVER_TRY(cusolverDnDgetrf_bufferSize(h, n, n, lu, n, &lwork));
+    if (cholesky) {
+        symmetrize_kernel<<<(unsigned)(((long long)n * n + 255) / 256), 256, 0, s>>>(lu, n);
+        CUSOLVER_TRY(cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, n, lu, n, &lwork));
+    } else {
+        CUSOLVER_TRY(cusolverDnDgetrf_bufferSize(h, n, n, lu, n, &lwork));
+    }
     if (ws_malloc(&work, (size_t)(lwork > 0 ? lwork : 1) * sizeof(double), s) != cudaSuccess) {
         rc = fail(EBEM_ERR_NOMEM, "LU workspace allocation failed");
         goto done;
     }
-    CUSOLVER_TRY(cusolverDnDgetrf(h, n, n, lu, n, work, ipiv, info));
+    if (cholesky) CUSOLVER_TRY(cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, n, lu, n, work, lwork, info));
+    else CUSOLVER_TRY(cusolverDnDgetrf(h, n, n, lu, n, work, ipiv, info));
     if (cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) {
         rc = fail(EBEM_ERR_CUDA, "LU factorisation failed");
         goto done;
     }
     if (hinfo != 0) {
-        rc = fail(EBEM_ERR_SINGULAR, "matrix is singular (zero pivot " + std::to_string(hinfo) + ")");
+        rc = cholesky ? fail(EBEM_ERR_SINGULAR, "the symmetric part of the matrix is not positive definite (leading "
+                                                "minor " + std::to_string(hinfo) + ")")
+                      : fail(EBEM_ERR_SINGULAR, "matrix is singular (zero pivot " + std::to_string(hinfo) + ")");
         goto done;
     }
     if (cudaMemsetAsync(plan->inv, 0, nn * sizeof(double), s) != cudaSuccess) {
@@ -486,7 +505,8 @@ int lu_plan_create(const double* dA, int n, cudaStream_t s, LuPlan* plan, bool p
         rc = fail(EBEM_ERR_CUDA, "inverse initialisation failed");
         goto done;
     }
-    CUSOLVER_TRY(cusolverDnDgetrs(h, CUBLAS_OP_N, n, n, lu, n, ipiv, plan->inv, n, info));
+    if (cholesky) CUSOLVER_TRY(cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, n, n, lu, n, plan->inv, n, info));
+    else CUSOLVER_TRY(cusolverDnDgetrs(h, CUBLAS_OP_N, n, n, lu, n, ipiv, plan->inv, n, info));
 done:
     ws_free(lu, s);
     ws_free(work, s);

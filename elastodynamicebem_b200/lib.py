@@ -50,6 +50,7 @@ PROTOTYPES = {
                                     C.c_void_p, C.c_int, C.c_void_p]),
     "ebem_rhs": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "ebem_march": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "ebem_march_ex": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "ebem_banded_assemble": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_void_p,
                                        C.POINTER(C.c_void_p)]),
     "ebem_banded_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong),

@@ -294,6 +294,17 @@ int ebem_rhs(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int datu
  * Returns EBEM_ERR_SINGULAR when E_0 has a zero pivot. */
 int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double* phi, void* stream);
 
+/* ebem_march with a choice of factorisation of E_0.  EBEM_FACTOR_LU is the
+ * reference's lu with partial pivoting (BEMenerg_coreSA_timeMarching.m:46);
+ * EBEM_FACTOR_CHOLESKY factors the symmetric part (E_0 + E_0^T) / 2, the
+ * north star's "E_0 Cholesky factorisation": E_0 of the semi-analytic
+ * assembly (outer quadrature, exact inner integral) is not exactly symmetric,
+ * so the two differ by the asymmetry's effect on the density.  Returns
+ * EBEM_ERR_SINGULAR when the symmetric part is not positive definite. */
+#define EBEM_FACTOR_LU 0
+#define EBEM_FACTOR_CHOLESKY 1
+int ebem_march_ex(const double* E, int n3, int L, const double* rhs, int nT, double* phi, int factor, void* stream);
+
 /* Pieces of ebem_march for callers that drive the steps themselves (the
  * row-panel marching across ranks, where each rank holds the rows
  * [r0, r0 + rows) of every E_l and one all-gather per step assembles the

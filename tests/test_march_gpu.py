@@ -152,3 +152,47 @@ def test_workspace_pool_reuse_and_release(ebem, oracle):
     assert rel(u2, u1) <= 1e-13 and rel(u3, u1) <= 1e-13
     phi2, _ = ebem.timemarch_sa(dm, w.params, 7, w.datum)
     assert rel(phi2.cpu().numpy(), phi.cpu().numpy()) <= 1e-13
+
+
+def test_cholesky_of_symmetric_part(ebem, oracle):
+    """The north star's Cholesky factorisation of E_0: it factors the
+    symmetric part (E_0 + E_0^T) / 2 (E_0 of the outer-quadrature /
+    exact-inner assembly is not symmetric: 8.0e-3 relative on this mesh), and
+    the marching with it equals a float64 numpy marching with that symmetric
+    part to 1e-12; against the reference's LU marching the density differs by
+    the asymmetry's effect, measured here and bounded."""
+    import torch
+    from elastodynamicebem_b200 import problem
+    w = problem.screen_workload()
+    dm = ebem.DeviceMesh(w.mesh)
+    L = ebem.num_blocks(dm, w.params)
+    E = ebem.assemble_sa(dm, w.params, 7, 0, L)
+    b = ebem.rhs(dm, w.params, 7, w.datum)
+    phi_lu = ebem.march(E, b).cpu().numpy()
+    phi_ch = ebem.march(E, b, factor=ebem.FACTOR_CHOLESKY).cpu().numpy()
+    En, bn = E.cpu().numpy(), b.cpu().numpy()
+    E0 = En[0]
+    asym = np.linalg.norm(E0 - E0.T) / np.linalg.norm(E0)
+    assert 5e-3 < asym < 1.2e-2
+    S = 0.5 * (E0 + E0.T)
+    ref = np.zeros_like(bn)
+    for n in range(bn.shape[0]):
+        rhs_n = bn[n].copy()
+        for l in range(1, min(n + 1, L)):
+            rhs_n -= En[l] @ ref[n - l]
+        ref[n] = np.linalg.solve(S, rhs_n)
+    assert rel(phi_ch, ref) <= 1e-12
+    d = rel(phi_ch, phi_lu)
+    print(f"E_0 asymmetry {asym:.2e}; density Cholesky(sym part) vs LU {d:.2e}")
+    assert d < 0.1
+
+
+def test_cholesky_rejects_indefinite(ebem):
+    import torch
+    from elastodynamicebem_b200.lib import EbemError
+    A = -torch.eye(6, dtype=torch.float64, device="cuda").unsqueeze(0)
+    b = torch.ones((2, 6), dtype=torch.float64, device="cuda")
+    with pytest.raises(EbemError) as ei:
+        ebem.march(A, b, factor=ebem.FACTOR_CHOLESKY)
+    assert ei.value.code == -5 and "positive definite" in str(ei.value)
+    assert torch.allclose(ebem.march(A, b), -b)                   # LU of the same matrix is fine
