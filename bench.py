@@ -184,26 +184,43 @@ def forms(core, problem, torch, w, dm, L, plain_rate):
         return e0.elapsed_time(e1) / reps
     n3 = 3 * dm.N
     out = {}
-    buf64 = torch.empty((L, n3, n3), dtype=torch.float64, device="cuda")
-    buf32 = torch.empty_like(buf64)
-    t64 = timed(lambda: core.assemble_sa(dm, w.params, w.n_gh, 0, L, out=buf64))
-    t32 = timed(lambda: core.assemble_sa(dm, w.params, w.n_gh, 0, L, out=buf32, prec=core.PREC_MIXED))
-    e_rel = float((buf32 - buf64).norm() / buf64.norm())
-    del buf32
-    phi64, _ = core.timemarch_sa(dm, w.params, w.n_gh, w.datum)
-    phi32, _ = core.timemarch_sa(dm, w.params, w.n_gh, w.datum, prec=core.PREC_MIXED)
-    u64 = core.pp_sa(dm, w.params, phi64, w.points, w.times)
-    u32 = core.pp_sa(dm, w.params, phi32, w.points, w.times)
-    out["mixed"] = {"assembly_ms": t32, "fp64_assembly_ms": t64, "speedup": t64 / t32, "blocks_rel_err": e_rel,
-                    "density_rel_err": float((phi32 - phi64).norm() / phi64.norm()),
-                    "displacement_rel_err": float((u32 - u64).norm() / u64.norm()),
-                    "scope": "FP32 edge Gauss-Legendre nodes, FP64 closed forms / moments / marching"}
-    del buf64, phi64, phi32
-    torch.cuda.empty_cache()
+
+    def mixed_form(n_gh):
+        # the sphere of 1280 triangles with outer rule n_gh: assembly times,
+        # errors of blocks, density and displacement (256 exterior points x 40
+        # times) of the mixed form against FP64; E_0's asymmetry and the
+        # density of the Cholesky factorisation of its symmetric part against LU
+        buf64 = torch.empty((L, n3, n3), dtype=torch.float64, device="cuda")
+        buf32 = torch.empty_like(buf64)
+        t64 = timed(lambda: core.assemble_sa(dm, w.params, n_gh, 0, L, out=buf64))
+        t32 = timed(lambda: core.assemble_sa(dm, w.params, n_gh, 0, L, out=buf32, prec=core.PREC_MIXED))
+        e_rel = float((buf32 - buf64).norm() / buf64.norm())
+        del buf32
+        E0 = buf64[0]
+        asym = float((E0 - E0.t()).norm() / E0.norm())
+        b = core.rhs(dm, w.params, n_gh, w.datum)
+        phi_ch = core.march(buf64.transpose(1, 2), b, factor=core.FACTOR_CHOLESKY)
+        phi64, _ = core.timemarch_sa(dm, w.params, n_gh, w.datum)
+        phi32, _ = core.timemarch_sa(dm, w.params, n_gh, w.datum, prec=core.PREC_MIXED)
+        u64 = core.pp_sa(dm, w.params, phi64, w.points, w.times)
+        u32 = core.pp_sa(dm, w.params, phi32, w.points, w.times)
+        res = {"assembly_ms": t32, "fp64_assembly_ms": t64, "speedup": t64 / t32, "blocks_rel_err": e_rel,
+               "density_rel_err": float((phi32 - phi64).norm() / phi64.norm()),
+               "displacement_rel_err": float((u32 - u64).norm() / u64.norm()),
+               "points": int(len(w.points)), "times": int(len(w.times)),
+               "e0_asymmetry": asym,
+               "cholesky_vs_lu_density_rel": float((phi_ch - phi64).norm() / phi64.norm()),
+               "scope": "FP32 edge Gauss-Legendre nodes, FP64 closed forms / moments / marching"}
+        del buf64, phi64, phi32, phi_ch
+        torch.cuda.empty_cache()
+        return res
+
+    out["mixed"] = mixed_form(w.n_gh)
+    out["mixed_gh12"] = mixed_form(12)
     inst = problem.batch_workload(count=64, seed=4)
     dms = [core.DeviceMesh(m) for _, m, _ in inst]
     prms = [p for _, _, p in inst]
-    nlag = [min(core.num_blocks(d, p), 8) for d, p in zip(dms, prms)]
+    nlag = [core.num_blocks(d, p) for d, p in zip(dms, prms)]          # all lags of every instance
     outs = [torch.empty((l, 3 * d.N, 3 * d.N), dtype=torch.float64, device="cuda") for d, l in zip(dms, nlag)]
     counts = [core.assemble_sa(d, p, 7, 0, l, out=o, count=True)[1] for d, p, l, o in zip(dms, prms, nlag, outs)]
     plan = core.BatchPlan(dms, prms, 7, nlag=nlag, prec=core.PREC_FP64)
@@ -213,7 +230,9 @@ def forms(core, problem, torch, w, dm, L, plain_rate):
     t_b32 = timed(lambda: plan32.assemble(outs))
     info = plan.info()
     out["batched"] = {"instances": len(inst), "N_range": [min(d.N for d in dms), max(d.N for d in dms)],
-                      "lags_per_instance": "min(L, 8)", "pair_integrals": int(sum(counts)),
+                      "lags_per_instance": "all (L of each instance)",
+                      "output_gb": sum(9 * d.N ** 2 * l * 8 for d, l in zip(dms, nlag)) / 1e9,
+                      "pair_integrals": int(sum(counts)),
                       "batch_ms": t_batch, "one_launch_per_instance_ms": t_seq, "speedup": t_seq / t_batch,
                       "batch_mixed_ms": t_b32, "pair_integrals_per_s": sum(counts) / t_batch * 1e3,
                       "tile": {"warps_per_block": info["warps_per_block"], "pairs_per_grab": info["pairs_per_grab"]}}
