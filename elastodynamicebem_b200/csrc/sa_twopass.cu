@@ -11,9 +11,9 @@
 // Pass 2 (sa_emit_kernel): every entry of the window's blocks,
 //   E_l = (F_{l+1} - 2 F_l + F_{l-1}) / (4 pi rho), clean-up |x| < 1e-14 -> 0
 // (calcMatrixSubBlock.m:15,23,111; calcMatrixBlock.m:77), zero outside the
-// pair's non-null lags, written (or added) one thread per entry with
-// consecutive threads on consecutive rows of a column: the output is written
-// in whole sectors, zeros included.  In one pass, the warp kernel wrote each
+// pair's non-null lags, written (or added) one thread per block with
+// consecutive threads on consecutive sources: the output is written in whole
+// sectors, zeros included.  In one pass, the warp kernel wrote each
 // block as 24-byte column pieces scattered 3N doubles apart and filled the
 // zeros of the lags outside each pair's band the same way (sphere of 1280
 // triangles, L = 40: 207 ms per step; two passes: 188 ms).
@@ -53,39 +53,61 @@ void profile_read(double ms[2], long long n[2], int reset) {
     }
 }
 
-// E_l of the window from the levels of one chunk of field columns.
-__global__ void __launch_bounds__(256) sa_emit_kernel(const double* __restrict__ Fb, const int2* __restrict__ band,
+// E_l of the window from the levels of one chunk of field columns: one
+// thread per (source, field, lag) block, consecutive threads on consecutive
+// sources of one field column, so each of the 9 stores of a warp covers one
+// contiguous 768-byte run of a column (the three row stores of a column fill
+// it completely); the levels are read as 16-byte pairs.
+__global__ void __launch_bounds__(128) sa_emit_kernel(const double* __restrict__ Fb, const int2* __restrict__ band,
                                                       int nsrc, int j0, int KL, int kbase, int lag0, double c4,
                                                       double* __restrict__ E, size_t ld, size_t ld_lag,
                                                       int accumulate) {
-    const long long rows = 3LL * nsrc;
-    const long long r3 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r3 >= rows) return;
-    const int col = blockIdx.y;                   // 3 jj + c
-    const int jj = col / 3, c = col - 3 * jj;
-    const int q = blockIdx.z, l = lag0 + q;
-    const int ii = (int)(r3 / 3), r = (int)(r3 - 3LL * ii);
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ii >= nsrc) return;
+    const int jj = blockIdx.y, q = blockIdx.z, l = lag0 + q;
     const int2 b = band[(long long)jj * nsrc + ii];
-    double v = 0.0;
+    double v[6] = {0, 0, 0, 0, 0, 0};
     if (b.x >= 0 && l >= b.x && l <= b.y) {
-        const int e = (r == 0) ? c : (c == 0 ? r : r + c + 1);        // (r, c) -> 11, 12, 13, 22, 23, 33
-        const double* f = Fb + ((long long)jj * KL * nsrc + ii) * 6 + e;
-        const long long ks = (long long)nsrc * 6;                       // one level
-        const double fk1 = f[(l + 1 - kbase) * ks];
-        const double fk = (l >= 1) ? f[(l - kbase) * ks] : 0.0;            // F_0 = 0
-        const double fkm = (l - 1 >= 1) ? f[(l - 1 - kbase) * ks] : 0.0;
-        v = ((fk1 + (-2.0) * fk) + fkm) / c4;
-        if (fabs(v) < 1.0e-14) v = 0.0;
+        const long long rec = (long long)jj * KL * nsrc + ii;          // record of level kbase
+        const long long ks = nsrc;                                       // records per level
+        double f1[6], f0[6] = {0, 0, 0, 0, 0, 0}, fm[6] = {0, 0, 0, 0, 0, 0};
+        const double2* p1 = reinterpret_cast<const double2*>(Fb + (rec + (l + 1 - kbase) * ks) * 6);
+#pragma unroll
+        for (int h = 0; h < 3; h++) { const double2 t = p1[h]; f1[2 * h] = t.x; f1[2 * h + 1] = t.y; }
+        if (l >= 1) {                                                      // F_0 = 0
+            const double2* p0 = reinterpret_cast<const double2*>(Fb + (rec + (l - kbase) * ks) * 6);
+#pragma unroll
+            for (int h = 0; h < 3; h++) { const double2 t = p0[h]; f0[2 * h] = t.x; f0[2 * h + 1] = t.y; }
+        }
+        if (l - 1 >= 1) {
+            const double2* pm = reinterpret_cast<const double2*>(Fb + (rec + (l - 1 - kbase) * ks) * 6);
+#pragma unroll
+            for (int h = 0; h < 3; h++) { const double2 t = pm[h]; fm[2 * h] = t.x; fm[2 * h + 1] = t.y; }
+        }
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+            const double x = ((f1[e] + (-2.0) * f0[e]) + fm[e]) / c4;
+            v[e] = (fabs(x) < 1.0e-14) ? 0.0 : x;
+        }
     }
-    double* dst = E + (size_t)q * ld_lag + (3 * (size_t)(j0 + jj) + c) * ld + (size_t)r3;
-    if (accumulate) *dst += v;
-    else *dst = v;
+    // (r, c) -> symmetric entry 11, 12, 13, 22, 23, 33
+    const int sym[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    double* base = E + (size_t)q * ld_lag + 3 * (size_t)(j0 + jj) * ld + 3 * (size_t)ii;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            double* dst = base + (size_t)c * ld + r;
+            const double x = v[sym[3 * c + r]];
+            if (accumulate) *dst += x;
+            else *dst = x;
+        }
 }
 
 int launch_sa_twopass(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                       double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count, int mixed,
                       cudaStream_t s) {
-    if (3LL * m.nt > 65535 || nlag > 65535) return fail(EBEM_ERR_INVALID, "mesh or lag window too large for one launch");
+    if (m.nt > 65535 || nlag > 65535) return fail(EBEM_ERR_INVALID, "mesh or lag window too large for one launch");
     const int kbase = std::max(1, lag0 - 1);
     const int KL = lag0 + nlag + 1 - kbase;           // levels kbase .. lag0 + nlag
     const size_t fbytes = (size_t)KL * nsrc * 6 * sizeof(double);
@@ -117,9 +139,8 @@ int launch_sa_twopass(const MeshData& m, const PhysParams& P, int n_gh, int lag0
         rc = launch_sa_fwarp(m, P, n_gh, lag0, nlag, src0, nsrc, j0, nj, kbase, KL, Fb, band, d_count, mixed, s);
         if (rc) break;
         mark();
-        const long long rows = 3LL * nsrc;
-        dim3 grid((unsigned)((rows + 255) / 256), (unsigned)(3 * nj), (unsigned)nlag);
-        sa_emit_kernel<<<grid, 256, 0, s>>>(Fb, band, nsrc, j0, KL, kbase, lag0, 4 * kPi * P.rho, d_E, ld, ld_lag,
+        dim3 grid((unsigned)((nsrc + 127) / 128), (unsigned)nj, (unsigned)nlag);
+        sa_emit_kernel<<<grid, 128, 0, s>>>(Fb, band, nsrc, j0, KL, kbase, lag0, 4 * kPi * P.rho, d_E, ld, ld_lag,
                                             accumulate);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, std::string("emission kernel: ") + cudaGetErrorString(e));
