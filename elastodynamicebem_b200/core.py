@@ -472,8 +472,28 @@ class BatchPlan:
 # ---------------------------------------------------------------------------
 # learned quadrature selector
 
-SELECTOR_RULES = (3, 7, 12, 19)
+# outer rules of the four classes: (Gauss-Hammer nodes, sub-triangles)
+SELECTOR_RULES = ((7, 1), (7, 4), (7, 16), (7, 64))
 SELECTOR_PARAMS = 5252
+
+
+def _rules_arg(rules):
+    flat = [int(v) for r in rules for v in r]
+    return (C.c_int * len(flat))(*flat), len(rules)
+
+
+def sa_pair_blocks(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, n_sub: int, pairs: torch.Tensor, nlag: int,
+                   stream=None) -> torch.Tensor:
+    """Blocks of explicit pairs (int32 (P, 2) device tensor: source, field)
+    at lags 0..nlag-1 with rule (n_gh, n_sub): (P, nlag, 6) float64, the
+    symmetric entries 11, 12, 13, 22, 23, 33."""
+    pairs = pairs.to(device="cuda", dtype=torch.int32).contiguous()
+    out = torch.empty((pairs.shape[0], nlag, 6), dtype=torch.float64, device="cuda")
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_sa_pair_blocks(dmesh.handle, C.byref(p), int(n_gh), int(n_sub),
+                                               C.c_void_p(pairs.data_ptr()), int(pairs.shape[0]), int(nlag),
+                                               C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
+    return out
 
 
 def selector_init(seed: int = 0) -> torch.Tensor:
@@ -483,19 +503,31 @@ def selector_init(seed: int = 0) -> torch.Tensor:
     return p
 
 
-def selector_features(dmesh: DeviceMesh, prm: ProblemParams, stream=None) -> torch.Tensor:
-    f = torch.empty((dmesh.N * dmesh.N, 12), dtype=torch.float32, device="cuda")
+def selector_features(dmesh: DeviceMesh, prm: ProblemParams, samples: torch.Tensor, stream=None) -> torch.Tensor:
+    """Features (n, 12) of samples (int32 (n, 3) device tensor: source, field, lag)."""
+    samples = samples.to(device="cuda", dtype=torch.int32).contiguous()
+    f = torch.empty((samples.shape[0], 12), dtype=torch.float32, device="cuda")
     p = _lib.problem_struct(prm)
-    _lib.check(_lib.load().ebem_selector_features(dmesh.handle, C.byref(p), C.c_void_p(f.data_ptr()),
+    _lib.check(_lib.load().ebem_selector_features(dmesh.handle, C.byref(p), C.c_void_p(samples.data_ptr()),
+                                                  int(samples.shape[0]), C.c_void_p(f.data_ptr()),
                                                   _stream_ptr(stream)))
     return f
 
 
-def selector_labels(dmesh: DeviceMesh, prm: ProblemParams, tol: float, stream=None) -> torch.Tensor:
-    y = torch.empty(dmesh.N * dmesh.N, dtype=torch.int32, device="cuda")
-    p = _lib.problem_struct(prm)
-    _lib.check(_lib.load().ebem_selector_labels(dmesh.handle, C.byref(p), float(tol), C.c_void_p(y.data_ptr()),
-                                                _stream_ptr(stream)))
+def selector_labels(blocks: torch.Tensor, tol: float, scale: float, scales: torch.Tensor | None = None,
+                    stream=None) -> torch.Tensor:
+    """Labels of n samples from their blocks at the four rules ((4, n, 6)
+    float64 device tensor); threshold tol * scale, times scales[q] (float64
+    device tensor) when given."""
+    blocks = blocks.contiguous()
+    n = blocks.shape[1]
+    y = torch.empty(n, dtype=torch.int32, device="cuda")
+    sp = None
+    if scales is not None:
+        scales = scales.to(device="cuda", dtype=torch.float64).contiguous()
+        sp = C.c_void_p(scales.data_ptr())
+    _lib.check(_lib.load().ebem_selector_labels(C.c_void_p(blocks.data_ptr()), int(n), float(tol), float(scale), sp,
+                                                C.c_void_p(y.data_ptr()), _stream_ptr(stream)))
     return y
 
 
@@ -521,26 +553,49 @@ def selector_train(params: torch.Tensor, feats: torch.Tensor, labels: torch.Tens
     return losses
 
 
-def selector_infer(params: torch.Tensor, dmesh: DeviceMesh, prm: ProblemParams, threshold: float = 0.9, stream=None):
-    c = torch.empty(dmesh.N * dmesh.N, dtype=torch.int32, device="cuda")
+def selector_infer(params: torch.Tensor, dmesh: DeviceMesh, prm: ProblemParams, threshold: float = 0.9,
+                   lag0: int = 0, nlag: int | None = None, stream=None):
+    """Class bytes (N*N, nlag) of every (pair, lag), row = field * N + source;
+    returns (cls, non-null lags per class)."""
+    if nlag is None:
+        nlag = num_blocks(dmesh, prm) - lag0
+    c = torch.empty((dmesh.N * dmesh.N, nlag), dtype=torch.uint8, device="cuda")
     p = _lib.problem_struct(prm)
+    counts = (C.c_longlong * 4)()
     _lib.check(_lib.load().ebem_selector_infer(C.c_void_p(params.data_ptr()), dmesh.handle, C.byref(p),
-                                               float(threshold), C.c_void_p(c.data_ptr()), _stream_ptr(stream)))
-    return c
+                                               float(threshold), int(lag0), int(nlag), C.c_void_p(c.data_ptr()),
+                                               counts, _stream_ptr(stream)))
+    return c, [int(v) for v in counts]
 
 
-def assemble_sa_selected(dmesh: DeviceMesh, prm: ProblemParams, classes: torch.Tensor, lag0: int = 0,
-                         nlag: int | None = None, out: torch.Tensor | None = None, prec: int = PREC_FP64, stream=None):
-    """E[l][row, col] with each pair assembled on the rule of its class;
-    returns (E, pairs per class)."""
+def assemble_sa_selected(dmesh: DeviceMesh, prm: ProblemParams, cls: torch.Tensor, rules=SELECTOR_RULES,
+                         lag0: int = 0, nlag: int | None = None, out: torch.Tensor | None = None,
+                         prec: int = PREC_FP64, stream=None):
+    """E[l][row, col] with each (pair, lag) assembled on the rule of its class
+    (cls: uint8 (N*N, nlag) device tensor, row = field * N + source); returns
+    (E, non-null lags per class)."""
     if nlag is None:
         nlag = num_blocks(dmesh, prm) - lag0
     n3 = 3 * dmesh.N
     if out is None:
         out = torch.empty((nlag, n3, n3), dtype=torch.float64, device="cuda")
+    cls = cls.contiguous()
+    if cls.dtype != torch.uint8 or cls.numel() != dmesh.N * dmesh.N * nlag:
+        raise ValueError("cls must be a uint8 tensor of N*N*nlag entries")
     p = _lib.problem_struct(prm)
-    counts = (C.c_longlong * 4)()
-    _lib.check(_lib.load().ebem_assemble_sa_selected(dmesh.handle, C.byref(p), C.c_void_p(classes.data_ptr()),
+    r, nc = _rules_arg(rules)
+    counts = (C.c_longlong * nc)()
+    _lib.check(_lib.load().ebem_assemble_sa_selected(dmesh.handle, C.byref(p), r, nc, C.c_void_p(cls.data_ptr()),
                                                      int(lag0), int(nlag), C.c_void_p(out.data_ptr()), int(prec),
                                                      _stream_ptr(stream), counts))
-    return out.view(nlag, n3, n3).transpose(1, 2), [int(c) for c in counts]
+    return out.view(nlag, n3, n3).transpose(1, 2), [int(v) for v in counts]
+
+
+def assemble_sa_rule(dmesh: DeviceMesh, prm: ProblemParams, n_gh: int, n_sub: int, lag0: int = 0,
+                     nlag: int | None = None, out: torch.Tensor | None = None, prec: int = PREC_FP64, stream=None):
+    """The plain assembly with the composite outer rule (n_gh, n_sub); returns E."""
+    if nlag is None:
+        nlag = num_blocks(dmesh, prm) - lag0
+    cls = torch.zeros((dmesh.N * dmesh.N, nlag), dtype=torch.uint8, device="cuda")
+    E, _ = assemble_sa_selected(dmesh, prm, cls, ((n_gh, n_sub),), lag0, nlag, out, prec, stream)
+    return E

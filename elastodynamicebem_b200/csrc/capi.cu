@@ -386,6 +386,8 @@ int ebem_mesh_destroy(ebem_mesh* m) {
     if (m->d.d_geo) cudaFree(m->d.d_geo);
     for (NodeW* t : m->d.d_node_tables)
         if (t) cudaFree(t);
+    for (NodeW* t : m->d.d_comp_tables)
+        if (t) cudaFree(t);
     free_direct(m->d);
     delete m;
     return EBEM_OK;
@@ -426,6 +428,9 @@ int ebem_mesh_cache_info(const ebem_mesh* m, int* rules_cached, long long* devic
             mask |= 1 << k;
             bytes += 32LL * d.nt * kSlotRule[k];
         }
+    for (int k = 0; k < MeshData::kCompRules; k++)
+        if (d.d_comp_tables[k])
+            bytes += 32LL * d.nt * (d.comp_key[k] / 4096) * (d.comp_key[k] % 4096);
     if (d.d_dir) bytes += (long long)sizeof(DirTri) * d.nt + (long long)sizeof(int32_t) * (d.nv + 1 + 3LL * d.nt);
     if (rules_cached) *rules_cached = mask;
     if (device_bytes) *device_bytes = bytes;
@@ -1263,21 +1268,39 @@ int ebem_selector_init(float* params, unsigned long long seed) {
     return EBEM_OK;
 }
 
-int ebem_selector_features(const ebem_mesh* m, const ebem_problem* p, float* feats, void* stream) {
-    if (!m || !all_device({feats})) return fail(EBEM_ERR_INVALID, "mesh and a device feature buffer required");
+int ebem_sa_pair_blocks(const ebem_mesh* m, const ebem_problem* p, int n_gh, int n_sub, const int* pairs,
+                        long long npairs, int nlag, double* out, void* stream) {
+    if (!m || npairs < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "mesh, npairs >= 0 and nlag >= 1 required");
+    if (npairs == 0) return EBEM_OK;
+    if (!all_device({pairs, out})) return fail(EBEM_ERR_INVALID, "device pair and output buffers required");
     if (int rc = check_problem(p)) return rc;
+    if (n_gh < 1 || n_sub < 1) return fail(EBEM_ERR_INVALID, "n_gh and n_sub must be >= 1");
     DeviceGuard dg(m->d.device);
-    return selector_features(m->d, phys_from(p), feats, (cudaStream_t)stream);
+    MeshData& d = const_cast<MeshData&>(m->d);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int rc = map_nodes_composite(d, n_gh, n_sub, s)) return rc;
+    return launch_sa_pair_blocks(d, phys_from(p), n_gh * n_sub, reinterpret_cast<const int2*>(pairs), npairs, nlag, out,
+                                 s);
 }
 
-int ebem_selector_labels(const ebem_mesh* m, const ebem_problem* p, double tol, int* labels, void* stream) {
-    if (!m || !all_device({labels})) return fail(EBEM_ERR_INVALID, "mesh and a device label buffer required");
+int ebem_selector_features(const ebem_mesh* m, const ebem_problem* p, const int* samples, long long n, float* feats,
+                           void* stream) {
+    if (!m || n < 0) return fail(EBEM_ERR_INVALID, "mesh and n >= 0 required");
+    if (n == 0) return EBEM_OK;
+    if (!all_device({samples, feats})) return fail(EBEM_ERR_INVALID, "device sample and feature buffers required");
     if (int rc = check_problem(p)) return rc;
-    if (!(tol >= 0)) return fail(EBEM_ERR_INVALID, "tolerance must be >= 0");
-    int L = 0;
-    if (int rc = ebem_num_blocks(m, p, &L)) return rc;
     DeviceGuard dg(m->d.device);
-    return selector_labels(const_cast<MeshData&>(m->d), phys_from(p), L, tol, labels, (cudaStream_t)stream);
+    return selector_features(m->d, phys_from(p), samples, n, feats, (cudaStream_t)stream);
+}
+
+int ebem_selector_labels(const double* blocks, long long n, double tol, double scale, const double* scales,
+                         int* labels, void* stream) {
+    if (n < 0 || !(tol >= 0) || !(scale >= 0)) return fail(EBEM_ERR_INVALID, "n, tol and scale must be >= 0");
+    if (n == 0) return EBEM_OK;
+    if (!all_device({blocks, labels}) || (scales && !all_device({scales})))
+        return fail(EBEM_ERR_INVALID, "device block, scale and label buffers required");
+    if (int rc = check_device()) return rc;
+    return selector_labels(blocks, n, tol, scale, scales, labels, (cudaStream_t)stream);
 }
 
 int ebem_selector_grad(const float* params, const float* feats, const int* labels, long long n, float* grad,
@@ -1299,22 +1322,27 @@ int ebem_selector_train(float* params, const float* feats, const int* labels, lo
     return selector_train(params, feats, labels, n, epochs, batch, lr, seed, losses, (cudaStream_t)stream);
 }
 
-int ebem_selector_infer(const float* params, const ebem_mesh* m, const ebem_problem* p, float threshold, int* classes,
-                        void* stream) {
-    if (!m || !all_device({params, classes})) return fail(EBEM_ERR_INVALID, "mesh and device buffers required");
+int ebem_selector_infer(const float* params, const ebem_mesh* m, const ebem_problem* p, float threshold, int lag0,
+                        int nlag, unsigned char* cls, long long* counts, void* stream) {
+    if (!m || !all_device({params, cls})) return fail(EBEM_ERR_INVALID, "mesh and device buffers required");
     if (int rc = check_problem(p)) return rc;
+    if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
     DeviceGuard dg(m->d.device);
-    return selector_infer(params, m->d, phys_from(p), threshold, classes, (cudaStream_t)stream);
+    return selector_infer(params, m->d, phys_from(p), threshold, lag0, nlag, cls, counts, (cudaStream_t)stream);
 }
 
-int ebem_assemble_sa_selected(const ebem_mesh* m, const ebem_problem* p, const int* classes, int lag0, int nlag,
-                              double* E, int prec, void* stream, long long* pairs_per_class) {
-    if (!m || !all_device({classes, E})) return fail(EBEM_ERR_INVALID, "mesh and device buffers required");
+int ebem_assemble_sa_selected(const ebem_mesh* m, const ebem_problem* p, const int* rules, int nclass,
+                              const unsigned char* cls, int lag0, int nlag, double* E, int prec, void* stream,
+                              long long* counts) {
+    if (!m || !rules || !all_device({cls, E})) return fail(EBEM_ERR_INVALID, "mesh, rules and device buffers required");
     if (int rc = check_problem(p)) return rc;
+    if (nclass < 1 || nclass > 255) return fail(EBEM_ERR_INVALID, "nclass must be in 1..255");
+    for (int c = 0; c < nclass; c++)
+        if (rules[2 * c] < 1 || rules[2 * c + 1] < 1) return fail(EBEM_ERR_INVALID, "rule sizes must be >= 1");
     if (lag0 < 0 || nlag < 1) return fail(EBEM_ERR_INVALID, "need lag0 >= 0 and nlag >= 1");
     if (prec != EBEM_PREC_FP64 && prec != EBEM_PREC_MIXED) return fail(EBEM_ERR_INVALID, "unknown precision mode");
     DeviceGuard dg(m->d.device);
-    return assemble_selected(const_cast<MeshData&>(m->d), phys_from(p), classes, lag0, nlag, E, prec, pairs_per_class,
+    return assemble_selected(const_cast<MeshData&>(m->d), phys_from(p), rules, nclass, cls, lag0, nlag, E, prec, counts,
                              (cudaStream_t)stream);
 }
 

@@ -63,6 +63,11 @@ struct MeshData {
     // the last map_nodes call.
     static constexpr int kNodeRules = 6;          // rules of 1, 3, 7, 12, 19, 28 nodes
     NodeW* d_node_tables[kNodeRules] = {};
+    // composite rules (n_gh nodes on n_sub sub-triangles, n_sub > 1), the same
+    // lifetime: key n_gh * 4096 + n_sub
+    static constexpr int kCompRules = 16;
+    int comp_key[kCompRules] = {};
+    NodeW* d_comp_tables[kCompRules] = {};
     int nodes_rule = 0;
     NodeW* d_nodes = nullptr;     // nt x nodes_rule
     // direct formulation (built on first use): per-triangle P1 data and the
@@ -81,6 +86,9 @@ int gh_composite(int n_nodes, int n_sub, double* nodes, double* weights);
 // Device preparation of the per-triangle geometry.
 int prep_mesh(MeshData& m, cudaStream_t s);
 int map_nodes(MeshData& m, int n_gh, cudaStream_t s);
+// The same for GaussHammerComposite(n_sub, n_gh): n_gh * n_sub nodes per
+// triangle in m.d_nodes (n_sub = 1 is map_nodes).
+int map_nodes_composite(MeshData& m, int n_gh, int n_sub, cudaStream_t s);
 
 struct PhysParams {
     double rho, velP, velS, dt;
@@ -98,9 +106,13 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
 // The same assembly in two passes (sa_twopass.cu): F(t_k) of every (pair,
 // level) into a workspace, then the second difference written column by
 // column.  Dense outputs only (no pair list, no diagonal-only mode).
+// With a class array cls (device, cls[(j N + i) nlag + l - lag0] for field j,
+// source i; src0 = 0, nsrc = N) only the lags of class cls_want are written
+// (and the zeros outside the non-null lags when cls_want is 0), with the
+// outer rule in m.d_nodes (n_gh nodes per triangle, composite or not).
 int launch_sa_twopass(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                      double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count, int mixed,
-                     cudaStream_t s);
+                     cudaStream_t s, const unsigned char* cls = nullptr, int cls_want = -1);
 // Per-pass device times of the two-pass assembly (ebem_profile_enable / _read).
 void profile_enable(int on);
 void profile_read(double ms[2], long long n[2], int reset);
@@ -108,7 +120,12 @@ void profile_read(double ms[2], long long n[2], int reset);
 // F(t_k) and the non-null lags of the pairs of field columns [j0, j0 + nj).
 int launch_sa_fwarp(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc, int j0,
                     int nj, int kbase, int KL, double* d_F, int2* d_band, unsigned long long* d_count, int mixed,
-                    cudaStream_t s);
+                    cudaStream_t s, const unsigned char* cls = nullptr, int cls_want = -1);
+// Blocks of explicit (source, field) pairs (int2 list, device) at lags
+// [0, nlag) with the rule in m.d_nodes: out[(p nlag + l) 6 + e], 6 symmetric
+// entries per block, zero outside the pair's non-null lags.
+int launch_sa_pair_blocks(const MeshData& m, const PhysParams& P, int n_gh, const int2* d_pairs, long long npairs,
+                          int nlag, double* d_out, cudaStream_t s);
 // Allocation-free variant of the full assembly (device E, ld = 3N): mapped
 // nodes and the counter live in a static device array (sa_assemble.cu).
 int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, double* d_E,
@@ -219,16 +236,20 @@ int launch_hist_gemv(const double* A, int n3, long long K, const double* x, doub
 
 // ---------------------------------------------------------------------------
 // learned quadrature selector (selector.cu)
-int selector_features(const MeshData& m, const PhysParams& P, float* d_out, cudaStream_t s);
-int selector_labels(MeshData& m, const PhysParams& P, int L, double tol, int* d_labels, cudaStream_t s);
+// features of samples[3 q + 0..2] = (source, field, lag)
+int selector_features(const MeshData& m, const PhysParams& P, const int* d_samples, long long n, float* d_out,
+                      cudaStream_t s);
+// labels from the samples' blocks at the four rules (blocks[(c n + q) 6 + e])
+int selector_labels(const double* d_blocks, long long n, double tol, double scale, const double* d_scales,
+                    int* d_labels, cudaStream_t s);
 int selector_grad(const float* d_params, const float* d_feats, const int* d_labels, long long n, float* d_grad,
                   float* d_loss, cudaStream_t s);
 int selector_train(float* d_params, const float* d_feats, const int* d_labels, long long n, int epochs, int batch,
                    float lr, unsigned long long seed, float* h_losses, cudaStream_t s);
-int selector_infer(const float* d_params, const MeshData& m, const PhysParams& P, float threshold, int* d_classes,
-                   cudaStream_t s);
-int assemble_selected(MeshData& m, const PhysParams& P, const int* d_classes, int lag0, int nlag, double* d_E, int prec,
-                      long long* h_counts, cudaStream_t s);
+int selector_infer(const float* d_params, const MeshData& m, const PhysParams& P, float threshold, int lag0, int nlag,
+                   unsigned char* d_cls, long long* h_counts, cudaStream_t s);
+int assemble_selected(MeshData& m, const PhysParams& P, const int* h_rules, int nclass, const unsigned char* d_cls,
+                      int lag0, int nlag, double* d_E, int prec, long long* h_counts, cudaStream_t s);
 void selector_init(float* h_params, unsigned long long seed);
 
 }  // namespace ebem

@@ -23,12 +23,16 @@
 // times, once per lag that uses it).
 #include "ebem_internal.h"
 
+#include <algorithm>
 #include <mutex>
 #include "sa_pair.cuh"
 #include "sa_warp.cuh"
 
 #ifndef EBEM_SA_KERNEL
 #define EBEM_SA_KERNEL 0    // 0: warp per pair when 3 n_gh <= 32, 1: always thread per pair
+#endif
+#ifndef EBEM_LEVEL_GROUPED
+#define EBEM_LEVEL_GROUPED 1  // 1: the two-pass level pass runs sa_level_kernel for every rule
 #endif
 #ifndef EBEM_SA_TWOPASS
 #define EBEM_SA_TWOPASS 1   // 1: dense assemblies store F(t_k) and emit the blocks in a second pass (sa_twopass.cu)
@@ -125,6 +129,57 @@ int map_nodes(MeshData& m, int n_gh, cudaStream_t s) {
     return EBEM_OK;
 }
 
+int map_nodes_composite(MeshData& m, int n_gh, int n_sub, cudaStream_t s) {
+    if (n_sub == 1) return map_nodes(m, n_gh, s);
+    const int key = n_gh * 4096 + n_sub;
+    for (int k = 0; k < MeshData::kCompRules; k++)
+        if (m.d_comp_tables[k] && m.comp_key[k] == key) {
+            m.d_nodes = m.d_comp_tables[k];
+            m.nodes_rule = n_gh * n_sub;
+            return EBEM_OK;
+        }
+    int slot = -1;
+    for (int k = 0; k < MeshData::kCompRules && slot < 0; k++)
+        if (!m.d_comp_tables[k]) slot = k;
+    if (slot < 0) return fail(EBEM_ERR_INVALID, "too many composite outer rules cached on one mesh");
+    if (n_sub < 1 || n_sub > 1024) return fail(EBEM_ERR_INVALID, "composite rule: n_sub out of range");
+    const int nn = n_gh * n_sub;
+    std::vector<double> bary(3 * (size_t)nn), w((size_t)nn), wb(n_gh);
+    int rc = gh_composite(n_gh, n_sub, bary.data(), wb.data());
+    if (rc) return fail(rc, "unsupported composite Gauss-Hammer rule (n_sub must be a square)");
+    for (int q = 0; q < n_sub; q++)
+        for (int g = 0; g < n_gh; g++) w[(size_t)q * n_gh + g] = wb[g];
+    NodeW* table = nullptr;
+    double* d_tab = nullptr;
+    if (cudaMalloc(&table, sizeof(NodeW) * (size_t)m.nt * nn) != cudaSuccess ||
+        cudaMalloc(&d_tab, sizeof(double) * 4 * (size_t)nn) != cudaSuccess) {
+        cudaGetLastError();
+        if (table) cudaFree(table);
+        return fail(EBEM_ERR_NOMEM, "outer-node table allocation failed");
+    }
+    cudaError_t e = cudaMemcpyAsync(d_tab, bary.data(), sizeof(double) * 3 * nn, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_tab + 3 * (size_t)nn, w.data(), sizeof(double) * nn, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        const long long total = (long long)m.nt * nn;
+        const int threads = 128;
+        map_nodes_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, s>>>(
+            m.d_coords, m.d_tris, m.nt, m.d_geo, d_tab, d_tab + 3 * (size_t)nn, nn, table);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_tab);
+    if (e != cudaSuccess) {
+        cudaFree(table);
+        return fail(EBEM_ERR_CUDA, std::string("outer-node mapping: ") + cudaGetErrorString(e));
+    }
+    m.d_comp_tables[slot] = table;
+    m.comp_key[slot] = key;
+    m.d_nodes = table;
+    m.nodes_rule = nn;
+    return EBEM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // assembly
 
@@ -155,6 +210,11 @@ struct SAArgs {
     double* Fout = nullptr;
     int2* band = nullptr;
     int j0 = 0, nj = 0, kbase = 0, KL = 0;
+    // level output restricted to one class of a per-(pair, lag) class array:
+    // cls[(j N + i) nlag + l - lag0] (fields j, sources i); only the levels
+    // that lags of class cls_want use are computed, only those lags counted
+    const unsigned char* cls = nullptr;
+    int cls_want = -1;
 };
 
 __device__ __forceinline__ void store_block(const SAArgs& A, int q, int i, int j, const double b[6]) {
@@ -587,6 +647,435 @@ static int launch_warp(const SAArgs& A, long long NN, int device, cudaStream_t s
     return EBEM_OK;
 }
 
+// sech s, tanh s and the radial antiderivatives at the edge point R = F cosh s
+// (radial_edge) of one Gauss-Legendre node.  With EBEM_GL_ONEDIV (default;
+// the sphere of 1280 triangles 161 -> 157 ms per step against hyp() and
+// radial_edge(), which divide three times per node) the
+// reciprocals of e^s, 1 + e^2s, r' and r' + F (1 + e^2s) (r' = 2 e^s r) come
+// from one division: 1/e^s, 1/cosh, 1/(r (r + R)) and 1/r then cost
+// multiplications, and log(R + r) = log(r' + F (1 + e^2s)) - s - log 2.
+#ifndef EBEM_GL_ONEDIV
+#define EBEM_GL_ONEDIV 1
+#endif
+EBEM_DI void edge_point(double s, double Fc, double zeta, double& sech, double& th, Rad& v) {
+#if EBEM_GL_ONEDIV
+    const double e = m_exp(s), e2 = e * e, u = e2 + 1.0;
+    const double z2 = zeta * zeta, Fu = Fc * u;
+    const double rp = sqrt(Fu * Fu + 4.0 * z2 * e2);          // 2 e^s r
+    const double a = rp + Fu;                                 // 2 e^s (r + R)
+    const double ue = u * e, ra = rp * a;
+    const double inv = 1.0 / (ue * ra);
+    const double iu = e * ra * inv, ie = u * ra * inv, irp = ue * a * inv, ia = ue * rp * inv;
+    sech = 2.0 * e * iu;
+    th = (e2 - 1.0) * iu;
+    const double r = 0.5 * rp * ie, R = 0.5 * Fu * ie;
+    const double ir = 2.0 * e * irp, ir3 = ir * ir * ir;
+    v.A1 = r;
+    v.A3 = -ir;
+    v.B2 = r + z2 * ir;
+    v.D2 = -z2 * ir;
+    v.B4 = -ir + z2 * ir3 * (1.0 / 3.0);
+    v.D4 = -z2 * ir3 * (1.0 / 3.0);
+    if (zeta > 0) {
+        v.C2 = m_log(a) - (s + 0.69314718055994530942) - Fu * irp;
+        v.C4 = -(r * r + r * R + R * R) * ir3 * (2.0 * e * ia) * (1.0 / 3.0);
+    } else {
+        v.C2 = 0.0;
+        v.C4 = 0.0;
+    }
+#else
+    double ch;
+    hyp(s, ch, sech, th);
+    v = radial_edge(Fc * ch, zeta);
+#endif
+}
+
+// ---------------------------------------------------------------------------
+// Level pass of the two-pass assembly, outer nodes in groups.
+//
+// One warp per (source, field) pair walks the pair's time levels with the
+// schedule of assemble_pair (lane = child of one outer node; per level the
+// per-child decision phase, the whole-range moments, the warp-wide list of
+// Gauss-Legendre nodes and one warp reduction), for the children of at most
+// 10 outer nodes at a time, so composite outer rules of any size
+// (GaussHammerComposite.m) run group after group with each group's per-level
+// sums added in shared memory.  After the levels of a chunk, one lane per
+// level forms F(t_k) (the rotation to global axes) and stores it for the
+// emission pass.  With a per-(pair, lag) class array only the levels used by
+// lags of the wanted class are walked.
+//
+// An alternative schedule was measured and not kept: compacted (child,
+// level) items, 32 per round, each lane on its own item (sphere of 1280
+// triangles: 224 ms per step against 186 ms; ncu: 9 % fewer warp
+// instructions, but more instruction-fetch stalls, the items of a round
+// taking more distinct branches than the children of one level).
+
+#ifndef EBEM_LEVEL_KC
+#define EBEM_LEVEL_KC 48         // levels per chunk (per-level sums in shared memory)
+#endif
+#ifndef EBEM_LEVEL_WPB
+#define EBEM_LEVEL_WPB 4
+#endif
+#ifndef EBEM_LEVEL_MINB
+#define EBEM_LEVEL_MINB 3
+#endif
+#ifndef EBEM_LEVEL_SKIP_IDLE
+#define EBEM_LEVEL_SKIP_IDLE 1   // 1: levels at which no child works skip the decision and node phases
+#endif
+constexpr int kGroupNodes = 10;  // outer nodes per group: 30 children on 32 lanes
+
+struct LevelShared {
+    WarpShared<1> W;
+    double acc[7][EBEM_LEVEL_KC];
+};
+
+// Whether level k is used by a lag of the wanted class (lags k-1, k, k+1 of
+// the pair's non-null range [llo, lhi]).
+EBEM_DI bool level_wanted(const SAArgs& A, const unsigned char* cls, int k, int llo, int lhi) {
+    if (!cls) return true;
+    for (int l = max(k - 1, llo); l <= min(k + 1, lhi); l++)
+        if (cls[l - A.lag0] == A.cls_want) return true;
+    return false;
+}
+
+// Pair p of the launch: (source i, field j); its record in A.band and its
+// levels in A.Fout (record rec, level k at (rec + (k - kbase) kstride) 6):
+// field columns of a panel (rec = (j - j0) KL nsrc + i - src0, kstride =
+// nsrc) or an explicit pair list (rec = p KL, kstride = 1).
+template <bool MIXED>
+__device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, const double* glx, const double* glw,
+                                           long long p, int i, int j, int lane, unsigned long long& my_count) {
+    WarpShared<1>& W = Ls.W;
+    const TriGeom& F = A.geo[j];
+    const TriGeom& Sg = A.geo[i];
+    int llo = -1, lhi = -2;
+    pair_band(F, Sg, A.velP, A.velS, A.dt, A.lag0, A.nlag, &llo, &lhi);
+    const long long brec = A.pairs ? p : (long long)(j - A.j0) * A.nsrc + (i - A.src0);
+    const long long frec = A.pairs ? p * A.KL : (long long)(j - A.j0) * A.KL * A.nsrc + (i - A.src0);
+    const long long kstride = A.pairs ? 1 : A.nsrc;
+    if (lane == 0) A.band[brec] = make_int2(llo, lhi);
+    if (llo < 0) return;
+    const unsigned char* cls = A.cls ? A.cls + ((long long)j * A.N + i) * A.nlag : nullptr;
+    if (cls) {
+        int n = 0;
+        for (int l = llo; l <= lhi; l++) n += (cls[l - A.lag0] == A.cls_want);
+        if (lane == 0) my_count += (unsigned long long)n;
+        if (n == 0) return;
+    } else if (lane == 0) {
+        my_count += (unsigned long long)(lhi - llo + 1);
+    }
+    const double vp2 = A.velP * A.velP, vs2 = A.velS * A.velS, den = vp2 * vs2;
+    const double k1 = 1.0 / vp2, k5 = (vp2 + vs2) / den, k6 = (vp2 - vs2) / den;
+    const int ngroups = (A.n_gh + kGroupNodes - 1) / kGroupNodes;
+    const int klo = max(1, llo - 1), khi = lhi + 1;
+    const int slot = lane;
+    LaneChild Cu;
+    bool hasmom = false, is_stat = false;
+    for (int kc0 = klo; kc0 <= khi; kc0 += EBEM_LEVEL_KC) {
+        const int kc1 = min(khi, kc0 + EBEM_LEVEL_KC - 1), nk = kc1 - kc0 + 1;
+        for (int x = lane; x < 7 * EBEM_LEVEL_KC; x += 32) (&Ls.acc[0][0])[x] = 0.0;
+        for (int grp = 0; grp < ngroups; grp++) {
+            const int g0 = kGroupNodes * grp, gn = min(kGroupNodes, A.n_gh - g0);
+            if (ngroups > 1 || kc0 == klo) {
+                // children of outer nodes [g0, g0 + gn): slot = 3 (g - g0) + child
+                __syncwarp();
+                Cu.live = false;
+                Cu.zeta = 0.0; Cu.sigma = 0.0; Cu.dMIN = 0.0; Cu.w = 0.0;
+                hasmom = false;
+                is_stat = false;
+                const int g = g0 + slot / 3, c = slot - 3 * (slot / 3);
+                if (slot < 3 * gn) {
+                    NodeW sp = A.nodes[(size_t)i * A.n_gh + g];
+                    NodeGeo G;
+                    node_geo(G, sp, F);
+                    Cu.zeta = G.zeta;
+                    Cu.sigma = G.sigma;
+                    Cu.dMIN = G.dMIN;
+                    Cu.w = sp.w;
+                    if (node_child_e(Cu.g, G, c)) {
+                        Cu.live = true;
+                        m_sincos(Cu.g.gamma, &Cu.sg, &Cu.cg);
+                    }
+                }
+                if (Cu.live) {
+                    const ChildE& gg = Cu.g;
+                    LevelCtx L0;
+                    L0.k5 = k5;
+                    L0.k6 = k6;
+                    const W4 w0 = origin_weights(Cu.zeta, L0);
+                    W.w0[0][slot] = w0.sc;
+                    W.w0[1][slot] = w0.in;
+                    W.w0[2][slot] = w0.mx;
+                    W.w0[3][slot] = w0.zz;
+                    W.amax[slot] = gg.amax;
+                    W.F[slot] = gg.F;
+                    W.cbp[slot] = gg.cb * gg.ct + gg.sb * gg.st;     // cos(beta - theta_V1)
+                    W.sbp[slot] = gg.sb * gg.ct - gg.cb * gg.st;     // sin(beta - theta_V1)
+                    W.zeta[slot] = Cu.zeta;
+                    W.zs[slot] = Cu.zeta * Cu.sigma;
+                    W.scale[slot] = Cu.w * gg.sgnC;
+                    if (MIXED) {
+                        W.Ff[slot] = (float)W.F[slot];
+                        W.cbpf[slot] = (float)W.cbp[slot];
+                        W.sbpf[slot] = (float)W.sbp[slot];
+                        W.zetaf[slot] = (float)W.zeta[slot];
+                        W.zsf[slot] = (float)W.zs[slot];
+                        W.scalef[slot] = (float)W.scale[slot];
+                    }
+                }
+            }
+            __syncwarp();
+            for (int k = kc0; k <= kc1; k++) {
+                if (!level_wanted(A, cls, k, llo, lhi)) continue;
+                const double t = k * A.dt;
+                LevelCtx L;
+                L.t2 = t * t;
+                L.RP = A.velP * t;
+                L.RS = A.velS * t;
+                L.k1 = k1;
+                L.k5 = k5;
+                L.k6 = k6;
+                double S = 0.0, T[6] = {0, 0, 0, 0, 0, 0};
+                Piece pc[3];
+                int np = 0, nsubs[3];
+                double hs[3];
+                int nn = 0;
+                // decision phase (per child)
+                int type = T_NONE;
+                double rhoP = -1.0, rhoS = -1.0;
+                if (Cu.live && !is_stat) type = classify(Cu.zeta, L.RP, L.RS, Cu.dMIN, rhoP, rhoS);
+                // no child at work at this level (about half the levels of a pair's
+                // band: the null test's distance bounds are conservative): F is the
+                // sum of the static children, zero when there are none
+                if (EBEM_LEVEL_SKIP_IDLE && __ballot_sync(0xffffffffu, type != T_NONE) == 0u) {
+                    if (__ballot_sync(0xffffffffu, is_stat) != 0u) {
+                        double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                        if (is_stat) {
+#pragma unroll
+                            for (int e = 0; e < 7; e++) v[e] = W.sv[e][slot];
+                        }
+                        const double tot = warp_reduce_scatter8(v, lane);
+                        const int e = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+                        if ((lane & 3) == 0 && e < 7) Ls.acc[e][k - kc0] += tot;
+                    }
+                    continue;
+                }
+                AccE Ac = {0, 0, 0, 0, 0, 0, 0};
+                int full = 0;
+                if (type != T_NONE) {
+                    W4 w0;
+                    w0.sc = W.w0[0][slot];
+                    w0.in = W.w0[1][slot];
+                    w0.mx = W.w0[2][slot];
+                    w0.zz = W.w0[3][slot];
+                    child_decide(Ac, pc, np, full, Cu, L, rhoP, rhoS, type, w0, W.amax[slot]);
+                }
+                // whole-range moments, computed by the whole warp once per child
+                const bool need = full && !hasmom;
+                unsigned mm = __ballot_sync(0xffffffffu, need);
+                while (mm) {
+                    const int b = __ffs(mm) - 1;
+                    mm &= mm - 1;
+                    const double Fb = __shfl_sync(0xffffffffu, Cu.g.F, b), cbb = __shfl_sync(0xffffffffu, Cu.g.cb, b);
+                    const double sbb = __shfl_sync(0xffffffffu, Cu.g.sb, b), zb = __shfl_sync(0xffffffffu, Cu.zeta, b);
+                    const double s1b = __shfl_sync(0xffffffffu, Cu.g.s1, b), s0b = __shfl_sync(0xffffffffu, Cu.g.s0, b);
+                    double m[16];
+                    moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx, glw);
+                    m[14] = 0.0;
+                    m[15] = 0.0;
+                    const double tot = warp_reduce_scatter16(m, lane);
+                    const int e = scatter16_index(lane);
+                    if (!(lane & 1) && e < 14) W.mom[e][b] = tot;
+                }
+                __syncwarp();
+                if (need) hasmom = true;
+                const double zs = Cu.zeta * Cu.sigma;
+                if (full & 1) apply_moments(Ac, W, slot, true, L, zs);
+                if (full & 2) apply_moments(Ac, W, slot, false, L, zs);
+                if (type != T_NONE) {
+                    double Sc = 0.0, Tc[6] = {0, 0, 0, 0, 0, 0};
+                    child_to_plane(Sc, Tc, Ac, Cu.g, Cu.w * Cu.g.sgnC);
+                    S += Sc;
+#pragma unroll
+                    for (int e = 0; e < 6; e++) T[e] += Tc[e];
+                    // inside the S front with its whole edge (only the full S piece):
+                    // level-independent from now on (the fronts only grow)
+                    if (type == T_SP_SP && full == 2 && np == 0) {
+                        W.sv[0][slot] = Sc;
+#pragma unroll
+                        for (int e = 0; e < 6; e++) W.sv[1 + e][slot] = Tc[e];
+                        is_stat = true;
+                    }
+                } else if (is_stat) {
+                    S += W.sv[0][slot];
+#pragma unroll
+                    for (int e = 0; e < 6; e++) T[e] += W.sv[1 + e][slot];
+                }
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    nsubs[q] = 0;
+                    hs[q] = 0.0;
+                    if (q < np) {
+                        double len = pc[q].shi - pc[q].slo;
+                        int ns = (int)ceil(len * (1.0 / EBEM_EDGE_H));
+                        ns = max(1, min(ns, 4096));
+                        nsubs[q] = ns;
+                        hs[q] = len / ns;
+                        nn += 10 * ns;
+                    }
+                }
+                // partial edge pieces of all children -> per-warp list
+                int totp, totn;
+                int pb = warp_excl_scan(np, lane, totp);
+                int o = warp_excl_scan(nn, lane, totn);
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    if (q < np) {
+                        W.slo[pb] = pc[q].slo;
+                        W.h[pb] = hs[q];
+                        W.off[pb] = o;
+                        W.who[pb] = slot | (pc[q].pterm ? 64 : 0);
+                        o += 10 * nsubs[q];
+                        pb++;
+                    }
+                }
+                if (lane == 31) W.off[totp] = totn;
+                __syncwarp();
+                // all lanes: Gauss-Legendre nodes of the list, plane frame
+                int pp = 0;
+                if (MIXED) {
+                    float Sf = 0.0f, Tf[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                    const float fk1 = (float)L.k1, ft2 = (float)L.t2, fk5 = (float)L.k5, fk6 = (float)L.k6;
+                    for (int idx = lane; idx < totn; idx += 32) {
+                        while (idx >= W.off[pp + 1]) pp++;
+                        const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
+                        const double h = W.h[pp];
+                        const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
+                        const int who = W.who[pp], cl = who & 63;
+                        edge_node_f32(Sf, Tf, s, (float)(0.5 * h * glw[q]), W.Ff[cl], W.cbpf[cl], W.sbpf[cl],
+                                      W.zetaf[cl], W.zsf[cl], W.scalef[cl], (who & 64) != 0, fk1, ft2, fk5, fk6);
+                    }
+                    S += (double)Sf;
+#pragma unroll
+                    for (int e = 0; e < 6; e++) T[e] += (double)Tf[e];
+                    totn = 0;    // the FP64 loop below has nothing left to do
+                }
+                for (int idx = lane; idx < totn; idx += 32) {
+                    while (idx >= W.off[pp + 1]) pp++;
+                    const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
+                    const double h = W.h[pp];
+                    const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
+                    const int who = W.who[pp], cl = who & 63;
+                    double sech, th;
+                    Rad v;
+                    edge_point(s, W.F[cl], W.zeta[cl], sech, th, v);
+                    const double cbq = W.cbp[cl], sbq = W.sbp[cl];
+                    const double cq = th * cbq + sech * sbq, sq = sech * cbq - th * sbq;
+                    W4 w = weigh(v, (who & 64) != 0, L);
+                    const double f = 0.5 * h * glw[q] * sech * W.scale[cl];
+                    const double fin = f * w.in, fmx = -W.zs[cl] * f * w.mx;
+                    S += f * w.sc;
+                    T[0] += fin * cq * cq;
+                    T[1] += fin * sq * cq;
+                    T[2] += fin * sq * sq;
+                    T[3] += fmx * cq;
+                    T[4] += fmx * sq;
+                    T[5] += f * w.zz;
+                }
+                __syncwarp();
+                // warp sums; lane scatter8_lane(e) holds entry e (S, T11, T12, T22, T13, T23, T33)
+                double v[8] = {S, T[0], T[1], T[2], T[3], T[4], T[5], 0.0};
+                const double tot = warp_reduce_scatter8(v, lane);
+                const int e = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+                if ((lane & 3) == 0 && e < 7) Ls.acc[e][k - kc0] += tot;
+            }
+            __syncwarp();
+        }
+        // F(t_k) = (S I + C^T M C) / 2 in global axes, one lane per level
+        for (int kl = lane; kl < nk; kl += 32) {
+            const int k = kc0 + kl;
+            if (!level_wanted(A, cls, k, llo, lhi)) continue;
+            const double S = Ls.acc[0][kl];
+            double T[6];
+#pragma unroll
+            for (int e = 0; e < 6; e++) T[e] = Ls.acc[1 + e][kl];
+            double M[3][3] = {{T[0], T[1], T[3]}, {T[1], T[2], T[4]}, {T[3], T[4], T[5]}};
+            const double* Cm = F.C;
+            double MC[3][3];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int cc = 0; cc < 3; cc++)
+                    MC[r][cc] = M[r][0] * Cm[cc] + M[r][1] * Cm[3 + cc] + M[r][2] * Cm[6 + cc];
+            double Rm[3][3];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int cc = r; cc < 3; cc++)
+                    Rm[r][cc] = Cm[r] * MC[0][cc] + Cm[3 + r] * MC[1][cc] + Cm[6 + r] * MC[2][cc];
+            double2* dst = reinterpret_cast<double2*>(A.Fout + (frec + (k - A.kbase) * kstride) * 6);
+            dst[0] = make_double2(0.5 * (S + Rm[0][0]), 0.5 * Rm[0][1]);
+            dst[1] = make_double2(0.5 * Rm[0][2], 0.5 * (S + Rm[1][1]));
+            dst[2] = make_double2(0.5 * Rm[1][2], 0.5 * (S + Rm[2][2]));
+        }
+        __syncwarp();
+    }
+}
+
+template <int WPB, int MINB, bool MIXED>
+__global__ void __launch_bounds__(32 * WPB, MINB) sa_level_kernel(SAArgs A) {
+    extern __shared__ __align__(16) unsigned char level_smem[];
+    LevelShared* Lsh = reinterpret_cast<LevelShared*>(level_smem);
+    __shared__ double glx[10], glw[10];
+    __shared__ unsigned long long blk_count;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    LevelShared& Ls = Lsh[wib];
+    if (threadIdx.x < 10) {
+        const int k = threadIdx.x < 5 ? threadIdx.x : threadIdx.x - 5;
+        glx[threadIdx.x] = (threadIdx.x < 5 ? -1.0 : 1.0) * gl_x(k);
+        glw[threadIdx.x] = gl_w(k);
+    }
+    if (threadIdx.x == 0) blk_count = 0;
+    __syncthreads();
+    const long long NP = A.pairs ? A.npairs : (long long)A.nsrc * A.nj;
+    const long long nwarps = (long long)gridDim.x * WPB;
+    unsigned long long my_count = 0;
+    for (long long p = (long long)blockIdx.x * WPB + wib; p < NP; p += nwarps) {
+        int i, j;
+        if (A.pairs) {
+            const int2 pj = A.pairs[p];
+            i = pj.x;
+            j = pj.y;
+        } else {
+            i = A.src0 + (int)(p % A.nsrc);
+            j = A.j0 + (int)(p / A.nsrc);
+        }
+        level_pair<MIXED>(A, Ls, glx, glw, p, i, j, lane, my_count);
+    }
+    if (A.count) {
+        if (lane == 0 && my_count) atomicAdd(&blk_count, my_count);
+        __syncthreads();
+        if (threadIdx.x == 0 && blk_count) atomicAdd(A.count, blk_count);
+    }
+}
+
+template <int WPB, int MINB, bool MIXED>
+static int launch_level(const SAArgs& A, long long NN, int device, cudaStream_t s) {
+    const size_t smem = sizeof(LevelShared) * WPB;
+    // the dynamic shared memory opt-in, on every launch: it belongs to the
+    // context, which a caller may have reset since the last call
+    EBEM_CUDA_TRY(cudaFuncSetAttribute(sa_level_kernel<WPB, MINB, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    long long want = (NN + WPB - 1) / WPB;
+    long long cap = (long long)sms * MINB * 16;
+    unsigned blocks = (unsigned)(want < cap ? want : cap);
+    if (blocks == 0) blocks = 1;
+    sa_level_kernel<WPB, MINB, MIXED><<<blocks, 32 * WPB, smem, s>>>(A);
+    EBEM_CUDA_TRY(cudaGetLastError());
+    return EBEM_OK;
+}
 int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
                        cudaStream_t s, int diag_only, int mixed, const int2* pairs, long long npairs) {
@@ -634,7 +1123,7 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
 // non-null lags in [lag0, lag0 + nlag) need, and those lags.
 int launch_sa_fwarp(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc, int j0,
                     int nj, int kbase, int KL, double* d_F, int2* d_band, unsigned long long* d_count, int mixed,
-                    cudaStream_t s) {
+                    cudaStream_t s, const unsigned char* cls, int cls_want) {
     SAArgs A;
     A.geo = m.d_geo;
     A.nodes = m.d_nodes;
@@ -662,7 +1151,12 @@ int launch_sa_fwarp(const MeshData& m, const PhysParams& P, int n_gh, int lag0, 
     A.nj = nj;
     A.kbase = kbase;
     A.KL = KL;
+    A.cls = cls;
+    A.cls_want = cls_want;
     const long long NN = (long long)nsrc * nj;
+    if (EBEM_LEVEL_GROUPED || 3 * n_gh > 64 || cls)
+        return mixed ? launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, true>(A, NN, m.device, s)
+                     : launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s);
     if (3 * n_gh <= 32)
         return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
                      : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
@@ -670,6 +1164,86 @@ int launch_sa_fwarp(const MeshData& m, const PhysParams& P, int n_gh, int lag0, 
         return mixed ? launch_warp<2, 2, EBEM_WARP2_MINB, true>(A, NN, m.device, s)
                      : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
     return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+}
+
+// Blocks of an explicit list of (source, field) pairs at every lag [0, nlag)
+// with the outer rule in m.d_nodes (n_gh nodes per triangle, composite or
+// not): out[(p nlag + l) 6 + e], the 6 symmetric entries (11, 12, 13, 22, 23,
+// 33) of E_l, zero outside the pair's non-null lags.
+__global__ void pair_emit_kernel(const double* __restrict__ Fb, const int2* __restrict__ band, long long np, int nlag,
+                                 int KL, double c4, double* __restrict__ out) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= np * nlag) return;
+    const long long p = t / nlag;
+    const int l = (int)(t - p * nlag);
+    const int2 b = band[p];
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (b.x >= 0 && l >= b.x && l <= b.y) {
+        // level k of pair p at (p KL + k - 1) 6 (kbase = 1); F_0 = 0
+        const double* rec = Fb + p * KL * 6;
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+            const double a1 = rec[l * 6 + e];
+            const double a0 = (l >= 1) ? rec[(l - 1) * 6 + e] : 0.0;
+            const double am = (l >= 2) ? rec[(l - 2) * 6 + e] : 0.0;
+            const double x = ((a1 + (-2.0) * a0) + am) / c4;
+            v[e] = (fabs(x) < 1.0e-14) ? 0.0 : x;
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < 6; e++) out[t * 6 + e] = v[e];
+}
+
+int launch_sa_pair_blocks(const MeshData& m, const PhysParams& P, int n_gh, const int2* d_pairs, long long npairs,
+                          int nlag, double* d_out, cudaStream_t s) {
+    if (npairs <= 0) return EBEM_OK;
+    const int KL = nlag;                          // levels 1 .. nlag
+    const long long chunk = std::max<long long>(1, ((long long)256 << 20) / ((long long)KL * 48 + 8));
+    const long long np0 = std::min(npairs, chunk);
+    double* Fb = nullptr;
+    if (ws_malloc(&Fb, (size_t)np0 * KL * 48 + (size_t)np0 * sizeof(int2), s) != cudaSuccess)
+        return fail(EBEM_ERR_NOMEM, "pair-block workspace allocation failed");
+    int2* band = reinterpret_cast<int2*>(reinterpret_cast<unsigned char*>(Fb) + (size_t)np0 * KL * 48);
+    int rc = EBEM_OK;
+    for (long long q0 = 0; q0 < npairs && rc == EBEM_OK; q0 += np0) {
+        const long long nq = std::min(np0, npairs - q0);
+        SAArgs A;
+        A.geo = m.d_geo;
+        A.nodes = m.d_nodes;
+        A.N = m.nt;
+        A.n_gh = n_gh;
+        A.velP = P.velP;
+        A.velS = P.velS;
+        A.dt = P.dt;
+        A.c4pirho = 4 * kPi * P.rho;
+        A.lag0 = 0;
+        A.nlag = nlag;
+        A.src0 = 0;
+        A.nsrc = m.nt;
+        A.diag_only = 0;
+        A.E = nullptr;
+        A.ld = 0;
+        A.ld_lag = 0;
+        A.accumulate = 0;
+        A.count = nullptr;
+        A.pairs = d_pairs + q0;
+        A.npairs = nq;
+        A.Fout = Fb;
+        A.band = band;
+        A.j0 = 0;
+        A.nj = 0;
+        A.kbase = 1;
+        A.KL = KL;
+        rc = launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, nq, m.device, s);
+        if (rc) break;
+        const long long nt = nq * nlag;
+        pair_emit_kernel<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(Fb, band, nq, nlag, KL, 4 * kPi * P.rho,
+                                                                     d_out + q0 * nlag * 6);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, std::string("pair blocks: ") + cudaGetErrorString(e));
+    }
+    ws_free(Fb, s);
+    return rc;
 }
 
 // Banded output: all lags [0, L) of every pair, written into the band

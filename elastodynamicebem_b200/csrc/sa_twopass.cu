@@ -59,15 +59,21 @@ void profile_read(double ms[2], long long n[2], int reset) {
 // contiguous 768-byte run of a column (the three row stores of a column fill
 // it completely); the levels are read as 16-byte pairs.
 __global__ void __launch_bounds__(128) sa_emit_kernel(const double* __restrict__ Fb, const int2* __restrict__ band,
-                                                      int nsrc, int j0, int KL, int kbase, int lag0, double c4,
+                                                      int nsrc, int j0, int KL, int kbase, int lag0, int nlag, double c4,
                                                       double* __restrict__ E, size_t ld, size_t ld_lag,
-                                                      int accumulate) {
+                                                      int accumulate, const unsigned char* __restrict__ cls,
+                                                      int cls_want) {
     const int ii = blockIdx.x * blockDim.x + threadIdx.x;
     if (ii >= nsrc) return;
     const int jj = blockIdx.y, q = blockIdx.z, l = lag0 + q;
     const int2 b = band[(long long)jj * nsrc + ii];
+    const bool inband = b.x >= 0 && l >= b.x && l <= b.y;
+    if (cls) {
+        // one class of a per-(pair, lag) class array (sources = all triangles)
+        if (inband ? cls[((long long)(j0 + jj) * nsrc + ii) * nlag + q] != cls_want : cls_want != 0) return;
+    }
     double v[6] = {0, 0, 0, 0, 0, 0};
-    if (b.x >= 0 && l >= b.x && l <= b.y) {
+    if (inband) {
         const long long rec = (long long)jj * KL * nsrc + ii;          // record of level kbase
         const long long ks = nsrc;                                       // records per level
         double f1[6], f0[6] = {0, 0, 0, 0, 0, 0}, fm[6] = {0, 0, 0, 0, 0, 0};
@@ -106,7 +112,8 @@ __global__ void __launch_bounds__(128) sa_emit_kernel(const double* __restrict__
 
 int launch_sa_twopass(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                       double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count, int mixed,
-                      cudaStream_t s) {
+                      cudaStream_t s, const unsigned char* cls, int cls_want) {
+    if (cls && (src0 != 0 || nsrc != m.nt)) return fail(EBEM_ERR_INVALID, "a class array needs all source rows");
     if (m.nt > 65535 || nlag > 65535) return fail(EBEM_ERR_INVALID, "mesh or lag window too large for one launch");
     const int kbase = std::max(1, lag0 - 1);
     const int KL = lag0 + nlag + 1 - kbase;           // levels kbase .. lag0 + nlag
@@ -136,12 +143,13 @@ int launch_sa_twopass(const MeshData& m, const PhysParams& P, int n_gh, int lag0
     mark();
     for (int j0 = 0; j0 < m.nt && rc == EBEM_OK; j0 += cols) {
         const int nj = std::min(cols, m.nt - j0);
-        rc = launch_sa_fwarp(m, P, n_gh, lag0, nlag, src0, nsrc, j0, nj, kbase, KL, Fb, band, d_count, mixed, s);
+        rc = launch_sa_fwarp(m, P, n_gh, lag0, nlag, src0, nsrc, j0, nj, kbase, KL, Fb, band, d_count, mixed, s, cls,
+                             cls_want);
         if (rc) break;
         mark();
         dim3 grid((unsigned)((nsrc + 127) / 128), (unsigned)nj, (unsigned)nlag);
-        sa_emit_kernel<<<grid, 128, 0, s>>>(Fb, band, nsrc, j0, KL, kbase, lag0, 4 * kPi * P.rho, d_E, ld, ld_lag,
-                                            accumulate);
+        sa_emit_kernel<<<grid, 128, 0, s>>>(Fb, band, nsrc, j0, KL, kbase, lag0, nlag, 4 * kPi * P.rho, d_E, ld,
+                                            ld_lag, accumulate, cls, cls_want);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, std::string("emission kernel: ") + cudaGetErrorString(e));
         mark();

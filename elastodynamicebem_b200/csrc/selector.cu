@@ -1,17 +1,21 @@
 // Learned quadrature selector: a small MLP (12 -> 64 -> 64 -> 4, ReLU,
-// softmax, FP32) predicts, for each (source, field) pair, the cheapest outer
-// Gauss-Hammer rule (3, 7, 12 or 19 nodes) whose blocks agree with the
-// maximal rule within a tolerance; below a confidence threshold it falls back
-// to the maximal rule.  No counterpart in the reference (which uses one rule
-// for all pairs, BEMenerg_setupCore.m:13-28).
+// softmax, FP32) predicts, for each (source, field, lag), which of four outer
+// rules -- a Gauss-Hammer order on a number of congruent sub-triangles of the
+// source triangle (GaussHammerComposite.m), given by the caller -- assembles
+// that block; below a confidence threshold it falls back to the last
+// (maximal) rule.  No counterpart in the reference (which uses one rule for
+// all pairs and lags, BEMenerg_setupCore.m:13-28).
 //
-// Everything runs in hand-written kernels: pair features, convergence labels
-// from the plain assembly at the four rules, mini-batch forward/backward with
-// the weight gradients as per-block contractions over the batch, Adam, and
-// inference.  The networks' GEMMs are tiny (<= 64 x 64 per sample); they run
-// on the FP32 pipes, which keep a whole epoch over 2e5 samples in
-// milliseconds.
+// Everything runs in hand-written kernels: per-(pair, lag) features, labels
+// from the plain method's convergence (the blocks of sampled pairs at the four
+// rules, the smallest rule within a tolerance of the maximal one),
+// mini-batch forward/backward with the weight gradients as per-block
+// contractions over the batch, Adam, inference over every non-null (pair,
+// lag) of a mesh, and the assembly of each class's lags with its rule.  The
+// network's GEMMs are tiny (<= 64 x 64 per sample); they run on the FP32
+// pipes.
 #include "ebem_internal.h"
+#include "sa_pair.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -24,20 +28,24 @@ constexpr int kF = 12, kH = 64, kC = 4;
 constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kH * kF, kOffW2 = kOffB1 + kH, kOffB2 = kOffW2 + kH * kH,
               kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kC * kH, kParams = kOffB3 + kC;
 static_assert(kParams == 5252, "parameter count");
-constexpr int kRules[kC] = {3, 7, 12, 19};
 
 // ---------------------------------------------------------------------------
-// features of pair (i source, j field), all O(1):
-//  0 log(d/h_j)  1 log(d/h_i)  2 gap/h_j (clipped)  3 log(h_i/h_j)  4 |n_i.n_j|
-//  5 |n_j.(c_i-c_j)|/d  6 |n_i.(c_i-c_j)|/d  7 log(c_P dt/h_j)  8 log(c_S dt/h_j)
-//  9 c_P/c_S - 1  10 same triangle  11 area_j/h_j^2
-// d = centroid distance (at least h_j/20), h = longest edge.
-__device__ void pair_features(float f[kF], const TriGeom& Ti, const TriGeom& Tj, bool same, double velP, double velS,
-                              double dt) {
+// features of (source i, field j, lag l), all O(1):
+//  0 log(d/h_j)  1 log(d/h_i)  2 gap/h_j (clipped, x 0.1)  3 log(h_i/h_j)
+//  4 |n_i.n_j|  5 |n_j.(c_i-c_j)|/d  6 |n_i.(c_i-c_j)|/d
+//  7 c_P l dt / r_min  8 c_S l dt / r_max  (x 0.1, clipped at 3)
+//  9 (c_P l dt - d)/h_j  10 (c_S l dt - d)/h_j  (x 0.1, clipped at +-3)
+// 11 log(c_S dt / h_j)
+// d = centroid distance (at least h_j/20), h = longest edge, r_min / r_max =
+// the null test's distance bounds d -/+ (h_i + h_j) (r_min at least h_j/20).
+__device__ void lag_features(float f[kF], const TriGeom& Ti, const TriGeom& Tj, int l, double velP, double velS,
+                             double dt) {
     const double v0 = Ti.ctr[0] - Tj.ctr[0], v1 = Ti.ctr[1] - Tj.ctr[1], v2 = Ti.ctr[2] - Tj.ctr[2];
     const double hj = Tj.maxL, hi = Ti.maxL;
     const double d = fmax(sqrt(v0 * v0 + v1 * v1 + v2 * v2), 0.05 * hj);
     const double gap = (d - hi - hj) / hj;
+    const double rmin = fmax(d - hi - hj, 0.05 * hj), rmax = d + hi + hj;
+    const double tP = velP * l * dt, tS = velS * l * dt;
     f[0] = (float)log(d / hj);
     f[1] = (float)log(d / hi);
     f[2] = (float)fmin(fmax(gap, -2.0), 20.0) * 0.1f;
@@ -45,57 +53,44 @@ __device__ void pair_features(float f[kF], const TriGeom& Ti, const TriGeom& Tj,
     f[4] = (float)fabs(Ti.n[0] * Tj.n[0] + Ti.n[1] * Tj.n[1] + Ti.n[2] * Tj.n[2]);
     f[5] = (float)(fabs(Tj.n[0] * v0 + Tj.n[1] * v1 + Tj.n[2] * v2) / d);
     f[6] = (float)(fabs(Ti.n[0] * v0 + Ti.n[1] * v1 + Ti.n[2] * v2) / d);
-    f[7] = (float)log(velP * dt / hj);
-    f[8] = (float)log(velS * dt / hj);
-    f[9] = (float)(velP / velS - 1.0);
-    f[10] = same ? 1.0f : 0.0f;
-    f[11] = (float)(Tj.area / (hj * hj));
+    f[7] = (float)fmin(0.1 * tP / rmin, 3.0);
+    f[8] = (float)fmin(0.1 * tS / rmax, 3.0);
+    f[9] = (float)fmin(fmax(0.1 * (tP - d) / hj, -3.0), 3.0);
+    f[10] = (float)fmin(fmax(0.1 * (tS - d) / hj, -3.0), 3.0);
+    f[11] = (float)log(velS * dt / hj);
 }
 
-__global__ void features_kernel(const TriGeom* __restrict__ geo, int N, double velP, double velS, double dt,
-                                float* __restrict__ out) {
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= (long long)N * N) return;
-    const int i = (int)(p % N), j = (int)(p / N);
+// Features of explicit samples (source, field, lag): samples[3 q + 0..2].
+__global__ void sample_features_kernel(const TriGeom* __restrict__ geo, const int* __restrict__ samples, long long n,
+                                       double velP, double velS, double dt, float* __restrict__ out) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int i = samples[3 * q], j = samples[3 * q + 1], l = samples[3 * q + 2];
     float f[kF];
-    pair_features(f, geo[i], geo[j], i == j, velP, velS, dt);
+    lag_features(f, geo[i], geo[j], l, velP, velS, dt);
 #pragma unroll
-    for (int k = 0; k < kF; k++) out[p * kF + k] = f[k];
+    for (int k = 0; k < kF; k++) out[q * kF + k] = f[k];
 }
 
-// max |E| over the whole array (non-negative doubles order like their bits)
-__global__ void absmax_kernel(const double* __restrict__ E, long long n, unsigned long long* out) {
-    double m = 0.0;
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-        m = fmax(m, fabs(E[k]));
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
-}
-
-// label of pair p: smallest rule whose blocks (all lags) differ from the
-// maximal rule's by at most tol * max|E_max|; else the maximal rule.
-__global__ void labels_kernel(const double* __restrict__ E0, const double* __restrict__ E1,
-                              const double* __restrict__ E2, const double* __restrict__ E3, int N, int L,
-                              const unsigned long long* __restrict__ scale_bits, double tol, int* __restrict__ labels) {
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= (long long)N * N) return;
-    const int i = (int)(p % N), j = (int)(p / N);
-    const double thr = tol * __longlong_as_double((long long)*scale_bits);
-    const size_t n3 = 3 * (size_t)N;
-    double err[3] = {0.0, 0.0, 0.0};
-    const double* Er[3] = {E0, E1, E2};
-    for (int l = 0; l < L; l++)
-        for (int c = 0; c < 3; c++)
-            for (int r = 0; r < 3; r++) {
-                const size_t idx = (size_t)l * n3 * n3 + (3 * (size_t)j + c) * n3 + 3 * (size_t)i + r;
-                const double ref = E3[idx];
-#pragma unroll
-                for (int q = 0; q < 3; q++) err[q] = fmax(err[q], fabs(Er[q][idx] - ref));
-            }
+// Label of each sample from its blocks at the kC rules (blocks[(c n + q) 6 +
+// e]): the smallest rule whose block differs from the maximal rule's by at
+// most tol * scale (tol * scale * scales[q] with per-sample scales) in every
+// entry; else the maximal rule.
+__global__ void labels_kernel(const double* __restrict__ blocks, long long n, double thr0,
+                              const double* __restrict__ scales, int* __restrict__ labels) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const double thr = scales ? thr0 * scales[q] : thr0;
+    const double* ref = blocks + ((size_t)(kC - 1) * n + q) * 6;
     int lab = kC - 1;
-    for (int q = 2; q >= 0; q--)
-        if (err[q] <= thr) lab = q;
-    labels[p] = lab;
+    for (int c = kC - 2; c >= 0; c--) {
+        const double* b = blocks + ((size_t)c * n + q) * 6;
+        double err = 0.0;
+#pragma unroll
+        for (int e = 0; e < 6; e++) err = fmax(err, fabs(b[e] - ref[e]));
+        if (err <= thr) lab = c;
+    }
+    labels[q] = lab;
 }
 
 // ---------------------------------------------------------------------------
@@ -245,105 +240,70 @@ __global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float*
     g[k] = 0.0f;
 }
 
-// Inference for every pair of a mesh: class of the largest probability, or
-// the maximal rule when that probability is below the threshold.
+// Inference for every non-null (pair, lag) of a mesh: cls[(j N + i) nlag + q]
+// for lag l = lag0 + q, the class of the largest probability, or the maximal
+// rule when that probability is below the threshold; 0 outside the pair's
+// non-null lags (nothing to assemble there).  One thread per pair walks its
+// lags; per-class counts of the non-null lags.
 __global__ void __launch_bounds__(128) infer_kernel(const float* __restrict__ params, const TriGeom* __restrict__ geo,
-                                                    int N, double velP, double velS, double dt, float threshold,
-                                                    int* __restrict__ classes) {
+                                                    int N, double velP, double velS, double dt, int lag0, int nlag,
+                                                    float threshold, unsigned char* __restrict__ cls,
+                                                    unsigned long long* __restrict__ counts) {
     __shared__ float w[kParams];
+    __shared__ unsigned long long cnt[kC];
     for (int k = threadIdx.x; k < kParams; k += blockDim.x) w[k] = params[k];
-    __syncthreads();
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= (long long)N * N) return;
-    const int i = (int)(p % N), j = (int)(p / N);
-    float x[kF], h1[kH], h2[kH], z[kC];
-    pair_features(x, geo[i], geo[j], i == j, velP, velS, dt);
-    mlp_forward(w, x, h1, h2, z);
-    float m = z[0];
-    int arg = 0;
-    for (int o = 1; o < kC; o++)
-        if (z[o] > m) { m = z[o]; arg = o; }
-    float den = 0.0f;
-    for (int o = 0; o < kC; o++) den += expf(z[o] - m);
-    const float pmax = 1.0f / den;
-    classes[p] = (pmax >= threshold) ? arg : kC - 1;
-}
-
-// Pair lists per class that keep the pair order of each tile of kSplit pairs
-// (so the assembly of a class walks the matrix in order): pass 1 counts the
-// classes of each tile, the host scans the counts, pass 2 writes each pair at
-// its tile's offset plus its rank among the tile's pairs of its class.
-constexpr int kSplit = 1024;
-
-__global__ void __launch_bounds__(kSplit) split_count_kernel(const int* __restrict__ classes, long long NN,
-                                                            unsigned* __restrict__ tile_counts) {
-    __shared__ unsigned cnt[kC];
     if (threadIdx.x < kC) cnt[threadIdx.x] = 0;
     __syncthreads();
-    const long long p = (long long)blockIdx.x * kSplit + threadIdx.x;
-    if (p < NN) atomicAdd(&cnt[classes[p]], 1u);
-    __syncthreads();
-    if (threadIdx.x < kC) tile_counts[(size_t)blockIdx.x * kC + threadIdx.x] = cnt[threadIdx.x];
-}
-
-__global__ void __launch_bounds__(kSplit) split_write_kernel(const int* __restrict__ classes, int N,
-                                                            const unsigned long long* __restrict__ tile_offsets,
-                                                            int2* __restrict__ lists) {
-    __shared__ unsigned wcnt[kSplit / 32][kC];
-    const long long NN = (long long)N * N;
-    const long long p = (long long)blockIdx.x * kSplit + threadIdx.x;
-    const int c = (p < NN) ? classes[p] : -1;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned rank = 0;
-#pragma unroll
-    for (int q = 0; q < kC; q++) {
-        const unsigned m = __ballot_sync(0xffffffffu, c == q);
-        if (c == q) rank = __popc(m & ((1u << lane) - 1u));
-        if (lane == 0) wcnt[warp][q] = __popc(m);
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < (long long)N * N) {
+        const int i = (int)(p % N), j = (int)(p / N);
+        int llo = -1, lhi = -2;
+        pair_band(geo[j], geo[i], velP, velS, dt, lag0, nlag, &llo, &lhi);
+        unsigned char* out = cls + p * nlag;
+        unsigned c_loc[kC] = {0, 0, 0, 0};
+        for (int q = 0; q < nlag; q++) {
+            const int l = lag0 + q;
+            int c = 0;
+            if (llo >= 0 && l >= llo && l <= lhi) {
+                float x[kF], h1[kH], h2[kH], z[kC];
+                lag_features(x, geo[i], geo[j], l, velP, velS, dt);
+                mlp_forward(w, x, h1, h2, z);
+                float m = z[0];
+                int arg = 0;
+                for (int o = 1; o < kC; o++)
+                    if (z[o] > m) { m = z[o]; arg = o; }
+                float den = 0.0f;
+                for (int o = 0; o < kC; o++) den += expf(z[o] - m);
+                c = (1.0f / den >= threshold) ? arg : kC - 1;
+                c_loc[c]++;
+            }
+            out[q] = (unsigned char)c;
+        }
+        for (int o = 0; o < kC; o++)
+            if (c_loc[o]) atomicAdd(&cnt[o], (unsigned long long)c_loc[o]);
     }
     __syncthreads();
-    if (c >= 0) {
-        unsigned before = 0;
-        for (int w = 0; w < warp; w++) before += wcnt[w][c];
-        const unsigned long long pos = tile_offsets[(size_t)blockIdx.x * kC + c] + before + rank;
-        lists[(size_t)c * NN + pos] = make_int2((int)(p % N), (int)(p / N));
-    }
+    if (threadIdx.x < kC && cnt[threadIdx.x]) atomicAdd(counts + threadIdx.x, cnt[threadIdx.x]);
 }
 
 // ---------------------------------------------------------------------------
 // host side
 
-int selector_features(const MeshData& m, const PhysParams& P, float* d_out, cudaStream_t s) {
-    const long long NN = (long long)m.nt * m.nt;
-    features_kernel<<<(unsigned)((NN + 127) / 128), 128, 0, s>>>(m.d_geo, m.nt, P.velP, P.velS, P.dt, d_out);
+int selector_features(const MeshData& m, const PhysParams& P, const int* d_samples, long long n, float* d_out,
+                      cudaStream_t s) {
+    if (n <= 0) return EBEM_OK;
+    sample_features_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(m.d_geo, d_samples, n, P.velP, P.velS, P.dt,
+                                                                        d_out);
     EBEM_CUDA_TRY(cudaGetLastError());
     return EBEM_OK;
 }
 
-int selector_labels(MeshData& m, const PhysParams& P, int L, double tol, int* d_labels, cudaStream_t s) {
-    const size_t n3 = 3 * (size_t)m.nt, per = n3 * n3 * L;
-    double* E[kC] = {nullptr, nullptr, nullptr, nullptr};
-    unsigned long long* d_scale = nullptr;
-    int rc = EBEM_OK;
-    for (int q = 0; q < kC && rc == EBEM_OK; q++)
-        if (cudaMalloc(&E[q], per * sizeof(double)) != cudaSuccess) { cudaGetLastError(); rc = fail(EBEM_ERR_NOMEM, "label assembly buffers"); }
-    if (rc == EBEM_OK && cudaMalloc(&d_scale, sizeof(unsigned long long)) != cudaSuccess) { cudaGetLastError(); rc = fail(EBEM_ERR_NOMEM, "alloc"); }
-    for (int q = 0; q < kC && rc == EBEM_OK; q++) {
-        rc = map_nodes(m, kRules[q], s);
-        if (!rc) rc = launch_sa_assemble(m, P, kRules[q], 0, L, 0, m.nt, E[q], n3, n3 * n3, 0, nullptr, s);
-    }
-    if (rc == EBEM_OK) {
-        cudaMemsetAsync(d_scale, 0, sizeof(unsigned long long), s);
-        absmax_kernel<<<296, 256, 0, s>>>(E[kC - 1], (long long)per, d_scale);
-        const long long NN = (long long)m.nt * m.nt;
-        labels_kernel<<<(unsigned)((NN + 127) / 128), 128, 0, s>>>(E[0], E[1], E[2], E[3], m.nt, L, d_scale, tol, d_labels);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, std::string("selector labels: ") + cudaGetErrorString(e));
-    }
-    for (int q = 0; q < kC; q++) if (E[q]) cudaFree(E[q]);
-    if (d_scale) cudaFree(d_scale);
-    return rc;
+int selector_labels(const double* d_blocks, long long n, double tol, double scale, const double* d_scales,
+                    int* d_labels, cudaStream_t s) {
+    if (n <= 0) return EBEM_OK;
+    labels_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(d_blocks, n, tol * scale, d_scales, d_labels);
+    EBEM_CUDA_TRY(cudaGetLastError());
+    return EBEM_OK;
 }
 
 static size_t grad_smem() { return sizeof(GradSmem); }
@@ -417,64 +377,54 @@ int selector_train(float* d_params, const float* d_feats, const int* d_labels, l
     return rc;
 }
 
-int selector_infer(const float* d_params, const MeshData& m, const PhysParams& P, float threshold, int* d_classes,
-                   cudaStream_t s) {
-    const long long NN = (long long)m.nt * m.nt;
-    infer_kernel<<<(unsigned)((NN + 127) / 128), 128, 0, s>>>(d_params, m.d_geo, m.nt, P.velP, P.velS, P.dt,
-                                                               threshold, d_classes);
-    EBEM_CUDA_TRY(cudaGetLastError());
-    return EBEM_OK;
-}
-
-int assemble_selected(MeshData& m, const PhysParams& P, const int* d_classes, int lag0, int nlag, double* d_E, int prec,
-                      long long* h_counts, cudaStream_t s) {
-    const long long NN = (long long)m.nt * m.nt;
-    const long long tiles = (NN + kSplit - 1) / kSplit;
-    unsigned* d_tc = nullptr;
-    unsigned long long* d_off = nullptr;
-    int2* lists = nullptr;
+int selector_infer(const float* d_params, const MeshData& m, const PhysParams& P, float threshold, int lag0, int nlag,
+                   unsigned char* d_cls, long long* h_counts, cudaStream_t s) {
+    unsigned long long* d_cnt = nullptr;
+    if (ws_malloc(&d_cnt, sizeof(unsigned long long) * kC, s) != cudaSuccess)
+        return fail(EBEM_ERR_NOMEM, "inference workspace allocation failed");
     int rc = EBEM_OK;
-    if (cudaMalloc(&d_tc, sizeof(unsigned) * tiles * kC) != cudaSuccess ||
-        cudaMalloc(&d_off, sizeof(unsigned long long) * tiles * kC) != cudaSuccess ||
-        cudaMalloc(&lists, sizeof(int2) * (size_t)NN * kC) != cudaSuccess) {
-        cudaGetLastError();
-        cudaFree(d_tc); cudaFree(d_off);
-        return fail(EBEM_ERR_NOMEM, "pair list allocation failed");
-    }
-    std::vector<unsigned> tc((size_t)tiles * kC);
-    std::vector<unsigned long long> off((size_t)tiles * kC);
-    unsigned long long total[kC] = {0, 0, 0, 0};
-    split_count_kernel<<<(unsigned)tiles, kSplit, 0, s>>>(d_classes, NN, d_tc);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(tc.data(), d_tc, sizeof(unsigned) * tc.size(), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaError_t e = cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * kC, s);
+    const long long NN = (long long)m.nt * m.nt;
     if (e == cudaSuccess) {
-        for (long long t = 0; t < tiles; t++)
-            for (int q = 0; q < kC; q++) {
-                off[(size_t)t * kC + q] = total[q];
-                total[q] += tc[(size_t)t * kC + q];
-            }
-        e = cudaMemcpyAsync(d_off, off.data(), sizeof(unsigned long long) * off.size(), cudaMemcpyHostToDevice, s);
-    }
-    if (e == cudaSuccess) {
-        split_write_kernel<<<(unsigned)tiles, kSplit, 0, s>>>(d_classes, m.nt, d_off, lists);
+        infer_kernel<<<(unsigned)((NN + 127) / 128), 128, 0, s>>>(d_params, m.d_geo, m.nt, P.velP, P.velS, P.dt, lag0,
+                                                                   nlag, threshold, d_cls, d_cnt);
         e = cudaGetLastError();
     }
-    if (e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, std::string("pair split: ") + cudaGetErrorString(e));
-    const size_t n3 = 3 * (size_t)m.nt;
-    for (int q = 0; q < kC && rc == EBEM_OK; q++) {
-        if (h_counts) h_counts[q] = (long long)total[q];
-        if (total[q] == 0) continue;
-        rc = map_nodes(m, kRules[q], s);
-        if (!rc)
-            rc = launch_sa_assemble(m, P, kRules[q], lag0, nlag, 0, m.nt, d_E, n3, n3 * n3, 0, nullptr, s, 0, prec,
-                                    lists + (size_t)q * NN, (long long)total[q]);
+    unsigned long long hc[kC] = {0, 0, 0, 0};
+    if (e == cudaSuccess && h_counts) {
+        e = cudaMemcpyAsync(hc, d_cnt, sizeof(hc), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        for (int c = 0; c < kC; c++) h_counts[c] = (long long)hc[c];
     }
-    if (rc == EBEM_OK && (e = cudaStreamSynchronize(s)) != cudaSuccess)
-        rc = fail(EBEM_ERR_CUDA, std::string("selected assembly: ") + cudaGetErrorString(e));
-    cudaFree(d_tc);
-    cudaFree(d_off);
-    cudaFree(lists);
+    if (e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, std::string("selector inference: ") + cudaGetErrorString(e));
+    ws_free(d_cnt, s);
+    return rc;
+}
+
+int assemble_selected(MeshData& m, const PhysParams& P, const int* h_rules, int nclass, const unsigned char* d_cls,
+                      int lag0, int nlag, double* d_E, int prec, long long* h_counts, cudaStream_t s) {
+    unsigned long long* d_cnt = nullptr;
+    if (ws_malloc(&d_cnt, sizeof(unsigned long long) * nclass, s) != cudaSuccess)
+        return fail(EBEM_ERR_NOMEM, "assembly workspace allocation failed");
+    int rc = EBEM_OK;
+    if (cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * nclass, s) != cudaSuccess)
+        rc = fail(EBEM_ERR_CUDA, "counter reset failed");
+    const size_t n3 = 3 * (size_t)m.nt;
+    // class 0 also writes the zeros outside every pair's non-null lags
+    for (int c = 0; c < nclass && rc == EBEM_OK; c++) {
+        rc = map_nodes_composite(m, h_rules[2 * c], h_rules[2 * c + 1], s);
+        if (!rc)
+            rc = launch_sa_twopass(m, P, h_rules[2 * c] * h_rules[2 * c + 1], lag0, nlag, 0, m.nt, d_E, n3, n3 * n3, 0,
+                                   d_cnt + c, prec, s, d_cls, c);
+    }
+    std::vector<unsigned long long> hc(nclass, 0ull);
+    if (rc == EBEM_OK && h_counts) {
+        cudaError_t e = cudaMemcpyAsync(hc.data(), d_cnt, sizeof(unsigned long long) * nclass, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(EBEM_ERR_CUDA, std::string("selected assembly: ") + cudaGetErrorString(e));
+        for (int c = 0; c < nclass; c++) h_counts[c] = (long long)hc[c];
+    }
+    ws_free(d_cnt, s);
     return rc;
 }
 

@@ -74,17 +74,22 @@ PROTOTYPES = {
     "ebem_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
                                   C.POINTER(C.c_longlong)]),
     "ebem_batch_destroy": (C.c_int, [C.c_void_p]),
+    "ebem_sa_pair_blocks": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_void_p, C.c_longlong,
+                                      C.c_int, C.c_void_p, C.c_void_p]),
     "ebem_selector_init": (C.c_int, [C.c_void_p, C.c_ulonglong]),
-    "ebem_selector_features": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_void_p, C.c_void_p]),
-    "ebem_selector_labels": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_double, C.c_void_p, C.c_void_p]),
+    "ebem_selector_features": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_void_p, C.c_longlong, C.c_void_p,
+                                         C.c_void_p]),
+    "ebem_selector_labels": (C.c_int, [C.c_void_p, C.c_longlong, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
     "ebem_selector_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p,
                                      C.c_void_p]),
     "ebem_selector_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_float,
                                       C.c_ulonglong, C.c_void_p, C.c_void_p]),
-    "ebem_selector_infer": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(ProblemC), C.c_float, C.c_void_p,
-                                      C.c_void_p]),
-    "ebem_assemble_sa_selected": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_void_p, C.c_int, C.c_int,
-                                            C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_longlong)]),
+    "ebem_selector_infer": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(ProblemC), C.c_float, C.c_int, C.c_int,
+                                      C.c_void_p, C.POINTER(C.c_longlong), C.c_void_p]),
+    "ebem_assemble_sa_selected": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.POINTER(C.c_int), C.c_int, C.c_void_p,
+                                            C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                            C.POINTER(C.c_longlong)]),
     "ebem_assemble_sa_ex": (C.c_int, [C.c_void_p, C.POINTER(ProblemC)] + [C.c_int] * 5 + [C.c_void_p, C.c_longlong,
                                       C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_longlong)]),
     "ebem_timemarch_sa_ex": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_int, C.c_int, C.c_int, C.c_void_p,

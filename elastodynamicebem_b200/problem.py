@@ -89,6 +89,19 @@ def sphere_workload(n_gh: int = 7, subdivisions: int = 3) -> Workload:
     return Workload(f"sphere_n{m.numberTriangles}", m, prm, n_gh, DATUM_RADIAL_SIN, pts, times)
 
 
+def graded_workload(nx: int = 32, ny: int = 64) -> Workload:
+    """Screen [-0.5,0.5]^2 graded toward the edges with exponent 2 (nx x ny
+    squares, 2 nx ny triangles: 4096 by default), rho=1, mu=1, lambda=2,
+    dt=0.0125, T=1 (80 steps), 7-point outer rule, g=(0,0,t^4 e^-2t);
+    displacement at 100 seeded points on z=0.3 at t_n, n=1..80."""
+    m = _mesh.screen_graded(nx, ny, 2.0)
+    prm = ProblemParams(1.0, 1.0, 2.0, 1.0, 80)
+    rng = np.random.default_rng(1)
+    pts = np.column_stack([rng.uniform(-0.5, 0.5, 100), rng.uniform(-0.5, 0.5, 100), np.full(100, 0.3)])
+    times = prm.dt * np.arange(1, prm.nT + 1)
+    return Workload(f"graded_n{m.numberTriangles}", m, prm, 7, DATUM_SCREEN_T4EXP, pts, times)
+
+
 # ---------------------------------------------------------------------------
 # direct formulation: the 1-D bar data of the reference and the bar workload
 

@@ -121,7 +121,8 @@ int ebem_mesh_info(const ebem_mesh* mesh, int* n_vertices, int* n_triangles);
 int ebem_mesh_derived(const ebem_mesh* mesh, double* normal, double* area, double* center, double* maxl);
 /* Device data the mesh handle holds: rules_cached bit k set when the mapped
  * outer-node table of rule k (1, 3, 7, 12, 19, 28 nodes) is cached, and the
- * device bytes held (geometry, cached tables, direct-formulation data).
+ * device bytes held (geometry, cached tables including composite rules,
+ * direct-formulation data).
  * No counterpart in the reference. */
 int ebem_mesh_cache_info(const ebem_mesh* mesh, int* rules_cached, long long* device_bytes);
 
@@ -221,38 +222,58 @@ int ebem_batch_info(const ebem_batch* batch, int* warps_per_block, int* pairs_pe
 int ebem_batch_destroy(ebem_batch* batch);
 
 /* Learned quadrature selector (no counterpart in the reference, which uses
- * one outer rule for all pairs, BEMenerg_setupCore.m:13-28).  A small MLP
- * (12 -> 64 -> 64 -> 4, ReLU, softmax, FP32; EBEM_SELECTOR_PARAMS floats:
- * W1[64][12], b1[64], W2[64][64], b2[64], W3[4][64], b3[4]) maps the 12
- * features of a (source, field) pair to one of the outer rules 3, 7, 12, 19
- * (class 0..3).  All buffers below are device buffers unless stated.
+ * one outer rule for every pair and lag, BEMenerg_setupCore.m:13-28).
+ * Outer rules are (n_gh, n_sub) pairs: the n_gh-node Gauss-Hammer rule on
+ * n_sub congruent sub-triangles of the source triangle (n_sub a square,
+ * GaussHammerComposite.m:1-55).  A small MLP (12 -> 64 -> 64 -> 4, ReLU,
+ * softmax, FP32; EBEM_SELECTOR_PARAMS floats: W1[64][12], b1[64],
+ * W2[64][64], b2[64], W3[4][64], b3[4]) maps the 12 features of a
+ * (source, field, lag) to one of four rules (class 0..3, class 3 the
+ * maximal one).  All buffers below are device buffers unless stated.
+ *   ebem_sa_pair_blocks  the plain method's blocks of explicit pairs
+ *              (pairs[2 p] = source, pairs[2 p + 1] = field) at lags
+ *              0..nlag-1 with rule (n_gh, n_sub): out[(p nlag + l) 6 + e],
+ *              the 6 symmetric entries 11, 12, 13, 22, 23, 33 of E_l, zero
+ *              outside the pair's non-null lags.
  *   _init      He-initialised parameters (host or device buffer).
- *   _features  N^2 x 12 features of every pair (pair p = field * N + source).
- *   _labels    N^2 classes from the plain method itself: the smallest rule
- *              whose blocks (all lags) differ from the 19-node rule's by at
- *              most tol * max|E| (else class 3); assembles the mesh four times.
+ *   _features  n x 12 features of samples[3 q .. 3 q + 2] = (source, field, lag).
+ *   _labels    labels of n samples from their blocks at the four rules
+ *              (blocks[(c n + q) 6 + e]): the smallest rule whose block
+ *              differs from the maximal rule's by at most tol * scale (times
+ *              scales[q] when the per-sample array is not NULL) in every
+ *              entry, else 3.
  *   _grad      gradient of the mean cross-entropy over n samples (+ loss).
  *   _train     Adam over shuffled mini-batches; losses (host, may be NULL)
  *              receives the full-set loss after each epoch.
- *   _infer     class of every pair, the maximal rule (3) where the largest
- *              probability is below threshold.
- * ebem_assemble_sa_selected assembles each pair with the rule of its class
- * (E as ebem_assemble_sa, device, every entry written); pairs_per_class (host,
- * 4 entries, may be NULL) receives the class sizes. */
+ *   _infer     class of every (pair, lag) of a mesh for lags lag0..lag0+nlag-1:
+ *              cls[(field N + source) nlag + l - lag0] (bytes); the maximal
+ *              rule where the largest probability is below threshold; 0 at
+ *              null lags.  counts (host, 4 entries, may be NULL): non-null
+ *              lags per class.
+ * ebem_assemble_sa_selected assembles every lag of every pair with the rule
+ * of its class, rules[2 c], rules[2 c + 1] (host, nclass pairs) for class c
+ * (E as ebem_assemble_sa, device, every entry written); counts (host, nclass
+ * entries, may be NULL) receives the non-null lags per class.  With every
+ * class byte 0 it is the plain assembly with rule (rules[0], rules[1]). */
 #define EBEM_SELECTOR_FEATURES 12
 #define EBEM_SELECTOR_CLASSES 4
 #define EBEM_SELECTOR_PARAMS 5252
+int ebem_sa_pair_blocks(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int n_sub, const int* pairs,
+                        long long npairs, int nlag, double* out, void* stream);
 int ebem_selector_init(float* params, unsigned long long seed);
-int ebem_selector_features(const ebem_mesh* mesh, const ebem_problem* prob, float* feats, void* stream);
-int ebem_selector_labels(const ebem_mesh* mesh, const ebem_problem* prob, double tol, int* labels, void* stream);
+int ebem_selector_features(const ebem_mesh* mesh, const ebem_problem* prob, const int* samples, long long n,
+                           float* feats, void* stream);
+int ebem_selector_labels(const double* blocks, long long n, double tol, double scale, const double* scales,
+                         int* labels, void* stream);
 int ebem_selector_grad(const float* params, const float* feats, const int* labels, long long n, float* grad,
                        float* loss, void* stream);
 int ebem_selector_train(float* params, const float* feats, const int* labels, long long n, int epochs, int batch,
                         float lr, unsigned long long seed, float* losses, void* stream);
 int ebem_selector_infer(const float* params, const ebem_mesh* mesh, const ebem_problem* prob, float threshold,
-                        int* classes, void* stream);
-int ebem_assemble_sa_selected(const ebem_mesh* mesh, const ebem_problem* prob, const int* classes, int lag0, int nlag,
-                              double* E, int prec, void* stream, long long* pairs_per_class);
+                        int lag0, int nlag, unsigned char* cls, long long* counts, void* stream);
+int ebem_assemble_sa_selected(const ebem_mesh* mesh, const ebem_problem* prob, const int* rules, int nclass,
+                              const unsigned char* cls, int lag0, int nlag, double* E, int prec, void* stream,
+                              long long* counts);
 
 /* ebem_assemble_sa_panel with a precision mode. */
 int ebem_assemble_sa_ex(const ebem_mesh* mesh, const ebem_problem* prob, int n_gh, int lag0, int nlag, int src0,

@@ -1,5 +1,6 @@
 """ORACLE — test infrastructure only.  CPU (numpy, float64) restatement of
-the learned quadrature selector's network and pair features, the checker for
+the learned quadrature selector's network, its (pair, lag) features and its
+convergence labels, the checker for
 the device kernels of elastodynamicebem_b200/csrc/selector.cu.  The selector
 has no counterpart in the reference.
 
@@ -44,24 +45,41 @@ def loss_and_grad(params, x, y):
     return loss, np.concatenate([g[name].ravel() for name, _ in SIZES])
 
 
-def features(mesh, prm):
-    """N^2 x 12 pair features (pair p = field * N + source), as selector.cu
-    defines them."""
-    N = mesh.numberTriangles
-    c, h, n, a = mesh.center, mesh.maxL, mesh.normal, mesh.area
-    i = np.tile(np.arange(N), N); j = np.repeat(np.arange(N), N)
+def lag_features(mesh, prm, samples):
+    """n x 12 features of samples (source, field, lag), as selector.cu
+    defines them (lag_features)."""
+    samples = np.asarray(samples)
+    i, j, l = samples[:, 0], samples[:, 1], samples[:, 2].astype(np.float64)
+    c, h, n = mesh.center, mesh.maxL, mesh.normal
     v = c[i] - c[j]
     d = np.maximum(np.linalg.norm(v, axis=1), 0.05 * h[j])
     gap = (d - h[i] - h[j]) / h[j]
-    f = np.zeros((N * N, F))
+    rmin = np.maximum(d - h[i] - h[j], 0.05 * h[j])
+    rmax = d + h[i] + h[j]
+    tP, tS = prm.velP * l * prm.dt, prm.velS * l * prm.dt
+    f = np.zeros((len(samples), F))
     f[:, 0] = np.log(d / h[j]); f[:, 1] = np.log(d / h[i])
     f[:, 2] = np.clip(gap, -2, 20) * 0.1
     f[:, 3] = np.log(h[i] / h[j])
     f[:, 4] = np.abs((n[i] * n[j]).sum(1))
     f[:, 5] = np.abs((n[j] * v).sum(1)) / d
     f[:, 6] = np.abs((n[i] * v).sum(1)) / d
-    f[:, 7] = np.log(prm.velP * prm.dt / h[j]); f[:, 8] = np.log(prm.velS * prm.dt / h[j])
-    f[:, 9] = prm.velP / prm.velS - 1
-    f[:, 10] = (i == j)
-    f[:, 11] = a[j] / h[j] ** 2
+    f[:, 7] = np.minimum(0.1 * tP / rmin, 3.0)
+    f[:, 8] = np.minimum(0.1 * tS / rmax, 3.0)
+    f[:, 9] = np.clip(0.1 * (tP - d) / h[j], -3.0, 3.0)
+    f[:, 10] = np.clip(0.1 * (tS - d) / h[j], -3.0, 3.0)
+    f[:, 11] = np.log(prm.velS * prm.dt / h[j])
     return f
+
+
+def labels(blocks, tol, scale, scales=None):
+    """Labels from blocks at the four rules ((4, n, 6)): the smallest rule
+    whose block is within tol * scale (times scales[q] when given) of the
+    maximal rule's in every entry."""
+    blocks = np.asarray(blocks)
+    err = np.abs(blocks[:-1] - blocks[-1][None]).max(axis=2)       # (3, n)
+    thr = tol * scale * (np.asarray(scales) if scales is not None else 1.0)
+    lab = np.full(blocks.shape[1], C - 1)
+    for c in range(C - 2, -1, -1):
+        lab[err[c] <= thr] = c
+    return lab

@@ -25,5 +25,23 @@ def test_oracle_gradient_matches_finite_differences():
 
 def test_features_finite_and_bounded():
     from elastodynamicebem_b200 import mesh, problem
-    f = S.features(mesh.icosphere(1), problem.ProblemParams(1, 1, 1, 1, 40))
+    m = mesh.icosphere(1)
+    rng = np.random.default_rng(3)
+    n = m.numberTriangles
+    samples = np.stack([rng.integers(0, n, 500), rng.integers(0, n, 500), rng.integers(0, 40, 500)], 1)
+    samples[:20, 1] = samples[:20, 0]                      # same-triangle pairs
+    f = S.lag_features(m, problem.ProblemParams(1, 1, 1, 1, 40), samples)
+    assert f.shape == (500, S.F)
     assert np.isfinite(f).all() and np.abs(f).max() < 50
+
+
+def test_labels_smallest_rule_within_tolerance():
+    rng = np.random.default_rng(4)
+    ref = rng.normal(size=(50, 6))
+    blocks = np.stack([ref + rng.normal(scale=s, size=ref.shape) for s in (1e-2, 1e-5, 1e-9)] + [ref])
+    lab = S.labels(blocks, 1e-6, 1.0)
+    assert (lab == 2).all()
+    lab = S.labels(blocks, 1e-3, 1.0)
+    assert (lab == 1).all()
+    blocks[:, 7] = blocks[3, 7]                            # every rule agrees on sample 7
+    assert S.labels(blocks, 0.0, 1.0)[7] == 0

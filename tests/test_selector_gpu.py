@@ -1,9 +1,9 @@
-"""Learned quadrature selector on the device: features and the network's
-gradient against the CPU restatement (oracle/selector_oracle.py), the
-convergence labels against the plain assemblies they come from, and a
-training run whose gain over the plain method is measured: time and
-time-marched density error of the selector-driven assembly against the plain
-assembly on the maximal (19-node) rule and on the 7-node rule."""
+"""Learned quadrature selector on the device: per-(pair, lag) features and
+the network's gradient against the CPU restatement
+(oracle/selector_oracle.py), the plain method's blocks with composite outer
+rules (GaussHammerComposite) against the dense assembly, the convergence
+labels, the assembly of each (pair, lag) on the rule of its class, and a
+training run whose gain is measured and asserted."""
 import os
 import sys
 
@@ -17,8 +17,6 @@ import selector_oracle as SO  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-TAU = 1e-3            # label tolerance, relative to max |E| of the maximal rule
-
 
 @pytest.fixture(scope="module")
 def ebem():
@@ -28,12 +26,28 @@ def ebem():
     return core
 
 
-def test_features_match_oracle(ebem):
+def _sphere80():
     from elastodynamicebem_b200 import mesh, problem
-    m, prm = mesh.icosphere(1), problem.ProblemParams(1.0, 1.0, 1.0, 1.0, 40)
+    return mesh.icosphere(1), problem.ProblemParams(1.0, 1.0, 1.0, 1.0, 40)
+
+
+def _sym(E, N, L):
+    """(N_src, N_fld, L, 6) symmetric entries of E[l][3i+a, 3j+b]."""
+    v = E.reshape(L, N, 3, N, 3).permute(1, 3, 0, 2, 4)
+    import torch
+    return torch.stack([v[..., 0, 0], v[..., 0, 1], v[..., 0, 2], v[..., 1, 1], v[..., 1, 2], v[..., 2, 2]], -1)
+
+
+def test_features_match_oracle(ebem):
+    import torch
+    m, prm = _sphere80()
     dm = ebem.DeviceMesh(m)
-    f = ebem.selector_features(dm, prm).cpu().numpy()
-    assert np.abs(f - SO.features(m, prm)).max() <= 1e-5
+    rng = np.random.default_rng(0)
+    N = m.numberTriangles
+    smp = np.stack([rng.integers(0, N, 2000), rng.integers(0, N, 2000), rng.integers(0, 41, 2000)], 1)
+    smp[:50, 1] = smp[:50, 0]
+    f = ebem.selector_features(dm, prm, torch.tensor(smp, dtype=torch.int32, device="cuda")).cpu().numpy()
+    assert np.abs(f - SO.lag_features(m, prm, smp)).max() <= 1e-5
 
 
 def test_gradient_matches_oracle(ebem):
@@ -50,48 +64,67 @@ def test_gradient_matches_oracle(ebem):
     assert np.linalg.norm(g - go) <= 1e-4 * np.linalg.norm(go)
 
 
-def test_labels_match_plain_assemblies(ebem):
+def test_labels_match_oracle(ebem):
     import torch
-    from elastodynamicebem_b200 import mesh, problem
-    m, prm = mesh.screen_uniform(4), problem.ProblemParams(1.0, 1.0, 2.0, 1.0, 20)
-    dm = ebem.DeviceMesh(m)
-    N = m.numberTriangles
-    lab = ebem.selector_labels(dm, prm, TAU).cpu().numpy()
-    L = ebem.num_blocks(dm, prm)
-    E = {r: ebem.assemble_sa(dm, prm, r, 0, L).clone().view(L, N, 3, N, 3) for r in (3, 7, 12, 19)}
-    scale = float(E[19].abs().max())
-    err = {r: (E[r] - E[19]).abs().amax(dim=(0, 2, 4)).cpu().numpy() for r in (3, 7, 12)}   # [i, j]
-    ref = np.full((N, N), 3)
-    for q, r in reversed(list(enumerate((3, 7, 12)))):
-        ref[err[r] <= TAU * scale] = q
-    assert np.array_equal(lab, ref.T.reshape(-1))       # pair p = j * N + i
+    rng = np.random.default_rng(2)
+    ref = rng.normal(size=(3000, 6))
+    scales = rng.choice([1e-2, 1e-5, 1e-8, 1e-11], size=(3, 3000, 1))
+    blocks = np.concatenate([ref[None] + rng.normal(size=(3, 3000, 6)) * scales, ref[None]])
+    sc = rng.uniform(0.1, 10.0, 3000)
+    for tol in (1e-4, 1e-7, 1e-10):
+        lab = ebem.selector_labels(torch.tensor(blocks, device="cuda"), tol, 2.0).cpu().numpy()
+        assert np.array_equal(lab, SO.labels(blocks, tol, 2.0))
+        lab = ebem.selector_labels(torch.tensor(blocks, device="cuda"), tol, 2.0, torch.tensor(sc)).cpu().numpy()
+        assert np.array_equal(lab, SO.labels(blocks, tol, 2.0, sc))
 
 
-def test_selected_assembly_per_class(ebem):
-    """Each pair is assembled on the rule of its class: one class everywhere
-    equals the plain assembly on that rule, and a mixed class map equals the
-    plain blocks of each pair's rule."""
+def test_composite_rules_pair_blocks_match_dense(ebem):
+    """The plain method with composite outer rules: the pair-list blocks equal
+    the dense assembly's, rule (7, 1) equals the ordinary 7-node assembly, and
+    refining the composite rule converges."""
     import torch
-    from elastodynamicebem_b200 import mesh, problem
-    m, prm = mesh.icosphere(1), problem.ProblemParams(1.0, 1.0, 1.0, 1.0, 40)
+    m, prm = _sphere80()
     dm = ebem.DeviceMesh(m)
-    N, L = m.numberTriangles, ebem.num_blocks(ebem.DeviceMesh(m), prm)
-    plain = {r: ebem.assemble_sa(dm, prm, r, 0, L).clone().view(L, N, 3, N, 3) for r in (3, 7, 12, 19)}
-    for q, r in enumerate((3, 7, 12, 19)):
-        cls = torch.full((N * N,), q, dtype=torch.int32, device="cuda")
-        E, counts = ebem.assemble_sa_selected(dm, prm, cls, 0, L)
-        assert counts[q] == N * N
-        assert float((E.clone().view(L, N, 3, N, 3) - plain[r]).norm() / plain[r].norm()) <= 1e-12
-    cls = torch.tensor(np.random.default_rng(2).integers(0, 4, N * N), dtype=torch.int32, device="cuda")
-    E, counts = ebem.assemble_sa_selected(dm, prm, cls, 0, L)
-    E = E.clone().view(L, N, 3, N, 3)
-    pick = cls.view(N, N).T.long()                        # [i, j] (pair p = j * N + i)
+    N, L = m.numberTriangles, ebem.num_blocks(dm, prm)
+    rng = np.random.default_rng(5)
+    pairs = torch.tensor(np.stack([rng.integers(0, N, 400), rng.integers(0, N, 400)], 1), dtype=torch.int32,
+                         device="cuda")
+    i, j = pairs[:, 0].long(), pairs[:, 1].long()
+    dense = {}
+    for n, sub in ((7, 1), (7, 4), (3, 16), (7, 16)):
+        E = ebem.assemble_sa_rule(dm, prm, n, sub, 0, L).clone()
+        dense[(n, sub)] = E
+        pb = ebem.sa_pair_blocks(dm, prm, n, sub, pairs, L)
+        ref = _sym(E, N, L)[i, j]
+        assert float((pb - ref).abs().max() / ref.abs().max()) <= 1e-13
+    E7 = ebem.assemble_sa(dm, prm, 7, 0, L)
+    assert float((dense[(7, 1)] - E7).abs().max() / E7.abs().max()) <= 1e-13
+    e1 = float((dense[(7, 1)] - dense[(7, 16)]).norm() / dense[(7, 16)].norm())
+    e4 = float((dense[(7, 4)] - dense[(7, 16)]).norm() / dense[(7, 16)].norm())
+    assert e4 < e1
+
+
+def test_selected_assembly_per_lag_class(ebem):
+    """Each (pair, lag) is assembled on the rule of its class: a random class
+    map equals, block by block, the plain assembly on each block's rule, and
+    the class counts add up to the non-null pair-lags."""
+    import torch
+    m, prm = _sphere80()
+    dm = ebem.DeviceMesh(m)
+    N, L = m.numberTriangles, ebem.num_blocks(dm, prm)
+    rules = ((7, 1), (3, 4), (7, 4), (12, 4))
+    plain = [ebem.assemble_sa_rule(dm, prm, n, sub, 0, L).clone().reshape(L, N, 3, N, 3) for n, sub in rules]
+    g = torch.Generator(device="cuda").manual_seed(3)
+    cls = torch.randint(0, 4, (N * N, L), dtype=torch.uint8, device="cuda", generator=g)
+    E, counts = ebem.assemble_sa_selected(dm, prm, cls, rules, 0, L)
+    E = E.clone().reshape(L, N, 3, N, 3)
+    pick = cls.view(N, N, L).permute(2, 1, 0)             # [l, i, j] (row = field * N + source)
     ref = torch.zeros_like(E)
-    for q, r in enumerate((3, 7, 12, 19)):
-        mask = (pick == q)[None, :, None, :, None]
-        ref = torch.where(mask, plain[r], ref)
-    assert float((E - ref).norm() / ref.norm()) <= 1e-12
-    assert sum(counts) == N * N
+    for c in range(4):
+        ref = torch.where((pick == c)[:, :, None, :, None], plain[c], ref)
+    assert float((E - ref).abs().max() / ref.abs().max()) <= 1e-13
+    _, nonnull = ebem.assemble_sa(dm, prm, 7, 0, L, count=True)
+    assert sum(counts) == nonnull
 
 
 def _timed(fn, reps=3):
@@ -108,57 +141,50 @@ def _timed(fn, reps=3):
 
 
 def test_trained_selector_gain(ebem):
-    """Train on pairs of screens and coarse spheres; use the network on a finer
-    sphere (not seen in training) and measure what it gains over the plain
-    method: assembly time and time-marched density error against the plain
-    assembly on the maximal rule (19 nodes) and on the 7-node rule."""
+    """Train on 200k seeded (pair, lag) samples of the configuration 1-4
+    meshes (labels from the plain method's convergence over the four rules),
+    then assemble configuration 2 (sphere of 1280 triangles) and a graded
+    screen with configuration 5's grading, time step and lags (1024
+    triangles, not among the training meshes) with the network's classes.
+    Asserted: the density and the post-processed displacement are within
+    1e-6 of the plain method on the maximal rule, and the selected assembly,
+    its four class passes included, costs at most 5 % more than that plain
+    assembly.  The gain is printed: it is small whatever the network does,
+    because the blocks that converge on a cheaper rule are those no
+    wavefront crosses, whose levels the plain kernel already passes over
+    cheaply (perfect labels gain 1.08x on the 320-triangle sphere)."""
     import torch
-    from elastodynamicebem_b200 import mesh, problem
-    train = [(mesh.screen_uniform(8), problem.ProblemParams(1.0, 1.0, 2.0, 1.0, 20)),
-             (mesh.screen_graded(6, 4), problem.ProblemParams(1.0, 1.0, 2.0, 1.0, 16)),
-             (mesh.icosphere(1), problem.ProblemParams(1.0, 1.0, 1.0, 1.0, 40)),
-             (mesh.icosphere(2), problem.ProblemParams(1.0, 1.0, 1.0, 1.0, 40))]
-    X, Y = [], []
-    for m, prm in train:
-        dm = ebem.DeviceMesh(m)
-        X.append(ebem.selector_features(dm, prm))
-        Y.append(ebem.selector_labels(dm, prm, TAU))
-    X, Y = torch.cat(X), torch.cat(Y)
-    perm = torch.randperm(X.shape[0], generator=torch.Generator().manual_seed(5)).cuda()
-    X, Y = X[perm].contiguous(), Y[perm].contiguous()
-    ntr = int(0.85 * X.shape[0])
+    from elastodynamicebem_b200 import problem
+    from elastodynamicebem_b200 import selector as S
+    X, Y = S.training_set(200_000)
+    n = X.shape[0]
+    ntr = int(0.9 * n)
     params = ebem.selector_init(seed=7)
     _, loss0 = ebem.selector_grad(params, X[:ntr], Y[:ntr])
-    losses = ebem.selector_train(params, X[:ntr], Y[:ntr], epochs=25, batch=512, lr=3e-3, seed=9)
+    losses = ebem.selector_train(params, X[:ntr], Y[:ntr], epochs=20, batch=512, lr=3e-3, seed=9)
     assert losses[-1] < 0.5 * loss0 and losses[-1] <= losses[0]
-    # held-out accuracy against the majority class
     _, lo_test = ebem.selector_grad(params, X[ntr:], Y[ntr:])
-    counts = torch.bincount(Y[ntr:].long(), minlength=4).float()
-    prior = counts / counts.sum()
-    base_loss = float(-(prior * torch.log(torch.clamp(prior, min=1e-12))).sum())
-    assert lo_test < base_loss
-    # gain on an unseen mesh: sphere of 1280 triangles, GH7 time and error for scale
-    w = problem.sphere_workload(7, 3)
-    dm = ebem.DeviceMesh(w.mesh)
-    L = ebem.num_blocks(dm, w.params)
-    classes = ebem.selector_infer(params, dm, w.params, 0.9)
-    buf = torch.empty((L, 3 * dm.N, 3 * dm.N), dtype=torch.float64, device="cuda")
-    t_sel, (E_sel, per_class) = _timed(lambda: ebem.assemble_sa_selected(dm, w.params, classes, 0, L, out=buf))
-    E_sel = E_sel.clone()
-    t19, E19 = _timed(lambda: ebem.assemble_sa(dm, w.params, 19, 0, L, out=buf))
-    E19 = E19.clone()
-    t7, E7 = _timed(lambda: ebem.assemble_sa(dm, w.params, 7, 0, L, out=buf))
-    E7 = E7.clone()
-    b = ebem.rhs(dm, w.params, 19, w.datum)
-    phi19 = ebem.march(E19, b)
-    phi_sel = ebem.march(E_sel, b)
-    phi7 = ebem.march(E7, ebem.rhs(dm, w.params, 7, w.datum))
-    err_sel = float((phi_sel - phi19).norm() / phi19.norm())
-    err7 = float((phi7 - phi19).norm() / phi19.norm())
-    print(f"\nselector on sphere N=1280: classes {per_class}; assembly {t_sel:.1f} ms vs GH19 {t19:.1f} ms "
-          f"({t19 / t_sel:.2f}x) and GH7 {t7:.1f} ms; density error vs GH19: selector {err_sel:.2e}, GH7 {err7:.2e}")
-    # What the network gains is measured and printed, not assumed: with the
-    # outer rules' slow convergence at the wavefronts it need not beat the
-    # plain rules (the measured trade-off is recorded with the design notes).
-    assert sum(per_class) == dm.N ** 2
-    assert np.isfinite(err_sel) and t_sel > 0
+    prior = torch.bincount(Y[ntr:].long(), minlength=4).double()
+    prior = prior / prior.sum()
+    assert lo_test < float(-(prior * torch.log(torch.clamp(prior, min=1e-12))).sum())
+    for w in (problem.sphere_workload(7, 3), problem.graded_workload(16, 32)):
+        dm = ebem.DeviceMesh(w.mesh)
+        L = ebem.num_blocks(dm, w.params)
+        n3 = 3 * dm.N
+        buf = torch.empty((L, n3, n3), dtype=torch.float64, device="cuda")
+        t_max, E = _timed(lambda: ebem.assemble_sa_rule(dm, w.params, *S.RULES[-1], 0, L, out=buf), reps=1)
+        b = ebem.rhs(dm, w.params, 7, w.datum)
+        phi_max = ebem.march(E, b)
+        t_sel, (E, counts) = _timed(lambda: S.assemble(params, dm, w.params, out=buf), reps=1)
+        phi_sel = ebem.march(E, b)
+        del E
+        u_max = ebem.pp_sa(dm, w.params, phi_max, w.points, w.times)
+        u_sel = ebem.pp_sa(dm, w.params, phi_sel, w.points, w.times)
+        err_d = float((phi_sel - phi_max).norm() / phi_max.norm())
+        err_u = float((u_sel - u_max).norm() / u_max.norm())
+        print(f"\nselector on {w.name}: non-null lags per class {counts}; assembly {t_sel:.1f} ms vs the maximal "
+              f"rule's {t_max:.1f} ms ({t_max / t_sel:.2f}x); density error {err_d:.2e}, displacement {err_u:.2e}")
+        assert err_d <= 1e-6 and err_u <= 1e-6
+        assert t_sel <= 1.05 * t_max
+        del buf
+        torch.cuda.empty_cache()
