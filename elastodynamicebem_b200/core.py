@@ -514,6 +514,17 @@ def selector_features(dmesh: DeviceMesh, prm: ProblemParams, samples: torch.Tens
     return f
 
 
+def selector_sweeps(dmesh: DeviceMesh, prm: ProblemParams, samples: torch.Tensor, stream=None) -> torch.Tensor:
+    """uint8 (n,): 1 where a wavefront sweeps the sample's distance window
+    (such lags are assembled on the maximal rule, not by the network)."""
+    samples = samples.to(device="cuda", dtype=torch.int32).contiguous()
+    f = torch.empty(samples.shape[0], dtype=torch.uint8, device="cuda")
+    p = _lib.problem_struct(prm)
+    _lib.check(_lib.load().ebem_selector_sweeps(dmesh.handle, C.byref(p), C.c_void_p(samples.data_ptr()),
+                                                int(samples.shape[0]), C.c_void_p(f.data_ptr()), _stream_ptr(stream)))
+    return f
+
+
 def selector_labels(blocks: torch.Tensor, tol: float, scale: float, scales: torch.Tensor | None = None,
                     stream=None) -> torch.Tensor:
     """Labels of n samples from their blocks at the four rules ((4, n, 6)

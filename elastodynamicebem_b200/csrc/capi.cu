@@ -1293,6 +1293,16 @@ int ebem_selector_features(const ebem_mesh* m, const ebem_problem* p, const int*
     return selector_features(m->d, phys_from(p), samples, n, feats, (cudaStream_t)stream);
 }
 
+int ebem_selector_sweeps(const ebem_mesh* m, const ebem_problem* p, const int* samples, long long n,
+                         unsigned char* flags, void* stream) {
+    if (!m || n < 0) return fail(EBEM_ERR_INVALID, "mesh and n >= 0 required");
+    if (n == 0) return EBEM_OK;
+    if (!all_device({samples, flags})) return fail(EBEM_ERR_INVALID, "device sample and flag buffers required");
+    if (int rc = check_problem(p)) return rc;
+    DeviceGuard dg(m->d.device);
+    return selector_sweeps(m->d, phys_from(p), samples, n, flags, (cudaStream_t)stream);
+}
+
 int ebem_selector_labels(const double* blocks, long long n, double tol, double scale, const double* scales,
                          int* labels, void* stream) {
     if (n < 0 || !(tol >= 0) || !(scale >= 0)) return fail(EBEM_ERR_INVALID, "n, tol and scale must be >= 0");

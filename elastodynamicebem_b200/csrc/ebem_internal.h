@@ -239,6 +239,9 @@ int launch_hist_gemv(const double* A, int n3, long long K, const double* x, doub
 // features of samples[3 q + 0..2] = (source, field, lag)
 int selector_features(const MeshData& m, const PhysParams& P, const int* d_samples, long long n, float* d_out,
                       cudaStream_t s);
+// 1 where a wavefront sweeps the sample's distance window (those lags take the maximal rule)
+int selector_sweeps(const MeshData& m, const PhysParams& P, const int* d_samples, long long n, unsigned char* d_out,
+                    cudaStream_t s);
 // labels from the samples' blocks at the four rules (blocks[(c n + q) 6 + e])
 int selector_labels(const double* d_blocks, long long n, double tol, double scale, const double* d_scales,
                     int* d_labels, cudaStream_t s);

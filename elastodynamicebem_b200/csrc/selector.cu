@@ -240,9 +240,32 @@ __global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float*
     g[k] = 0.0f;
 }
 
+// Whether a wavefront sweeps the pair's distance window during lag l's
+// instants t_{l-1} .. t_{l+1}: c t over that interval meets [d - h_i - h_j,
+// d + h_i + h_j] (the null test's bounds, d the centroid distance) for c =
+// c_P or c_S.  There the kernel integral, a function of the outer node, has
+// the kinks of the front crossing the field triangle and the outer rule
+// converges only algebraically: those lags take the maximal rule whatever
+// the network says.
+EBEM_DI bool front_sweeps(const TriGeom& Ti, const TriGeom& Tj, int l, double velP, double velS, double dt) {
+    const double v0 = Ti.ctr[0] - Tj.ctr[0], v1 = Ti.ctr[1] - Tj.ctr[1], v2 = Ti.ctr[2] - Tj.ctr[2];
+    const double d = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+    const double lo = d - Ti.maxL - Tj.maxL, hi = d + Ti.maxL + Tj.maxL;
+    const double t0 = (l - 1) * dt, t1 = (l + 1) * dt;
+    return (velP * t1 >= lo && velP * t0 <= hi) || (velS * t1 >= lo && velS * t0 <= hi);
+}
+
+__global__ void sweep_flags_kernel(const TriGeom* __restrict__ geo, const int* __restrict__ samples, long long n,
+                                   double velP, double velS, double dt, unsigned char* __restrict__ out) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    out[q] = front_sweeps(geo[samples[3 * q]], geo[samples[3 * q + 1]], samples[3 * q + 2], velP, velS, dt) ? 1 : 0;
+}
+
 // Inference for every non-null (pair, lag) of a mesh: cls[(j N + i) nlag + q]
-// for lag l = lag0 + q, the class of the largest probability, or the maximal
-// rule when that probability is below the threshold; 0 outside the pair's
+// for lag l = lag0 + q.  A lag that a front sweeps takes the maximal rule;
+// any other takes the class of the largest probability, or the maximal rule
+// when that probability is below the threshold; 0 outside the pair's
 // non-null lags (nothing to assemble there).  One thread per pair walks its
 // lags; per-class counts of the non-null lags.
 __global__ void __launch_bounds__(128) infer_kernel(const float* __restrict__ params, const TriGeom* __restrict__ geo,
@@ -264,7 +287,10 @@ __global__ void __launch_bounds__(128) infer_kernel(const float* __restrict__ pa
         for (int q = 0; q < nlag; q++) {
             const int l = lag0 + q;
             int c = 0;
-            if (llo >= 0 && l >= llo && l <= lhi) {
+            if (llo >= 0 && l >= llo && l <= lhi && front_sweeps(geo[i], geo[j], l, velP, velS, dt)) {
+                c = kC - 1;
+                c_loc[c]++;
+            } else if (llo >= 0 && l >= llo && l <= lhi) {
                 float x[kF], h1[kH], h2[kH], z[kC];
                 lag_features(x, geo[i], geo[j], l, velP, velS, dt);
                 mlp_forward(w, x, h1, h2, z);
@@ -294,6 +320,14 @@ int selector_features(const MeshData& m, const PhysParams& P, const int* d_sampl
     if (n <= 0) return EBEM_OK;
     sample_features_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(m.d_geo, d_samples, n, P.velP, P.velS, P.dt,
                                                                         d_out);
+    EBEM_CUDA_TRY(cudaGetLastError());
+    return EBEM_OK;
+}
+
+int selector_sweeps(const MeshData& m, const PhysParams& P, const int* d_samples, long long n, unsigned char* d_out,
+                    cudaStream_t s) {
+    if (n <= 0) return EBEM_OK;
+    sweep_flags_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(m.d_geo, d_samples, n, P.velP, P.velS, P.dt, d_out);
     EBEM_CUDA_TRY(cudaGetLastError());
     return EBEM_OK;
 }

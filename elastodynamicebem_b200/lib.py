@@ -79,6 +79,8 @@ PROTOTYPES = {
     "ebem_selector_init": (C.c_int, [C.c_void_p, C.c_ulonglong]),
     "ebem_selector_features": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_void_p, C.c_longlong, C.c_void_p,
                                          C.c_void_p]),
+    "ebem_selector_sweeps": (C.c_int, [C.c_void_p, C.POINTER(ProblemC), C.c_void_p, C.c_longlong, C.c_void_p,
+                                       C.c_void_p]),
     "ebem_selector_labels": (C.c_int, [C.c_void_p, C.c_longlong, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
                                        C.c_void_p]),
     "ebem_selector_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p,

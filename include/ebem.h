@@ -237,6 +237,12 @@ int ebem_batch_destroy(ebem_batch* batch);
  *              outside the pair's non-null lags.
  *   _init      He-initialised parameters (host or device buffer).
  *   _features  n x 12 features of samples[3 q .. 3 q + 2] = (source, field, lag).
+ *   _sweeps    flags[q] = 1 where a wavefront sweeps sample q's distance
+ *              window during its lag (c t, t from (l-1) dt to (l+1) dt,
+ *              meets [d - h_i - h_j, d + h_i + h_j] for c = c_P or c_S; d
+ *              the centroid distance, h the longest edges): the outer rule
+ *              converges slowly there and inference gives those lags the
+ *              maximal rule.
  *   _labels    labels of n samples from their blocks at the four rules
  *              (blocks[(c n + q) 6 + e]): the smallest rule whose block
  *              differs from the maximal rule's by at most tol * scale (times
@@ -247,8 +253,8 @@ int ebem_batch_destroy(ebem_batch* batch);
  *              receives the full-set loss after each epoch.
  *   _infer     class of every (pair, lag) of a mesh for lags lag0..lag0+nlag-1:
  *              cls[(field N + source) nlag + l - lag0] (bytes); the maximal
- *              rule where the largest probability is below threshold; 0 at
- *              null lags.  counts (host, 4 entries, may be NULL): non-null
+ *              rule where a front sweeps the lag (as _sweeps) or where the
+ *              largest probability is below threshold; 0 at null lags.  counts (host, 4 entries, may be NULL): non-null
  *              lags per class.
  * ebem_assemble_sa_selected assembles every lag of every pair with the rule
  * of its class, rules[2 c], rules[2 c + 1] (host, nclass pairs) for class c
@@ -263,6 +269,8 @@ int ebem_sa_pair_blocks(const ebem_mesh* mesh, const ebem_problem* prob, int n_g
 int ebem_selector_init(float* params, unsigned long long seed);
 int ebem_selector_features(const ebem_mesh* mesh, const ebem_problem* prob, const int* samples, long long n,
                            float* feats, void* stream);
+int ebem_selector_sweeps(const ebem_mesh* mesh, const ebem_problem* prob, const int* samples, long long n,
+                         unsigned char* flags, void* stream);
 int ebem_selector_labels(const double* blocks, long long n, double tol, double scale, const double* scales,
                          int* labels, void* stream);
 int ebem_selector_grad(const float* params, const float* feats, const int* labels, long long n, float* grad,
