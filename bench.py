@@ -40,16 +40,16 @@ FLOPS_PER_PAIR_INTEGRAL = 19_232.0
 FLOPS_PER_PAIR_INTEGRAL_REF_SCHEDULE = 53_560.0
 
 # DRAM bytes (read + write) of the dominant kernel, the level pass of the
-# two-pass assembly (sa_assemble_warp_kernel storing F(t_k) of every pair and
-# level): ncu on the sphere N=320 case (2,478,740 pair-integrals, one launch)
-# measured 13.16 MB read + 131.14 MB written; the writes are the stored levels,
-# which grow with the pair-integrals, so a launch's traffic is scaled by the
+# two-pass assembly (sa_level_kernel storing F(t_k) of every pair and level):
+# ncu on the sphere N=320 case (2,478,740 pair-integrals, one launch) measured
+# 12.75 MB read + 102.93 MB written; the writes are the stored levels, which
+# grow with the pair-integrals, so a launch's traffic is scaled by the
 # pair-integrals it processes.
-NCU_LEVEL_PASS_BYTES_N320 = 13.158656e6 + 131.140096e6
+NCU_LEVEL_PASS_BYTES_N320 = 12.745728e6 + 102.928896e6
 NCU_LEVEL_PASS_UNITS_N320 = 2_478_740
 
 
-KERNEL = "sa_assemble_warp_kernel (level pass)"
+KERNEL = "sa_level_kernel (level pass)"
 
 
 def log(*a):
@@ -217,6 +217,7 @@ def forms(core, problem, torch, w, dm, L, plain_rate):
 
     out["mixed"] = mixed_form(w.n_gh)
     out["mixed_gh12"] = mixed_form(12)
+    out["selector"] = selector_form(core, torch, w, dm, L, timed)
     inst = problem.batch_workload(count=64, seed=4)
     dms = [core.DeviceMesh(m) for _, m, _ in inst]
     prms = [p for _, _, p in inst]
@@ -240,6 +241,45 @@ def forms(core, problem, torch, w, dm, L, plain_rate):
     del outs
     torch.cuda.empty_cache()
     return out
+
+
+def selector_form(core, torch, w, dm, L, timed):
+    """The learned selector on the benchmark sphere: trained on 200k (pair,
+    lag) samples of the configuration 1-4 meshes, then the selected assembly
+    (FP64, and with the mixed form) against the plain assembly on the maximal
+    rule, with the density and displacement errors against the latter."""
+    from elastodynamicebem_b200 import selector as S
+    t0 = time.perf_counter()
+    X, Y = S.training_set(200_000)
+    params, losses = S.train(X, Y, epochs=20)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    n3 = 3 * dm.N
+    buf = torch.empty((L, n3, n3), dtype=torch.float64, device="cuda")
+    p = w.params
+    t_max = timed(lambda: core.assemble_sa_rule(dm, p, *S.RULES[-1], 0, L, out=buf), reps=1)
+    E = core.assemble_sa_rule(dm, p, *S.RULES[-1], 0, L, out=buf)
+    b = core.rhs(dm, p, 7, w.datum)
+    phi_max = core.march(E, b)
+    u_max = core.pp_sa(dm, p, phi_max, w.points, w.times)
+    t_inf = timed(lambda: core.selector_infer(params, dm, p, S.THRESHOLD, 0, L), reps=1)
+    cls, counts = core.selector_infer(params, dm, p, S.THRESHOLD, 0, L)
+    res = {"rules": [list(r) for r in S.RULES], "train_samples": int(X.shape[0]), "train_s": t_train,
+           "final_loss": float(losses[-1]), "lags_per_class": counts, "max_rule_ms": t_max, "inference_ms": t_inf}
+    for name, prec in (("fp64", core.PREC_FP64), ("mixed", core.PREC_MIXED)):
+        t = timed(lambda: core.assemble_sa_selected(dm, p, cls, S.RULES, 0, L, out=buf, prec=prec), reps=1)
+        E, _ = core.assemble_sa_selected(dm, p, cls, S.RULES, 0, L, out=buf, prec=prec)
+        phi = core.march(E, b)
+        u = core.pp_sa(dm, p, phi, w.points, w.times)
+        res[name] = {"assembly_ms": t, "speedup_vs_max_rule": t_max / t,
+                     "density_rel_err": float((phi - phi_max).norm() / phi_max.norm()),
+                     "displacement_rel_err": float((u - u_max).norm() / u_max.norm())}
+    res["scope"] = ("selector classes per (pair, lag) among the rules, lags a wavefront sweeps on the maximal "
+                    "rule; the batched launch takes one rule per plan, so selector + mixed is the combination "
+                    "measured on this mesh")
+    del buf, E, phi_max, cls
+    torch.cuda.empty_cache()
+    return res
 
 
 def workload_config(w, L: int, pairs: int, world: int) -> dict:
