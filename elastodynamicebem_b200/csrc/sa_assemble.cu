@@ -727,6 +727,7 @@ constexpr int kGroupNodes = 10;  // outer nodes per group: 30 children on 32 lan
 struct LevelShared {
     WarpShared<1> W;
     double acc[7][EBEM_LEVEL_KC];
+    double carry[2][6];          // direct output: F of the two levels before the chunk
 };
 
 // Whether level k is used by a lag of the wanted class (lags k-1, k, k+1 of
@@ -742,6 +743,18 @@ EBEM_DI bool level_wanted(const SAArgs& A, const unsigned char* cls, int k, int 
 // levels in A.Fout (record rec, level k at (rec + (k - kbase) kstride) 6):
 // field columns of a panel (rec = (j - j0) KL nsrc + i - src0, kstride =
 // nsrc) or an explicit pair list (rec = p KL, kstride = 1).
+// The dynamic shared memory opt-in of a kernel, before every launch that is
+// not being captured: it belongs to the context, which a caller may have
+// reset since the last call; a captured launch relies on the uncaptured one
+// before it (the batch plan runs its launch before capturing it).
+template <class K>
+static int opt_in_smem(K kernel, size_t smem, cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) return EBEM_OK;
+    EBEM_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return EBEM_OK;
+}
+
 template <bool MIXED>
 __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, const double* glx, const double* glw,
                                            long long p, int i, int j, int lane, unsigned long long& my_count) {
@@ -749,12 +762,33 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
     const TriGeom& F = A.geo[j];
     const TriGeom& Sg = A.geo[i];
     int llo = -1, lhi = -2;
-    pair_band(F, Sg, A.velP, A.velS, A.dt, A.lag0, A.nlag, &llo, &lhi);
+    long long bbase = 0;
+    if (A.Eb) {
+        // banded output: the band comes from the structure pass, so writes stay in the pair's blocks
+        const long long pb = (long long)(i - A.src0) * A.N + j;
+        bbase = A.boff[pb];
+        const int nb = (int)(A.boff[pb + 1] - bbase);
+        if (nb > 0) {
+            llo = A.blo[pb];
+            lhi = llo + nb - 1;
+        }
+    } else {
+        pair_band(F, Sg, A.velP, A.velS, A.dt, A.lag0, A.nlag, &llo, &lhi);
+    }
     const long long brec = A.pairs ? p : (long long)(j - A.j0) * A.nsrc + (i - A.src0);
     const long long frec = A.pairs ? p * A.KL : (long long)(j - A.j0) * A.KL * A.nsrc + (i - A.src0);
     const long long kstride = A.pairs ? 1 : A.nsrc;
-    if (lane == 0) A.band[brec] = make_int2(llo, lhi);
+    if (A.band && lane == 0) A.band[brec] = make_int2(llo, lhi);
+    // direct dense output: the zeros of the window's lags outside the band
+    const bool dense = !A.Fout && !A.Eb;
+    if (dense && !A.accumulate) {
+        for (int idx = lane; idx < A.nlag * 9; idx += 32) {
+            const int q = idx / 9, e = idx - 9 * q, l = A.lag0 + q;
+            if (llo < 0 || l < llo || l > lhi) store_entry(A, q, i, j, e, 0.0);
+        }
+    }
     if (llo < 0) return;
+    if (!A.Fout && lane < 12) (&Ls.carry[0][0])[lane] = 0.0;
     const unsigned char* cls = A.cls ? A.cls + ((long long)j * A.N + i) * A.nlag : nullptr;
     if (cls) {
         int n = 0;
@@ -1013,12 +1047,52 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
 #pragma unroll
                 for (int cc = r; cc < 3; cc++)
                     Rm[r][cc] = Cm[r] * MC[0][cc] + Cm[3 + r] * MC[1][cc] + Cm[6 + r] * MC[2][cc];
-            double2* dst = reinterpret_cast<double2*>(A.Fout + (frec + (k - A.kbase) * kstride) * 6);
-            dst[0] = make_double2(0.5 * (S + Rm[0][0]), 0.5 * Rm[0][1]);
-            dst[1] = make_double2(0.5 * Rm[0][2], 0.5 * (S + Rm[1][1]));
-            dst[2] = make_double2(0.5 * Rm[1][2], 0.5 * (S + Rm[2][2]));
+            const double Fk[6] = {0.5 * (S + Rm[0][0]), 0.5 * Rm[0][1], 0.5 * Rm[0][2],
+                                  0.5 * (S + Rm[1][1]), 0.5 * Rm[1][2], 0.5 * (S + Rm[2][2])};
+            if (A.Fout) {
+                double2* dst = reinterpret_cast<double2*>(A.Fout + (frec + (k - A.kbase) * kstride) * 6);
+                dst[0] = make_double2(Fk[0], Fk[1]);
+                dst[1] = make_double2(Fk[2], Fk[3]);
+                dst[2] = make_double2(Fk[4], Fk[5]);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 6; e++) Ls.acc[e][kl] = Fk[e];     // this lane's level only
+            }
         }
         __syncwarp();
+        if (!A.Fout) {
+            // direct output: E_l = (F_{l+1} - 2 F_l + F_{l-1}) / (4 pi rho) for the
+            // lags l = k - 1 completed by the chunk's levels k, clean-up |x| < 1e-14
+            // (calcMatrixSubBlock.m:15,23,111; calcMatrixBlock.m:77); F_0 = 0
+            const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+            for (int kl = lane; kl < nk; kl += 32) {
+                const int k = kc0 + kl, l = k - 1;
+                if (l < llo || l > lhi) continue;
+                double b[6];
+#pragma unroll
+                for (int e = 0; e < 6; e++) {
+                    const double f1 = Ls.acc[e][kl];
+                    const double f0 = (k - 1 < 1) ? 0.0 : (kl >= 1 ? Ls.acc[e][kl - 1] : Ls.carry[1][e]);
+                    const double fm = (k - 2 < 1) ? 0.0 : (kl >= 2 ? Ls.acc[e][kl - 2] : Ls.carry[kl][e]);
+                    const double v = ((f1 + (-2.0) * f0) + fm) / A.c4pirho;
+                    b[e] = (fabs(v) < 1.0e-14) ? 0.0 : v;
+                }
+                if (A.Eb) {
+#pragma unroll
+                    for (int e = 0; e < 6; e++) A.Eb[(bbase + (l - llo)) * 6 + e] = b[e];
+                } else {
+#pragma unroll
+                    for (int e9 = 0; e9 < 9; e9++) store_entry(A, l - A.lag0, i, j, e9, b[map[e9]]);
+                }
+            }
+            __syncwarp();
+            if (lane < 6) {
+                const double c1 = Ls.carry[1][lane];
+                Ls.carry[0][lane] = (nk >= 2) ? Ls.acc[lane][nk - 2] : c1;
+                Ls.carry[1][lane] = Ls.acc[lane][nk - 1];
+            }
+            __syncwarp();
+        }
     }
 }
 
@@ -1037,7 +1111,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_level_kernel(SAArgs A) {
     }
     if (threadIdx.x == 0) blk_count = 0;
     __syncthreads();
-    const long long NP = A.pairs ? A.npairs : (long long)A.nsrc * A.nj;
+    const long long NP = A.pairs ? A.npairs : A.diag_only ? (long long)A.nsrc : (long long)A.nsrc * A.nj;
     const long long nwarps = (long long)gridDim.x * WPB;
     unsigned long long my_count = 0;
     for (long long p = (long long)blockIdx.x * WPB + wib; p < NP; p += nwarps) {
@@ -1048,7 +1122,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_level_kernel(SAArgs A) {
             j = pj.y;
         } else {
             i = A.src0 + (int)(p % A.nsrc);
-            j = A.j0 + (int)(p / A.nsrc);
+            j = A.diag_only ? i : A.j0 + (int)(p / A.nsrc);
         }
         level_pair<MIXED>(A, Ls, glx, glw, p, i, j, lane, my_count);
     }
@@ -1062,10 +1136,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_level_kernel(SAArgs A) {
 template <int WPB, int MINB, bool MIXED>
 static int launch_level(const SAArgs& A, long long NN, int device, cudaStream_t s) {
     const size_t smem = sizeof(LevelShared) * WPB;
-    // the dynamic shared memory opt-in, on every launch: it belongs to the
-    // context, which a caller may have reset since the last call
-    EBEM_CUDA_TRY(cudaFuncSetAttribute(sa_level_kernel<WPB, MINB, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
+    if (int rc = opt_in_smem(sa_level_kernel<WPB, MINB, MIXED>, smem, s)) return rc;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     long long want = (NN + WPB - 1) / WPB;
@@ -1102,8 +1173,13 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
     A.count = d_count;
     A.pairs = pairs;
     A.npairs = npairs;
+    A.j0 = 0;
+    A.nj = m.nt;
     long long NN = diag_only ? (long long)nsrc : (long long)nsrc * m.nt;
     if (pairs) NN = npairs;
+    if (EBEM_SA_KERNEL == 0 && EBEM_LEVEL_GROUPED)
+        return mixed ? launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, true>(A, NN, m.device, s)
+                     : launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s);
     if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 32)
         return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
                      : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
@@ -1274,7 +1350,12 @@ int launch_sa_assemble_banded(const MeshData& m, const PhysParams& P, int n_gh, 
     A.Eb = d_Eb;
     A.boff = d_boff;
     A.blo = d_blo;
+    A.j0 = 0;
+    A.nj = m.nt;
     const long long NN = (long long)m.nt * m.nt;
+    if (EBEM_LEVEL_GROUPED)
+        return mixed ? launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, true>(A, NN, m.device, s)
+                     : launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s);
     if (3 * n_gh <= 32)
         return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
                      : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
@@ -1390,9 +1471,12 @@ int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh,
     A.count = count ? d_count : nullptr;
     A.pairs = nullptr;
     A.npairs = 0;
+    A.j0 = 0;
+    A.nj = m.nt;
     const long long NN = (long long)m.nt * m.nt;
-    int rc = (3 * n_gh <= 32) ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s)
-                              : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
+    int rc = EBEM_LEVEL_GROUPED ? launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s)
+             : (3 * n_gh <= 32) ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s)
+                                : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
     if (rc) return rc;
     if (count) {
         EBEM_CUDA_TRY(cudaMemcpyAsync(host_count, d_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
@@ -1464,6 +1548,81 @@ sa_batch_kernel(const BatchInst* __restrict__ insts, int ninst, long long total,
     }
 }
 
+// The same persistent batch on the grouped level schedule (level_pair with
+// direct output): per pair the per-level sums of level_pair, one lane per
+// level forming F(t_k) and writing the blocks of the lags it completes.
+template <int WPB, int MINB, bool MIXED>
+__global__ void __launch_bounds__(32 * WPB, MINB)
+sa_batch_level_kernel(const BatchInst* __restrict__ insts, int ninst, long long total, int n_gh, int chunk,
+                      unsigned long long* next) {
+    extern __shared__ __align__(16) unsigned char batch_smem[];
+    LevelShared* Lsh = reinterpret_cast<LevelShared*>(batch_smem);
+    __shared__ double glx[10], glw[10];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    LevelShared& Ls = Lsh[wib];
+    if (threadIdx.x < 10) {
+        const int k = threadIdx.x < 5 ? threadIdx.x : threadIdx.x - 5;
+        glx[threadIdx.x] = (threadIdx.x < 5 ? -1.0 : 1.0) * gl_x(k);
+        glw[threadIdx.x] = gl_w(k);
+    }
+    __syncthreads();
+    unsigned long long unused = 0;
+    while (true) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(next, (unsigned long long)chunk);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if ((long long)base >= total) break;
+        const long long end = min((long long)base + chunk, total);
+        for (long long p = (long long)base; p < end; p++) {
+            int lo = 0, hi = ninst - 1;                 // last instance with pair_begin <= p
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (insts[mid].pair_begin <= p) lo = mid;
+                else hi = mid - 1;
+            }
+            const BatchInst& I = insts[lo];
+            SAArgs A;
+            A.geo = I.geo;
+            A.nodes = I.nodes;
+            A.N = I.N;
+            A.n_gh = n_gh;
+            A.velP = I.velP;
+            A.velS = I.velS;
+            A.dt = I.dt;
+            A.c4pirho = I.c4pirho;
+            A.lag0 = 0;
+            A.nlag = I.nlag;
+            A.src0 = 0;
+            A.nsrc = I.N;
+            A.diag_only = 0;
+            A.E = I.E;
+            A.ld = 3 * (size_t)I.N;
+            A.ld_lag = A.ld * A.ld;
+            A.accumulate = 0;
+            A.count = nullptr;
+            A.pairs = nullptr;
+            A.npairs = 0;
+            A.j0 = 0;
+            A.nj = I.N;
+            const long long q = p - I.pair_begin;
+            level_pair<MIXED>(A, Ls, glx, glw, q, (int)(q % I.N), (int)(q / I.N), lane, unused);
+        }
+    }
+}
+
+template <int WPB, int MINB, bool MIXED>
+static int launch_batch_level(const BatchInst* d_insts, int ninst, long long total, int n_gh, int chunk,
+                              unsigned long long* d_next, int device, cudaStream_t s) {
+    const size_t smem = sizeof(LevelShared) * WPB;
+    if (int rc = opt_in_smem(sa_batch_level_kernel<WPB, MINB, MIXED>, smem, s)) return rc;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const unsigned blocks = (unsigned)(sms * MINB);       // one resident wave: persistent
+    sa_batch_level_kernel<WPB, MINB, MIXED><<<blocks, 32 * WPB, smem, s>>>(d_insts, ninst, total, n_gh, chunk, d_next);
+    EBEM_CUDA_TRY(cudaGetLastError());
+    return EBEM_OK;
+}
+
 template <int R, int WPB, int MINB, bool MIXED>
 static int launch_batch_t(const BatchInst* d_insts, int ninst, long long total, int n_gh, int chunk,
                           unsigned long long* d_next, int device, cudaStream_t s) {
@@ -1477,6 +1636,13 @@ static int launch_batch_t(const BatchInst* d_insts, int ninst, long long total, 
 
 int launch_sa_batch(const BatchInst* d_insts, int ninst, long long total, int n_gh, int mixed, int wpb, int chunk,
                     unsigned long long* d_next, int device, cudaStream_t s) {
+    if (EBEM_LEVEL_GROUPED) {
+        if (wpb == 2)
+            return mixed ? launch_batch_level<2, 6, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
+                         : launch_batch_level<2, 6, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
+        return mixed ? launch_batch_level<4, 3, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
+                     : launch_batch_level<4, 3, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
+    }
     if (3 * n_gh <= 32) {
         if (wpb == 2)
             // FP64 at a 170-register cap (1.2 % faster than 128 registers in an

@@ -69,7 +69,8 @@ def samples_for_mesh(m, prm, n_samples: int, rules=RULES, tol: float = TOL, seed
     L = core.num_blocks(dm, prm)
     rng = np.random.default_rng(seed)
     N = dm.N
-    npairs = max(64, int(3 * n_samples / max(1, 0.5 * L)))
+    # most non-null lags are swept by a front: draw enough pairs for n_samples free ones
+    npairs = max(64, int(12 * n_samples / max(1, 0.5 * L)))
     pairs = np.stack([rng.integers(0, N, npairs), rng.integers(0, N, npairs)], 1)
     tp = torch.tensor(pairs, dtype=torch.int32, device="cuda")
     blocks = torch.stack([core.sa_pair_blocks(dm, prm, n, s, tp, L) for n, s in rules])   # (4, P, L, 6)
