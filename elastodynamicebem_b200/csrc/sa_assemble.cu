@@ -31,9 +31,6 @@
 #ifndef EBEM_SA_KERNEL
 #define EBEM_SA_KERNEL 0    // 0: warp per pair when 3 n_gh <= 32, 1: always thread per pair
 #endif
-#ifndef EBEM_LEVEL_GROUPED
-#define EBEM_LEVEL_GROUPED 1  // 1: the two-pass level pass runs sa_level_kernel for every rule
-#endif
 #ifndef EBEM_SA_TWOPASS
 #define EBEM_SA_TWOPASS 1   // 1: dense assemblies store F(t_k) and emit the blocks in a second pass (sa_twopass.cu)
 #endif
@@ -215,6 +212,8 @@ struct SAArgs {
     // that lags of class cls_want use are computed, only those lags counted
     const unsigned char* cls = nullptr;
     int cls_want = -1;
+    // direct dense output into a buffer already zeroed: only the band's blocks are written
+    int zeros_written = 0;
 };
 
 __device__ __forceinline__ void store_block(const SAArgs& A, int q, int i, int j, const double b[6]) {
@@ -299,353 +298,6 @@ __device__ __forceinline__ void store_entry(const SAArgs& A, int q, int i, int j
     else *dst = v;
 }
 
-// The whole time-level walk of one (source i, field j) pair by one warp.
-template <int R, bool MIXED>
-__device__ __forceinline__ void assemble_pair(const SAArgs& A, WarpShared<R>& W, const double* glx, const double* glw,
-                                              int i, int j, int lane, unsigned long long& my_count) {
-    const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
-    const TriGeom& F = A.geo[j];
-    const TriGeom& Sg = A.geo[i];
-    int llo = -1, lhi = -2;
-    long long bbase = 0;
-    if (A.Eb) {
-        // the band comes from the structure pass, so writes stay in the pair's blocks
-        const long long p = (long long)(i - A.src0) * A.N + j;
-        bbase = A.boff[p];
-        const int nb = (int)(A.boff[p + 1] - bbase);
-        if (nb > 0) {
-            llo = A.blo[p];
-            lhi = llo + nb - 1;
-        }
-    } else {
-        pair_band(F, Sg, A.velP, A.velS, A.dt, A.lag0, A.nlag, &llo, &lhi);
-    }
-    if (lane == 0 && llo >= 0) my_count += (unsigned long long)(lhi - llo + 1);
-    if (A.Fout && lane == 0) A.band[(long long)(j - A.j0) * A.nsrc + (i - A.src0)] = make_int2(llo, lhi);
-    if (!A.accumulate && !A.Eb && !A.Fout) {
-        for (int idx = lane; idx < A.nlag * 9; idx += 32) {
-            const int q = idx / 9, e = idx - 9 * q, l = A.lag0 + q;
-            if (llo < 0 || l < llo || l > lhi) store_entry(A, q, i, j, e, 0.0);
-        }
-    }
-    if (llo < 0) return;
-    // slot u of this lane = child c of outer node g, slot = lane + 32 u = 3 g + c
-    LaneChild C[R];
-    bool hasmom[R];
-#pragma unroll
-    for (int u = 0; u < R; u++) {
-        const int slot = lane + 32 * u;
-        LaneChild& Cu = C[u];
-        Cu.live = false;
-        Cu.zeta = 0.0; Cu.sigma = 0.0; Cu.dMIN = 0.0; Cu.w = 0.0;
-        hasmom[u] = false;
-        const int g = slot / 3, c = slot - 3 * (slot / 3);
-        if (g < A.n_gh) {
-            NodeW sp = A.nodes[(size_t)i * A.n_gh + g];
-            NodeGeo G;
-            node_geo(G, sp, F);
-            Cu.zeta = G.zeta;
-            Cu.sigma = G.sigma;
-            Cu.dMIN = G.dMIN;
-            Cu.w = sp.w;
-            if (node_child_e(Cu.g, G, c)) {
-                Cu.live = true;
-                m_sincos(Cu.g.gamma, &Cu.sg, &Cu.cg);
-            }
-        }
-        if (Cu.live) {
-            const ChildE& gg = Cu.g;
-            LevelCtx L0;
-            L0.k5 = (A.velP * A.velP + A.velS * A.velS) / ((A.velP * A.velS) * (A.velP * A.velS));
-            L0.k6 = (A.velP * A.velP - A.velS * A.velS) / ((A.velP * A.velS) * (A.velP * A.velS));
-            const W4 w0 = origin_weights(Cu.zeta, L0);
-            W.w0[0][slot] = w0.sc;
-            W.w0[1][slot] = w0.in;
-            W.w0[2][slot] = w0.mx;
-            W.w0[3][slot] = w0.zz;
-            W.amax[slot] = gg.amax;
-            W.F[slot] = gg.F;
-            W.cbp[slot] = gg.cb * gg.ct + gg.sb * gg.st;     // cos(beta - theta_V1)
-            W.sbp[slot] = gg.sb * gg.ct - gg.cb * gg.st;     // sin(beta - theta_V1)
-            W.zeta[slot] = Cu.zeta;
-            W.zs[slot] = Cu.zeta * Cu.sigma;
-            W.scale[slot] = Cu.w * gg.sgnC;
-            if (MIXED) {
-                W.Ff[slot] = (float)W.F[slot];
-                W.cbpf[slot] = (float)W.cbp[slot];
-                W.sbpf[slot] = (float)W.sbp[slot];
-                W.zetaf[slot] = (float)W.zeta[slot];
-                W.zsf[slot] = (float)W.zs[slot];
-                W.scalef[slot] = (float)W.scale[slot];
-            }
-        }
-    }
-    unsigned stat = 0;          // bit u: child of slot u has become static
-    __syncwarp();
-    const int klo = max(1, llo - 1), khi = lhi + 1;
-    double Fm2[6] = {0, 0, 0, 0, 0, 0}, Fm1[6] = {0, 0, 0, 0, 0, 0}, Fk[6];
-    const double vp2 = A.velP * A.velP, vs2 = A.velS * A.velS, den = vp2 * vs2;
-    for (int k = klo; k <= khi; k++) {
-        const double t = k * A.dt;
-        LevelCtx L;
-        L.t2 = t * t;
-        L.RP = A.velP * t;
-        L.RS = A.velS * t;
-        L.k1 = 1.0 / vp2;
-        L.k5 = (vp2 + vs2) / den;
-        L.k6 = (vp2 - vs2) / den;
-        double S = 0.0, T[6] = {0, 0, 0, 0, 0, 0};
-        Piece pc[R][3];
-        int np[R], nsubs[R][3];
-        double hs[R][3];
-        int nn = 0, npl = 0;
-#pragma unroll
-        for (int u = 0; u < R; u++) {
-            const int slot = lane + 32 * u;
-            const LaneChild& Cu = C[u];
-            // decision phase (per child)
-            int type = T_NONE;
-            double rhoP = -1.0, rhoS = -1.0;
-            const bool is_static = (stat >> u) & 1u;
-            if (Cu.live && !is_static) type = classify(Cu.zeta, L.RP, L.RS, Cu.dMIN, rhoP, rhoS);
-            AccE Ac = {0, 0, 0, 0, 0, 0, 0};
-            int full = 0;
-            np[u] = 0;
-            if (type != T_NONE) {
-                W4 w0;
-                w0.sc = W.w0[0][slot];
-                w0.in = W.w0[1][slot];
-                w0.mx = W.w0[2][slot];
-                w0.zz = W.w0[3][slot];
-                child_decide(Ac, pc[u], np[u], full, Cu, L, rhoP, rhoS, type, w0, W.amax[slot]);
-            }
-            // whole-range moments, computed by the whole warp once per child
-            const bool need = full && !hasmom[u];
-            unsigned mm = __ballot_sync(0xffffffffu, need);
-            while (mm) {
-                const int b = __ffs(mm) - 1;
-                mm &= mm - 1;
-                const double Fb = __shfl_sync(0xffffffffu, Cu.g.F, b), cbb = __shfl_sync(0xffffffffu, Cu.g.cb, b);
-                const double sbb = __shfl_sync(0xffffffffu, Cu.g.sb, b), zb = __shfl_sync(0xffffffffu, Cu.zeta, b);
-                const double s1b = __shfl_sync(0xffffffffu, Cu.g.s1, b), s0b = __shfl_sync(0xffffffffu, Cu.g.s0, b);
-                double m[16];
-                moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx, glw);
-                m[14] = 0.0;
-                m[15] = 0.0;
-                const double tot = warp_reduce_scatter16(m, lane);
-                const int e = scatter16_index(lane);
-                if (!(lane & 1) && e < 14) W.mom[e][b + 32 * u] = tot;
-            }
-            __syncwarp();
-            if (need) hasmom[u] = true;
-            const double zs = Cu.zeta * Cu.sigma;
-            if (full & 1) apply_moments(Ac, W, slot, true, L, zs);
-            if (full & 2) apply_moments(Ac, W, slot, false, L, zs);
-            if (type != T_NONE) {
-                double Sc = 0.0, Tc[6] = {0, 0, 0, 0, 0, 0};
-                child_to_plane(Sc, Tc, Ac, Cu.g, Cu.w * Cu.g.sgnC);
-                S += Sc;
-#pragma unroll
-                for (int e = 0; e < 6; e++) T[e] += Tc[e];
-                // inside the S front with its whole edge (only the full S piece):
-                // level-independent from now on (the fronts only grow)
-                if (type == T_SP_SP && full == 2 && np[u] == 0) {
-                    W.sv[0][slot] = Sc;
-#pragma unroll
-                    for (int e = 0; e < 6; e++) W.sv[1 + e][slot] = Tc[e];
-                    stat |= 1u << u;
-                }
-            } else if (is_static) {
-                S += W.sv[0][slot];
-#pragma unroll
-                for (int e = 0; e < 6; e++) T[e] += W.sv[1 + e][slot];
-            }
-#pragma unroll
-            for (int q = 0; q < 3; q++) {
-                if (q < np[u]) {
-                    double len = pc[u][q].shi - pc[u][q].slo;
-                    int ns = (int)ceil(len * (1.0 / EBEM_EDGE_H));
-                    ns = max(1, min(ns, 4096));
-                    nsubs[u][q] = ns;
-                    hs[u][q] = len / ns;
-                    nn += 10 * ns;
-                }
-            }
-            npl += np[u];
-        }
-        // partial edge pieces of all children -> per-warp list
-        int totp, totn;
-        int pb = warp_excl_scan(npl, lane, totp);
-        int o = warp_excl_scan(nn, lane, totn);
-#pragma unroll
-        for (int u = 0; u < R; u++) {
-#pragma unroll
-            for (int q = 0; q < 3; q++) {
-                if (q < np[u]) {
-                    W.slo[pb] = pc[u][q].slo;
-                    W.h[pb] = hs[u][q];
-                    W.off[pb] = o;
-                    W.who[pb] = (lane + 32 * u) | (pc[u][q].pterm ? 64 : 0);
-                    o += 10 * nsubs[u][q];
-                    pb++;
-                }
-            }
-        }
-        if (lane == 31) W.off[totp] = totn;
-        __syncwarp();
-        // all lanes: Gauss-Legendre nodes of the list, plane frame
-        int pp = 0;
-        if (MIXED) {
-            float Sf = 0.0f, Tf[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-            const float k1 = (float)L.k1, t2 = (float)L.t2, k5 = (float)L.k5, k6 = (float)L.k6;
-            for (int idx = lane; idx < totn; idx += 32) {
-                while (idx >= W.off[pp + 1]) pp++;
-                const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
-                const double h = W.h[pp];
-                const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
-                const int who = W.who[pp], cl = who & 63;
-                edge_node_f32(Sf, Tf, s, (float)(0.5 * h * glw[q]), W.Ff[cl], W.cbpf[cl], W.sbpf[cl], W.zetaf[cl],
-                              W.zsf[cl], W.scalef[cl], (who & 64) != 0, k1, t2, k5, k6);
-            }
-            // per-lane FP32 partial sums join the FP64 lane sums reduced below
-            S += (double)Sf;
-#pragma unroll
-            for (int e = 0; e < 6; e++) T[e] += (double)Tf[e];
-            totn = 0;    // the FP64 loop below has nothing left to do
-        }
-        for (int idx = lane; idx < totn; idx += 32) {
-            while (idx >= W.off[pp + 1]) pp++;
-            const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
-            const double h = W.h[pp];
-            const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
-            const int who = W.who[pp], cl = who & 63;
-            double ch, sech, th;
-            hyp(s, ch, sech, th);
-            const double cbq = W.cbp[cl], sbq = W.sbp[cl];
-            const double cq = th * cbq + sech * sbq, sq = sech * cbq - th * sbq;
-            Rad v = radial_edge(W.F[cl] * ch, W.zeta[cl]);
-            W4 w = weigh(v, (who & 64) != 0, L);
-            const double f = 0.5 * h * glw[q] * sech * W.scale[cl];
-            const double fin = f * w.in, fmx = -W.zs[cl] * f * w.mx;
-            S += f * w.sc;
-            T[0] += fin * cq * cq;
-            T[1] += fin * sq * cq;
-            T[2] += fin * sq * sq;
-            T[3] += fmx * cq;
-            T[4] += fmx * sq;
-            T[5] += f * w.zz;
-        }
-        __syncwarp();
-        {
-            double v[8] = {S, T[0], T[1], T[2], T[3], T[4], T[5], 0.0};
-            const double tot = warp_reduce_scatter8(v, lane);
-            S = __shfl_sync(0xffffffffu, tot, scatter8_lane(0));
-#pragma unroll
-            for (int e = 0; e < 6; e++) T[e] = __shfl_sync(0xffffffffu, tot, scatter8_lane(1 + e));
-        }
-        // F(t_k) = (S I + C^T M C) / 2 in global axes
-        {
-            double M[3][3] = {{T[0], T[1], T[3]}, {T[1], T[2], T[4]}, {T[3], T[4], T[5]}};
-            const double* Cm = F.C;
-            double MC[3][3];
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) MC[r][c] = M[r][0] * Cm[c] + M[r][1] * Cm[3 + c] + M[r][2] * Cm[6 + c];
-            double Rm[3][3];
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-#pragma unroll
-                for (int c = r; c < 3; c++) Rm[r][c] = Cm[r] * MC[0][c] + Cm[3 + r] * MC[1][c] + Cm[6 + r] * MC[2][c];
-            Fk[0] = 0.5 * (S + Rm[0][0]);
-            Fk[1] = 0.5 * Rm[0][1];
-            Fk[2] = 0.5 * Rm[0][2];
-            Fk[3] = 0.5 * (S + Rm[1][1]);
-            Fk[4] = 0.5 * Rm[1][2];
-            Fk[5] = 0.5 * (S + Rm[2][2]);
-        }
-        const int l = k - 1;
-        if (A.Fout) {
-            if (lane < 6)
-                A.Fout[(((long long)(j - A.j0) * A.KL + (k - A.kbase)) * A.nsrc + (i - A.src0)) * 6 + lane] = Fk[lane];
-        } else if (A.Eb) {
-            if (l >= llo && l <= lhi && lane < 6) {
-                double prev = (l - 1 >= 1) ? Fm2[lane] : 0.0;
-                double v = ((Fk[lane] + (-2.0) * Fm1[lane]) + prev) / A.c4pirho;
-                A.Eb[(bbase + (l - llo)) * 6 + lane] = (fabs(v) < 1.0e-14) ? 0.0 : v;
-            }
-        } else if (l >= llo && l <= lhi && lane < 9) {
-            const int e = map[lane];
-            double prev = (l - 1 >= 1) ? Fm2[e] : 0.0;
-            double v = ((Fk[e] + (-2.0) * Fm1[e]) + prev) / A.c4pirho;
-            store_entry(A, l - A.lag0, i, j, lane, (fabs(v) < 1.0e-14) ? 0.0 : v);
-        }
-#pragma unroll
-        for (int e = 0; e < 6; e++) { Fm2[e] = Fm1[e]; Fm1[e] = Fk[e]; }
-    }
-}
-
-// One warp per pair (schedule described in sa_warp.cuh); R children per lane
-// (3 n_gh <= 32 R), WPB warps per block.
-#ifndef EBEM_WARP_WPB
-#define EBEM_WARP_WPB 4    // warps per block of the one-child-per-lane kernel
-#endif
-#ifndef EBEM_WARP2_MINB
-#define EBEM_WARP2_MINB 4  // blocks per SM of the two-children-per-lane kernel (12- and 19-node rules)
-#endif
-#ifndef EBEM_WARP_MINB
-#define EBEM_WARP_MINB 3   // 170 registers: 3 blocks (12 warps) per SM (2.7 % faster than 4 blocks / 128 registers)
-#endif
-template <int R, int WPB, int MINB, bool MIXED>
-__global__ void __launch_bounds__(32 * WPB, MINB) sa_assemble_warp_kernel(SAArgs A) {
-    __shared__ WarpShared<R> Wsh[WPB];
-    __shared__ double glx[10], glw[10];
-    __shared__ unsigned long long blk_count;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    WarpShared<R>& W = Wsh[wib];
-    if (threadIdx.x < 10) {
-        const int k = threadIdx.x < 5 ? threadIdx.x : threadIdx.x - 5;
-        glx[threadIdx.x] = (threadIdx.x < 5 ? -1.0 : 1.0) * gl_x(k);
-        glw[threadIdx.x] = gl_w(k);
-    }
-    if (threadIdx.x == 0) blk_count = 0;
-    __syncthreads();
-    const long long NP = A.pairs      ? A.npairs
-                         : A.diag_only ? (long long)A.nsrc
-                                       : (long long)A.nsrc * (A.Fout ? A.nj : A.N);
-    const long long nwarps = (long long)gridDim.x * WPB;
-    unsigned long long my_count = 0;
-    for (long long p = (long long)blockIdx.x * WPB + wib; p < NP; p += nwarps) {
-        int i, j;
-        if (A.pairs) {
-            const int2 pj = A.pairs[p];
-            i = pj.x;
-            j = pj.y;
-        } else {
-            i = A.src0 + (int)(p % A.nsrc);
-            j = A.diag_only ? i : A.j0 + (int)(p / A.nsrc);
-        }
-        assemble_pair<R, MIXED>(A, W, glx, glw, i, j, lane, my_count);
-    }
-    if (A.count) {
-        if (lane == 0 && my_count) atomicAdd(&blk_count, my_count);
-        __syncthreads();
-        if (threadIdx.x == 0 && blk_count) atomicAdd(A.count, blk_count);
-    }
-}
-
-template <int R, int WPB, int MINB, bool MIXED>
-static int launch_warp(const SAArgs& A, long long NN, int device, cudaStream_t s) {
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    long long want = (NN + WPB - 1) / WPB;
-    long long cap = (long long)sms * 16 * 4 / WPB;
-    unsigned blocks = (unsigned)(want < cap ? want : cap);
-    if (blocks == 0) blocks = 1;
-    sa_assemble_warp_kernel<R, WPB, MINB, MIXED><<<blocks, 32 * WPB, 0, s>>>(A);
-    EBEM_CUDA_TRY(cudaGetLastError());
-    return EBEM_OK;
-}
 
 // sech s, tanh s and the radial antiderivatives at the edge point R = F cosh s
 // (radial_edge) of one Gauss-Legendre node.  With EBEM_GL_ONEDIV (default;
@@ -694,7 +346,7 @@ EBEM_DI void edge_point(double s, double Fc, double zeta, double& sech, double& 
 // Level pass of the two-pass assembly, outer nodes in groups.
 //
 // One warp per (source, field) pair walks the pair's time levels with the
-// schedule of assemble_pair (lane = child of one outer node; per level the
+// schedule of sa_warp.cuh (lane = child of one outer node; per level the
 // per-child decision phase, the whole-range moments, the warp-wide list of
 // Gauss-Legendre nodes and one warp reduction), for the children of at most
 // 10 outer nodes at a time, so composite outer rules of any size
@@ -781,7 +433,7 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
     if (A.band && lane == 0) A.band[brec] = make_int2(llo, lhi);
     // direct dense output: the zeros of the window's lags outside the band
     const bool dense = !A.Fout && !A.Eb;
-    if (dense && !A.accumulate) {
+    if (dense && !A.accumulate && !A.zeros_written) {
         for (int idx = lane; idx < A.nlag * 9; idx += 32) {
             const int q = idx / 9, e = idx - 9 * q, l = A.lag0 + q;
             if (llo < 0 || l < llo || l > lhi) store_entry(A, q, i, j, e, 0.0);
@@ -1150,7 +802,7 @@ static int launch_level(const SAArgs& A, long long NN, int device, cudaStream_t 
 int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag0, int nlag, int src0, int nsrc,
                        double* d_E, size_t ld, size_t ld_lag, int accumulate, unsigned long long* d_count,
                        cudaStream_t s, int diag_only, int mixed, const int2* pairs, long long npairs) {
-    if (EBEM_SA_TWOPASS && EBEM_SA_KERNEL == 0 && 3 * n_gh <= 64 && !diag_only && !pairs)
+    if (EBEM_SA_TWOPASS && EBEM_SA_KERNEL == 0 && !diag_only && !pairs)
         return launch_sa_twopass(m, P, n_gh, lag0, nlag, src0, nsrc, d_E, ld, ld_lag, accumulate, d_count, mixed, s);
     SAArgs A;
     A.geo = m.d_geo;
@@ -1177,14 +829,9 @@ int launch_sa_assemble(const MeshData& m, const PhysParams& P, int n_gh, int lag
     A.nj = m.nt;
     long long NN = diag_only ? (long long)nsrc : (long long)nsrc * m.nt;
     if (pairs) NN = npairs;
-    if (EBEM_SA_KERNEL == 0 && EBEM_LEVEL_GROUPED)
+    if (EBEM_SA_KERNEL == 0)
         return mixed ? launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, true>(A, NN, m.device, s)
                      : launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s);
-    if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 32)
-        return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
-                     : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
-    if (EBEM_SA_KERNEL == 0 && 3 * n_gh <= 64)
-        return mixed ? launch_warp<2, 2, EBEM_WARP2_MINB, true>(A, NN, m.device, s) : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
     if (pairs || mixed) return fail(EBEM_ERR_INVALID, "pair lists and mixed precision need the warp kernel");
     int threads = 128;
     long long blocks = (NN + threads - 1) / threads;
@@ -1230,16 +877,8 @@ int launch_sa_fwarp(const MeshData& m, const PhysParams& P, int n_gh, int lag0, 
     A.cls = cls;
     A.cls_want = cls_want;
     const long long NN = (long long)nsrc * nj;
-    if (EBEM_LEVEL_GROUPED || 3 * n_gh > 64 || cls)
-        return mixed ? launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, true>(A, NN, m.device, s)
-                     : launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s);
-    if (3 * n_gh <= 32)
-        return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
-                     : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
-    if (3 * n_gh <= 64)
-        return mixed ? launch_warp<2, 2, EBEM_WARP2_MINB, true>(A, NN, m.device, s)
-                     : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
-    return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+    return mixed ? launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, true>(A, NN, m.device, s)
+                 : launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s);
 }
 
 // Blocks of an explicit list of (source, field) pairs at every lag [0, nlag)
@@ -1353,13 +992,8 @@ int launch_sa_assemble_banded(const MeshData& m, const PhysParams& P, int n_gh, 
     A.j0 = 0;
     A.nj = m.nt;
     const long long NN = (long long)m.nt * m.nt;
-    if (EBEM_LEVEL_GROUPED)
-        return mixed ? launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, true>(A, NN, m.device, s)
-                     : launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s);
-    if (3 * n_gh <= 32)
-        return mixed ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, true>(A, NN, m.device, s)
-                     : launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s);
-    return mixed ? launch_warp<2, 2, EBEM_WARP2_MINB, true>(A, NN, m.device, s) : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
+    return mixed ? launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, true>(A, NN, m.device, s)
+                 : launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -1474,9 +1108,7 @@ int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh,
     A.j0 = 0;
     A.nj = m.nt;
     const long long NN = (long long)m.nt * m.nt;
-    int rc = EBEM_LEVEL_GROUPED ? launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s)
-             : (3 * n_gh <= 32) ? launch_warp<1, EBEM_WARP_WPB, EBEM_WARP_MINB, false>(A, NN, m.device, s)
-                                : launch_warp<2, 2, EBEM_WARP2_MINB, false>(A, NN, m.device, s);
+    int rc = launch_level<EBEM_LEVEL_WPB, EBEM_LEVEL_MINB, false>(A, NN, m.device, s);
     if (rc) return rc;
     if (count) {
         EBEM_CUDA_TRY(cudaMemcpyAsync(host_count, d_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
@@ -1489,68 +1121,10 @@ int launch_sa_assemble_noalloc(const MeshData& m, const PhysParams& P, int n_gh,
 // Batched assembly: many meshes (instances) in one persistent launch.  Each
 // warp grabs `chunk` consecutive pairs of the concatenated pair space
 // (instance b owns pairs [pair_begin[b], pair_begin[b] + N_b^2)) from a global
-// counter and assembles them with the same per-pair walk as the single-mesh
-// kernel, so a batch result equals the single-mesh results to rounding.
-
-template <int R, int WPB, int MINB, bool MIXED>
-__global__ void __launch_bounds__(32 * WPB, MINB)
-sa_batch_kernel(const BatchInst* __restrict__ insts, int ninst, long long total, int n_gh, int chunk,
-                unsigned long long* next) {
-    __shared__ WarpShared<R> Wsh[WPB];
-    __shared__ double glx[10], glw[10];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    WarpShared<R>& W = Wsh[wib];
-    if (threadIdx.x < 10) {
-        const int k = threadIdx.x < 5 ? threadIdx.x : threadIdx.x - 5;
-        glx[threadIdx.x] = (threadIdx.x < 5 ? -1.0 : 1.0) * gl_x(k);
-        glw[threadIdx.x] = gl_w(k);
-    }
-    __syncthreads();
-    unsigned long long unused = 0;
-    while (true) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(next, (unsigned long long)chunk);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if ((long long)base >= total) break;
-        const long long end = min((long long)base + chunk, total);
-        for (long long p = (long long)base; p < end; p++) {
-            int lo = 0, hi = ninst - 1;                 // last instance with pair_begin <= p
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (insts[mid].pair_begin <= p) lo = mid;
-                else hi = mid - 1;
-            }
-            const BatchInst& I = insts[lo];
-            SAArgs A;
-            A.geo = I.geo;
-            A.nodes = I.nodes;
-            A.N = I.N;
-            A.n_gh = n_gh;
-            A.velP = I.velP;
-            A.velS = I.velS;
-            A.dt = I.dt;
-            A.c4pirho = I.c4pirho;
-            A.lag0 = 0;
-            A.nlag = I.nlag;
-            A.src0 = 0;
-            A.nsrc = I.N;
-            A.diag_only = 0;
-            A.E = I.E;
-            A.ld = 3 * (size_t)I.N;
-            A.ld_lag = A.ld * A.ld;
-            A.accumulate = 0;
-            A.count = nullptr;
-            A.pairs = nullptr;
-            A.npairs = 0;
-            const long long q = p - I.pair_begin;
-            assemble_pair<R, MIXED>(A, W, glx, glw, (int)(q % I.N), (int)(q / I.N), lane, unused);
-        }
-    }
-}
-
-// The same persistent batch on the grouped level schedule (level_pair with
-// direct output): per pair the per-level sums of level_pair, one lane per
-// level forming F(t_k) and writing the blocks of the lags it completes.
+// counter and assembles them with level_pair's per-pair walk (direct output),
+// so a batch result equals the single-mesh results to rounding: per pair the
+// per-level sums of level_pair, one lane per level forming F(t_k) and writing
+// the blocks of the lags it completes.
 template <int WPB, int MINB, bool MIXED>
 __global__ void __launch_bounds__(32 * WPB, MINB)
 sa_batch_level_kernel(const BatchInst* __restrict__ insts, int ninst, long long total, int n_gh, int chunk,
@@ -1604,6 +1178,7 @@ sa_batch_level_kernel(const BatchInst* __restrict__ insts, int ninst, long long 
             A.npairs = 0;
             A.j0 = 0;
             A.nj = I.N;
+            A.zeros_written = 1;
             const long long q = p - I.pair_begin;
             level_pair<MIXED>(A, Ls, glx, glw, q, (int)(q % I.N), (int)(q / I.N), lane, unused);
         }
@@ -1623,40 +1198,37 @@ static int launch_batch_level(const BatchInst* d_insts, int ninst, long long tot
     return EBEM_OK;
 }
 
-template <int R, int WPB, int MINB, bool MIXED>
-static int launch_batch_t(const BatchInst* d_insts, int ninst, long long total, int n_gh, int chunk,
-                          unsigned long long* d_next, int device, cudaStream_t s) {
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const unsigned blocks = (unsigned)(sms * MINB);       // one resident wave: persistent
-    sa_batch_kernel<R, WPB, MINB, MIXED><<<blocks, 32 * WPB, 0, s>>>(d_insts, ninst, total, n_gh, chunk, d_next);
-    EBEM_CUDA_TRY(cudaGetLastError());
-    return EBEM_OK;
+// Zeros of every instance's output (the output pointers read from the device
+// table at run time, as the assembly reads them): blockIdx.y = instance,
+// 16-byte stores over its 9 N^2 nlag doubles.  The assembly then writes only
+// the blocks of each pair's non-null lags; zeroing the whole buffer at copy
+// bandwidth costs less than the scattered zero blocks of the direct output.
+__global__ void batch_zero_kernel(const BatchInst* __restrict__ insts) {
+    const BatchInst& I = insts[blockIdx.y];
+    const long long n = 9LL * I.N * I.N * I.nlag;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    if ((reinterpret_cast<size_t>(I.E) & 15) == 0) {
+        double2* E2 = reinterpret_cast<double2*>(I.E);
+        const double2 z = make_double2(0.0, 0.0);
+        for (long long k = t0; k < n / 2; k += stride) E2[k] = z;
+        if ((n & 1) && t0 == 0) I.E[n - 1] = 0.0;
+    } else {
+        // an output that starts off a 16-byte boundary: 8-byte stores
+        for (long long k = t0; k < n; k += stride) I.E[k] = 0.0;
+    }
 }
 
 int launch_sa_batch(const BatchInst* d_insts, int ninst, long long total, int n_gh, int mixed, int wpb, int chunk,
                     unsigned long long* d_next, int device, cudaStream_t s) {
-    if (EBEM_LEVEL_GROUPED) {
-        if (wpb == 2)
-            return mixed ? launch_batch_level<2, 6, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
-                         : launch_batch_level<2, 6, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
-        return mixed ? launch_batch_level<4, 3, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
-                     : launch_batch_level<4, 3, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
-    }
-    if (3 * n_gh <= 32) {
-        if (wpb == 2)
-            // FP64 at a 170-register cap (1.2 % faster than 128 registers in an
-            // A/B of the 64-instance batch); the mixed form at 128 registers
-            // (1.4 % faster than 170 in the same A/B)
-            return mixed ? launch_batch_t<1, 2, 8, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
-                         : launch_batch_t<1, 2, 6, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
-        return mixed ? launch_batch_t<1, 4, 4, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
-                     : launch_batch_t<1, 4, 3, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
-    }
-    if (3 * n_gh <= 64)
-        return mixed ? launch_batch_t<2, 2, 4, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
-                     : launch_batch_t<2, 2, 4, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
-    return fail(EBEM_ERR_INVALID, "outer rule must have 3, 7, 12 or 19 nodes");
+    (void)n_gh;
+    if (ninst > 65535) return fail(EBEM_ERR_INVALID, "too many batch instances for one launch");
+    batch_zero_kernel<<<dim3(148, (unsigned)ninst), 256, 0, s>>>(d_insts);
+    EBEM_CUDA_TRY(cudaGetLastError());
+    if (wpb == 2)
+        return mixed ? launch_batch_level<2, 6, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
+                     : launch_batch_level<2, 6, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
+    return mixed ? launch_batch_level<4, 3, true>(d_insts, ninst, total, n_gh, chunk, d_next, device, s)
+                 : launch_batch_level<4, 3, false>(d_insts, ninst, total, n_gh, chunk, d_next, device, s);
 }
 
 }  // namespace ebem

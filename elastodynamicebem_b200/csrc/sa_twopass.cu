@@ -1,6 +1,6 @@
 // Semi-analytic assembly of dense outputs in two passes.
 //
-// Pass 1 (sa_assemble_warp_kernel in its level-output mode, sa_assemble.cu):
+// Pass 1 (sa_level_kernel in its level-output mode, sa_assemble.cu):
 // one warp per (source, field) pair walks the pair's time levels and stores
 // F(t_k), the combined kernel integral at instant k dt
 // (BEMenerg_coreSA_calcMatrixSubBlock.m:101-104 summed over the outer nodes
@@ -18,8 +18,8 @@
 // zeros of the lags outside each pair's band the same way (sphere of 1280
 // triangles, L = 40: 207 ms per step; two passes: 188 ms).
 //
-// The values equal the one-pass kernel's bit for bit (the same per-pair
-// arithmetic and the same second-difference expression).
+// The values equal those of the level kernel's direct output bit for bit
+// (the same per-pair arithmetic and the same second-difference expression).
 //
 // The level buffer holds, per chunk of field columns, (columns) x (levels) x
 // (sources) x 6 doubles plus one int2 per pair; the columns are split into

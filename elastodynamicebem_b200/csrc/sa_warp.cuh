@@ -23,12 +23,11 @@
 //   list and their Gauss-Legendre nodes are evaluated by all 32 lanes, each
 //   node weighted by its child's node weight and orientation sign and taken
 //   in the plane frame, so every lane sums into the same pair value.
-// * The per-level pair value is a warp reduction; every lane forms F(t_k)
-//   and the sliding window, lanes 0..8 store the 3x3 block.
+// * The per-level pair value is a warp reduction into per-level sums; after
+//   a chunk of levels one lane per level forms F(t_k) (level_pair in
+//   sa_assemble.cu).
 //
-// Grid-stride over pairs (pair p = field j * nsrc + source i - src0, or the
-// diagonal pairs), one warp at a time per pair.  Rules with more than 32
-// children (12 and 19 outer nodes) give each lane two children (R = 2).
+// Rules with more than 30 children run their outer nodes in groups of 10.
 #pragma once
 
 #include "sa_pair.cuh"
