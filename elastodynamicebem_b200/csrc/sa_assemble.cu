@@ -356,11 +356,18 @@ EBEM_DI void edge_point(double s, double Fc, double zeta, double& sech, double& 
 // emission pass.  With a per-(pair, lag) class array only the levels used by
 // lags of the wanted class are walked.
 //
-// An alternative schedule was measured and not kept: compacted (child,
-// level) items, 32 per round, each lane on its own item (sphere of 1280
-// triangles: 224 ms per step against 186 ms; ncu: 9 % fewer warp
+// Two alternative schedules were measured and not kept.  Compacted (child,
+// level) items, 32 per round, each lane on its own item: sphere of 1280
+// triangles 224 ms per step against 186 ms (ncu: 9 % fewer warp
 // instructions, but more instruction-fetch stalls, the items of a round
-// taking more distinct branches than the children of one level).
+// taking more distinct branches than the children of one level).  Groups
+// of 10 consecutive outer nodes of up to three pairs of one field column
+// (30 lanes busy instead of 21 with the 7-node rule, per-pair level sums):
+// 165.9 ms against 167.2 ms with the 7-node rule, 104.7 against 135.4 ms
+// with the 3-node rule; the children of different pairs take more distinct
+// branches per pass than those of one pair, which cancels most of the lanes
+// gained, and the results then depend on how pairs fall into groups (a
+// source-row sub-panel no longer reproduces the full assembly bit for bit).
 
 #ifndef EBEM_LEVEL_KC
 #define EBEM_LEVEL_KC 48         // levels per chunk (per-level sums in shared memory)
@@ -370,9 +377,6 @@ EBEM_DI void edge_point(double s, double Fc, double zeta, double& sech, double& 
 #endif
 #ifndef EBEM_LEVEL_MINB
 #define EBEM_LEVEL_MINB 3
-#endif
-#ifndef EBEM_LEVEL_SKIP_NOPIECE
-#define EBEM_LEVEL_SKIP_NOPIECE 1   // 1: levels without partial edge pieces skip the piece list and node loop
 #endif
 #ifndef EBEM_LEVEL_SKIP_IDLE
 #define EBEM_LEVEL_SKIP_IDLE 1   // 1: levels at which no child works skip the decision and node phases
@@ -613,68 +617,65 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
                         nn += 10 * ns;
                     }
                 }
-                // partial edge pieces of all children -> per-warp list, their nodes
-                // (skipped at levels where no child has a partial edge piece)
-                if (!EBEM_LEVEL_SKIP_NOPIECE || __any_sync(0xffffffffu, np > 0)) {
-                    int totp, totn;
-                    int pb = warp_excl_scan(np, lane, totp);
-                    int o = warp_excl_scan(nn, lane, totn);
+                // partial edge pieces of all children -> per-warp list
+                int totp, totn;
+                int pb = warp_excl_scan(np, lane, totp);
+                int o = warp_excl_scan(nn, lane, totn);
 #pragma unroll
-                    for (int q = 0; q < 3; q++) {
-                        if (q < np) {
-                            W.slo[pb] = pc[q].slo;
-                            W.h[pb] = hs[q];
-                            W.off[pb] = o;
-                            W.who[pb] = slot | (pc[q].pterm ? 64 : 0);
-                            o += 10 * nsubs[q];
-                            pb++;
-                        }
+                for (int q = 0; q < 3; q++) {
+                    if (q < np) {
+                        W.slo[pb] = pc[q].slo;
+                        W.h[pb] = hs[q];
+                        W.off[pb] = o;
+                        W.who[pb] = slot | (pc[q].pterm ? 64 : 0);
+                        o += 10 * nsubs[q];
+                        pb++;
                     }
-                    if (lane == 31) W.off[totp] = totn;
-                    __syncwarp();
-                    // all lanes: Gauss-Legendre nodes of the list, plane frame
-                    int pp = 0;
-                    if (MIXED) {
-                        float Sf = 0.0f, Tf[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-                        const float fk1 = (float)L.k1, ft2 = (float)L.t2, fk5 = (float)L.k5, fk6 = (float)L.k6;
-                        for (int idx = lane; idx < totn; idx += 32) {
-                            while (idx >= W.off[pp + 1]) pp++;
-                            const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
-                            const double h = W.h[pp];
-                            const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
-                            const int who = W.who[pp], cl = who & 63;
-                            edge_node_f32(Sf, Tf, s, (float)(0.5 * h * glw[q]), W.Ff[cl], W.cbpf[cl], W.sbpf[cl],
-                                          W.zetaf[cl], W.zsf[cl], W.scalef[cl], (who & 64) != 0, fk1, ft2, fk5, fk6);
-                        }
-                        S += (double)Sf;
-#pragma unroll
-                        for (int e = 0; e < 6; e++) T[e] += (double)Tf[e];
-                        totn = 0;    // the FP64 loop below has nothing left to do
-                    }
+                }
+                if (lane == 31) W.off[totp] = totn;
+                __syncwarp();
+                // all lanes: Gauss-Legendre nodes of the list, plane frame
+                int pp = 0;
+                if (MIXED) {
+                    float Sf = 0.0f, Tf[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                    const float fk1 = (float)L.k1, ft2 = (float)L.t2, fk5 = (float)L.k5, fk6 = (float)L.k6;
                     for (int idx = lane; idx < totn; idx += 32) {
                         while (idx >= W.off[pp + 1]) pp++;
                         const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
                         const double h = W.h[pp];
                         const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
                         const int who = W.who[pp], cl = who & 63;
-                        double sech, th;
-                        Rad v;
-                        edge_point(s, W.F[cl], W.zeta[cl], sech, th, v);
-                        const double cbq = W.cbp[cl], sbq = W.sbp[cl];
-                        const double cq = th * cbq + sech * sbq, sq = sech * cbq - th * sbq;
-                        W4 w = weigh(v, (who & 64) != 0, L);
-                        const double f = 0.5 * h * glw[q] * sech * W.scale[cl];
-                        const double fin = f * w.in, fmx = -W.zs[cl] * f * w.mx;
-                        S += f * w.sc;
-                        T[0] += fin * cq * cq;
-                        T[1] += fin * sq * cq;
-                        T[2] += fin * sq * sq;
-                        T[3] += fmx * cq;
-                        T[4] += fmx * sq;
-                        T[5] += f * w.zz;
+                        edge_node_f32(Sf, Tf, s, (float)(0.5 * h * glw[q]), W.Ff[cl], W.cbpf[cl], W.sbpf[cl],
+                                      W.zetaf[cl], W.zsf[cl], W.scalef[cl], (who & 64) != 0, fk1, ft2, fk5, fk6);
                     }
-                    __syncwarp();
+                    S += (double)Sf;
+#pragma unroll
+                    for (int e = 0; e < 6; e++) T[e] += (double)Tf[e];
+                    totn = 0;    // the FP64 loop below has nothing left to do
                 }
+                for (int idx = lane; idx < totn; idx += 32) {
+                    while (idx >= W.off[pp + 1]) pp++;
+                    const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
+                    const double h = W.h[pp];
+                    const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
+                    const int who = W.who[pp], cl = who & 63;
+                    double sech, th;
+                    Rad v;
+                    edge_point(s, W.F[cl], W.zeta[cl], sech, th, v);
+                    const double cbq = W.cbp[cl], sbq = W.sbp[cl];
+                    const double cq = th * cbq + sech * sbq, sq = sech * cbq - th * sbq;
+                    W4 w = weigh(v, (who & 64) != 0, L);
+                    const double f = 0.5 * h * glw[q] * sech * W.scale[cl];
+                    const double fin = f * w.in, fmx = -W.zs[cl] * f * w.mx;
+                    S += f * w.sc;
+                    T[0] += fin * cq * cq;
+                    T[1] += fin * sq * cq;
+                    T[2] += fin * sq * sq;
+                    T[3] += fmx * cq;
+                    T[4] += fmx * sq;
+                    T[5] += f * w.zz;
+                }
+                __syncwarp();
                 // warp sums; lane scatter8_lane(e) holds entry e (S, T11, T12, T22, T13, T23, T33)
                 double v[8] = {S, T[0], T[1], T[2], T[3], T[4], T[5], 0.0};
                 const double tot = warp_reduce_scatter8(v, lane);
