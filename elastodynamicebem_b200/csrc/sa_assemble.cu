@@ -378,6 +378,9 @@ EBEM_DI void edge_point(double s, double Fc, double zeta, double& sech, double& 
 #ifndef EBEM_LEVEL_MINB
 #define EBEM_LEVEL_MINB 3
 #endif
+#ifndef EBEM_GL_ADAPT
+#define EBEM_GL_ADAPT 1   // 1: 6 or 8 Gauss-Legendre nodes on edge pieces up to 1/4 or 1/2 long, else 10
+#endif
 #ifndef EBEM_LEVEL_SKIP_IDLE
 #define EBEM_LEVEL_SKIP_IDLE 1   // 1: levels at which no child works skip the decision and node phases
 #endif
@@ -530,7 +533,7 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
                 L.k6 = k6;
                 double S = 0.0, T[6] = {0, 0, 0, 0, 0, 0};
                 Piece pc[3];
-                int np = 0, nsubs[3];
+                int np = 0, nsubs[3], ngs[3];
                 double hs[3];
                 int nn = 0;
                 // decision phase (per child)
@@ -573,7 +576,7 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
                     const double sbb = __shfl_sync(0xffffffffu, Cu.g.sb, b), zb = __shfl_sync(0xffffffffu, Cu.zeta, b);
                     const double s1b = __shfl_sync(0xffffffffu, Cu.g.s1, b), s0b = __shfl_sync(0xffffffffu, Cu.g.s0, b);
                     double m[16];
-                    moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx, glw);
+                    moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx + 14, glw + 14);
                     m[14] = 0.0;
                     m[15] = 0.0;
                     const double tot = warp_reduce_scatter16(m, lane);
@@ -607,14 +610,17 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
 #pragma unroll
                 for (int q = 0; q < 3; q++) {
                     nsubs[q] = 0;
+                    ngs[q] = 10;
                     hs[q] = 0.0;
                     if (q < np) {
                         double len = pc[q].shi - pc[q].slo;
                         int ns = (int)ceil(len * (1.0 / EBEM_EDGE_H));
                         ns = max(1, min(ns, 4096));
+                        // nodes per sub-piece: 6 up to length 1/4, 8 up to 1/2 (gl6_x)
+                        if (EBEM_GL_ADAPT && ns == 1) ngs[q] = len <= 0.25 ? 6 : (len <= 0.5 ? 8 : 10);
                         nsubs[q] = ns;
                         hs[q] = len / ns;
-                        nn += 10 * ns;
+                        nn += ngs[q] * ns;
                     }
                 }
                 // partial edge pieces of all children -> per-warp list
@@ -627,8 +633,8 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
                         W.slo[pb] = pc[q].slo;
                         W.h[pb] = hs[q];
                         W.off[pb] = o;
-                        W.who[pb] = slot | (pc[q].pterm ? 64 : 0);
-                        o += 10 * nsubs[q];
+                        W.who[pb] = slot | (pc[q].pterm ? 64 : 0) | (((ngs[q] - 6) >> 1) << 7);
+                        o += ngs[q] * nsubs[q];
                         pb++;
                     }
                 }
@@ -641,10 +647,11 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
                     const float fk1 = (float)L.k1, ft2 = (float)L.t2, fk5 = (float)L.k5, fk6 = (float)L.k6;
                     for (int idx = lane; idx < totn; idx += 32) {
                         while (idx >= W.off[pp + 1]) pp++;
-                        const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
+                        const int who = W.who[pp], cl = who & 63, code = who >> 7;
+                        const int u = idx - W.off[pp], sub = code == 2 ? u / 10 : 0;
+                        const int q = u - (6 + 2 * code) * sub + (code == 0 ? 0 : (code == 1 ? 6 : 14));
                         const double h = W.h[pp];
                         const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
-                        const int who = W.who[pp], cl = who & 63;
                         edge_node_f32(Sf, Tf, s, (float)(0.5 * h * glw[q]), W.Ff[cl], W.cbpf[cl], W.sbpf[cl],
                                       W.zetaf[cl], W.zsf[cl], W.scalef[cl], (who & 64) != 0, fk1, ft2, fk5, fk6);
                     }
@@ -655,10 +662,11 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
                 }
                 for (int idx = lane; idx < totn; idx += 32) {
                     while (idx >= W.off[pp + 1]) pp++;
-                    const int u = idx - W.off[pp], sub = u / 10, q = u - 10 * sub;
+                    const int who = W.who[pp], cl = who & 63, code = who >> 7;
+                    const int u = idx - W.off[pp], sub = code == 2 ? u / 10 : 0;
+                    const int q = u - (6 + 2 * code) * sub + (code == 0 ? 0 : (code == 1 ? 6 : 14));
                     const double h = W.h[pp];
                     const double s = W.slo[pp] + (sub + 0.5) * h + 0.5 * h * glx[q];
-                    const int who = W.who[pp], cl = who & 63;
                     double sech, th;
                     Rad v;
                     edge_point(s, W.F[cl], W.zeta[cl], sech, th, v);
@@ -759,15 +767,11 @@ template <int WPB, int MINB, bool MIXED>
 __global__ void __launch_bounds__(32 * WPB, MINB) sa_level_kernel(SAArgs A) {
     extern __shared__ __align__(16) unsigned char level_smem[];
     LevelShared* Lsh = reinterpret_cast<LevelShared*>(level_smem);
-    __shared__ double glx[10], glw[10];
+    __shared__ double gt[48];          // Gauss-Legendre nodes and weights (gl_table_entry)
     __shared__ unsigned long long blk_count;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     LevelShared& Ls = Lsh[wib];
-    if (threadIdx.x < 10) {
-        const int k = threadIdx.x < 5 ? threadIdx.x : threadIdx.x - 5;
-        glx[threadIdx.x] = (threadIdx.x < 5 ? -1.0 : 1.0) * gl_x(k);
-        glw[threadIdx.x] = gl_w(k);
-    }
+    if (threadIdx.x < 24) gl_table_entry(threadIdx.x, gt[threadIdx.x], gt[24 + threadIdx.x]);
     if (threadIdx.x == 0) blk_count = 0;
     __syncthreads();
     const long long NP = A.pairs ? A.npairs : A.diag_only ? (long long)A.nsrc : (long long)A.nsrc * A.nj;
@@ -783,7 +787,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sa_level_kernel(SAArgs A) {
             i = A.src0 + (int)(p % A.nsrc);
             j = A.diag_only ? i : A.j0 + (int)(p / A.nsrc);
         }
-        level_pair<MIXED>(A, Ls, glx, glw, p, i, j, lane, my_count);
+        level_pair<MIXED>(A, Ls, gt, gt + 24, p, i, j, lane, my_count);
     }
     if (A.count) {
         if (lane == 0 && my_count) atomicAdd(&blk_count, my_count);
@@ -1138,14 +1142,10 @@ sa_batch_level_kernel(const BatchInst* __restrict__ insts, int ninst, long long 
                       unsigned long long* next) {
     extern __shared__ __align__(16) unsigned char batch_smem[];
     LevelShared* Lsh = reinterpret_cast<LevelShared*>(batch_smem);
-    __shared__ double glx[10], glw[10];
+    __shared__ double gt[48];          // Gauss-Legendre nodes and weights (gl_table_entry)
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     LevelShared& Ls = Lsh[wib];
-    if (threadIdx.x < 10) {
-        const int k = threadIdx.x < 5 ? threadIdx.x : threadIdx.x - 5;
-        glx[threadIdx.x] = (threadIdx.x < 5 ? -1.0 : 1.0) * gl_x(k);
-        glw[threadIdx.x] = gl_w(k);
-    }
+    if (threadIdx.x < 24) gl_table_entry(threadIdx.x, gt[threadIdx.x], gt[24 + threadIdx.x]);
     __syncthreads();
     unsigned long long unused = 0;
     while (true) {
@@ -1187,7 +1187,7 @@ sa_batch_level_kernel(const BatchInst* __restrict__ insts, int ninst, long long 
             A.nj = I.N;
             A.zeros_written = 1;
             const long long q = p - I.pair_begin;
-            level_pair<MIXED>(A, Ls, glx, glw, q, (int)(q % I.N), (int)(q / I.N), lane, unused);
+            level_pair<MIXED>(A, Ls, gt, gt + 24, q, (int)(q % I.N), (int)(q / I.N), lane, unused);
         }
     }
 }
