@@ -299,49 +299,6 @@ __device__ __forceinline__ void store_entry(const SAArgs& A, int q, int i, int j
 }
 
 
-// sech s, tanh s and the radial antiderivatives at the edge point R = F cosh s
-// (radial_edge) of one Gauss-Legendre node.  With EBEM_GL_ONEDIV (default;
-// the sphere of 1280 triangles 161 -> 157 ms per step against hyp() and
-// radial_edge(), which divide three times per node) the
-// reciprocals of e^s, 1 + e^2s, r' and r' + F (1 + e^2s) (r' = 2 e^s r) come
-// from one division: 1/e^s, 1/cosh, 1/(r (r + R)) and 1/r then cost
-// multiplications, and log(R + r) = log(r' + F (1 + e^2s)) - s - log 2.
-#ifndef EBEM_GL_ONEDIV
-#define EBEM_GL_ONEDIV 1
-#endif
-EBEM_DI void edge_point(double s, double Fc, double zeta, double& sech, double& th, Rad& v) {
-#if EBEM_GL_ONEDIV
-    const double e = m_exp(s), e2 = e * e, u = e2 + 1.0;
-    const double z2 = zeta * zeta, Fu = Fc * u;
-    const double rp = sqrt(Fu * Fu + 4.0 * z2 * e2);          // 2 e^s r
-    const double a = rp + Fu;                                 // 2 e^s (r + R)
-    const double ue = u * e, ra = rp * a;
-    const double inv = 1.0 / (ue * ra);
-    const double iu = e * ra * inv, ie = u * ra * inv, irp = ue * a * inv, ia = ue * rp * inv;
-    sech = 2.0 * e * iu;
-    th = (e2 - 1.0) * iu;
-    const double r = 0.5 * rp * ie, R = 0.5 * Fu * ie;
-    const double ir = 2.0 * e * irp, ir3 = ir * ir * ir;
-    v.A1 = r;
-    v.A3 = -ir;
-    v.B2 = r + z2 * ir;
-    v.D2 = -z2 * ir;
-    v.B4 = -ir + z2 * ir3 * (1.0 / 3.0);
-    v.D4 = -z2 * ir3 * (1.0 / 3.0);
-    if (zeta > 0) {
-        v.C2 = m_log(a) - (s + 0.69314718055994530942) - Fu * irp;
-        v.C4 = -(r * r + r * R + R * R) * ir3 * (2.0 * e * ia) * (1.0 / 3.0);
-    } else {
-        v.C2 = 0.0;
-        v.C4 = 0.0;
-    }
-#else
-    double ch;
-    hyp(s, ch, sech, th);
-    v = radial_edge(Fc * ch, zeta);
-#endif
-}
-
 // ---------------------------------------------------------------------------
 // Level pass of the two-pass assembly, outer nodes in groups.
 //
@@ -377,9 +334,6 @@ EBEM_DI void edge_point(double s, double Fc, double zeta, double& sech, double& 
 #endif
 #ifndef EBEM_LEVEL_MINB
 #define EBEM_LEVEL_MINB 3
-#endif
-#ifndef EBEM_GL_ADAPT
-#define EBEM_GL_ADAPT 1   // 1: 6 or 8 Gauss-Legendre nodes on edge pieces up to 1/4 or 1/2 long, else 10
 #endif
 #ifndef EBEM_LEVEL_SKIP_IDLE
 #define EBEM_LEVEL_SKIP_IDLE 1   // 1: levels at which no child works skip the decision and node phases
@@ -576,7 +530,7 @@ __device__ __forceinline__ void level_pair(const SAArgs& A, LevelShared& Ls, con
                     const double sbb = __shfl_sync(0xffffffffu, Cu.g.sb, b), zb = __shfl_sync(0xffffffffu, Cu.zeta, b);
                     const double s1b = __shfl_sync(0xffffffffu, Cu.g.s1, b), s0b = __shfl_sync(0xffffffffu, Cu.g.s0, b);
                     double m[16];
-                    moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx + 14, glw + 14);
+                    moment_share(m, Fb, cbb, sbb, zb, s1b, s0b, lane, glx, glw);
                     m[14] = 0.0;
                     m[15] = 0.0;
                     const double tot = warp_reduce_scatter16(m, lane);

@@ -34,6 +34,10 @@
 
 namespace ebem {
 
+#ifndef EBEM_GL_ADAPT
+#define EBEM_GL_ADAPT 1   // 1: 6 or 8 Gauss-Legendre nodes on edge pieces up to 1/4 or 1/2 long, else 10
+#endif
+
 // Per-warp shared state for R children per lane (32 R child slots, at most
 // 3 edge pieces per child and level).
 template <int R>
@@ -127,8 +131,53 @@ EBEM_DI void hyp(double s, double& ch, double& sech, double& th) {
     th = 0.5 * (e - ie) * sech;
 }
 
+// sech s, tanh s and the radial antiderivatives at the edge point R = F cosh s
+// (radial_edge) of one Gauss-Legendre node.  With EBEM_GL_ONEDIV (default;
+// the sphere of 1280 triangles 161 -> 157 ms per step against hyp() and
+// radial_edge(), which divide three times per node) the
+// reciprocals of e^s, 1 + e^2s, r' and r' + F (1 + e^2s) (r' = 2 e^s r) come
+// from one division: 1/e^s, 1/cosh, 1/(r (r + R)) and 1/r then cost
+// multiplications, and log(R + r) = log(r' + F (1 + e^2s)) - s - log 2.
+#ifndef EBEM_GL_ONEDIV
+#define EBEM_GL_ONEDIV 1
+#endif
+EBEM_DI void edge_point(double s, double Fc, double zeta, double& sech, double& th, Rad& v) {
+#if EBEM_GL_ONEDIV
+    const double e = m_exp(s), e2 = e * e, u = e2 + 1.0;
+    const double z2 = zeta * zeta, Fu = Fc * u;
+    const double rp = sqrt(Fu * Fu + 4.0 * z2 * e2);          // 2 e^s r
+    const double a = rp + Fu;                                 // 2 e^s (r + R)
+    const double ue = u * e, ra = rp * a;
+    const double inv = 1.0 / (ue * ra);
+    const double iu = e * ra * inv, ie = u * ra * inv, irp = ue * a * inv, ia = ue * rp * inv;
+    sech = 2.0 * e * iu;
+    th = (e2 - 1.0) * iu;
+    const double r = 0.5 * rp * ie, R = 0.5 * Fu * ie;
+    const double ir = 2.0 * e * irp, ir3 = ir * ir * ir;
+    v.A1 = r;
+    v.A3 = -ir;
+    v.B2 = r + z2 * ir;
+    v.D2 = -z2 * ir;
+    v.B4 = -ir + z2 * ir3 * (1.0 / 3.0);
+    v.D4 = -z2 * ir3 * (1.0 / 3.0);
+    if (zeta > 0) {
+        v.C2 = m_log(a) - (s + 0.69314718055994530942) - Fu * irp;
+        v.C4 = -(r * r + r * R + R * R) * ir3 * (2.0 * e * ia) * (1.0 / 3.0);
+    } else {
+        v.C2 = 0.0;
+        v.C4 = 0.0;
+    }
+#else
+    double ch;
+    hyp(s, ch, sech, th);
+    v = radial_edge(Fc * ch, zeta);
+#endif
+}
+
 // Moments of one child (child frame), this lane's share of the nodes
-// n = lane, lane + 32, ... of the whole-range rule.
+// n = lane, lane + 32, ... of the whole-range rule: sub-pieces of length
+// h <= EBEM_EDGE_H, 6, 8 or 10 Gauss-Legendre nodes each for h up to 1/4,
+// 1/2 or 1 (glx, glw: the table of gl_table_entry).
 EBEM_DI void moment_share(double m[14], double F, double cb, double sb, double zeta, double s1, double s0, int lane,
                           const double* glx, const double* glw) {
 #pragma unroll
@@ -138,14 +187,16 @@ EBEM_DI void moment_share(double m[14], double F, double cb, double sb, double z
     int nsub = (int)ceil(len * (1.0 / EBEM_EDGE_H));
     nsub = max(1, min(nsub, 4096));
     double h = len / nsub;
-    for (int idx = lane; idx < nsub * 10; idx += 32) {
-        int sub = idx / 10, q = idx - 10 * sub;
-        double s = s1 + (sub + 0.5) * h + 0.5 * h * glx[q];
-        double ch, sech, th;
-        hyp(s, ch, sech, th);
+    const int ng = (EBEM_GL_ADAPT && h <= 0.25) ? 6 : ((EBEM_GL_ADAPT && h <= 0.5) ? 8 : 10);
+    const int base = ng == 6 ? 0 : (ng == 8 ? 6 : 14);
+    for (int idx = lane; idx < nsub * ng; idx += 32) {
+        int sub = idx / ng, q = idx - ng * sub;
+        double s = s1 + (sub + 0.5) * h + 0.5 * h * glx[base + q];
+        double sech, th;
+        Rad v;
+        edge_point(s, F, zeta, sech, th, v);
         double c = th * cb + sech * sb, sn = sech * cb - th * sb;
-        Rad v = radial_edge(F * ch, zeta);
-        double f = 0.5 * h * glw[q] * sech;
+        double f = 0.5 * h * glw[base + q] * sech;
         double cc = c * c, sc = sn * c, ss = sn * sn;
         m[0] += f * v.A1;
         m[1] += f * v.A3;
