@@ -1088,7 +1088,13 @@ struct ebem_batch {
     BatchInst* d_insts = nullptr;
     unsigned long long* d_next = nullptr;  // work counter, reset inside the graph
     long long total = 0;
+    std::vector<PhysParams> params;
     int wpb = 4, chunk = 4;
+    // schedule: 0 the persistent launch over all instances, 1 one two-pass
+    // assembly per instance (captured in the same way; its graph holds the
+    // output pointers, so new outputs mean a new capture)
+    int sched = 0;
+    std::vector<double*> cap_E;            // outputs of the captured per-instance schedule
     float tuned_ms = -1.0f;
     bool tuned = false;
     cudaStream_t cap = nullptr;
@@ -1098,6 +1104,22 @@ struct ebem_batch {
 
 namespace {
 
+// One two-pass assembly per instance (the single-mesh path: level pass and
+// whole-sector emission), on the rule table the plan recorded.
+int batch_run_twopass(ebem_batch* b, cudaStream_t s) {
+    for (int k = 0; k < b->n; k++) {
+        const BatchInst& I = b->h_insts[k];
+        MeshData m = b->meshes[k]->d;
+        m.d_nodes = const_cast<NodeW*>(I.nodes);
+        m.nodes_rule = b->n_gh;
+        const size_t n3 = 3 * (size_t)I.N;
+        if (int rc = launch_sa_twopass(m, b->params[k], b->n_gh, 0, I.nlag, 0, I.N, I.E, n3, n3 * n3, 0, nullptr,
+                                       b->prec == EBEM_PREC_MIXED, s))
+            return rc;
+    }
+    return EBEM_OK;
+}
+
 int batch_run_direct(ebem_batch* b, int wpb, int chunk, cudaStream_t s) {
     EBEM_CUDA_TRY(cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), s));
     return launch_sa_batch(b->d_insts, b->n, b->total, b->n_gh, b->prec == EBEM_PREC_MIXED, wpb, chunk, b->d_next,
@@ -1106,34 +1128,13 @@ int batch_run_direct(ebem_batch* b, int wpb, int chunk, cudaStream_t s) {
 
 // Autotuner: time every (warps per block, pairs per grab) candidate once on the
 // batch itself and keep the fastest, then capture the launch in a CUDA graph.
-int batch_tune_and_capture(ebem_batch* b, cudaStream_t s) {
-    std::vector<int> wpbs = (3 * b->n_gh <= 32) ? std::vector<int>{2, 4} : std::vector<int>{2};
-    const int chunks[3] = {1, 4, 16};
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    EBEM_CUDA_TRY(cudaEventCreate(&e0));
-    EBEM_CUDA_TRY(cudaEventCreate(&e1));
-    int rc = batch_run_direct(b, wpbs.back(), 4, s);          // warm-up (module load, caches)
-    float best = 1e30f;
-    for (int w : wpbs)
-        for (int c : chunks) {
-            if (rc) break;
-            cudaEventRecord(e0, s);
-            rc = batch_run_direct(b, w, c, s);
-            cudaEventRecord(e1, s);
-            if (!rc && cudaEventSynchronize(e1) == cudaSuccess) {
-                float ms = 0.0f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (ms < best) { best = ms; b->wpb = w; b->chunk = c; }
-            }
-        }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (rc) return rc;
-    b->tuned_ms = best;
-    b->tuned = true;
+// Captures the chosen schedule into b->graph / b->exec (replacing any earlier one).
+int batch_capture(ebem_batch* b) {
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
     if (!b->cap) EBEM_CUDA_TRY(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
     EBEM_CUDA_TRY(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
-    int crc = batch_run_direct(b, b->wpb, b->chunk, b->cap);
+    int crc = b->sched == 1 ? batch_run_twopass(b, b->cap) : batch_run_direct(b, b->wpb, b->chunk, b->cap);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(b->cap, &g);
     if (crc) { if (g) cudaGraphDestroy(g); return crc; }
@@ -1141,7 +1142,54 @@ int batch_tune_and_capture(ebem_batch* b, cudaStream_t s) {
     b->graph = g;
     e = cudaGraphInstantiate(&b->exec, g, 0);
     if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("batch graph instantiation: ") + cudaGetErrorString(e));
+    b->cap_E.assign(b->n, nullptr);
+    for (int k = 0; k < b->n; k++) b->cap_E[k] = b->h_insts[k].E;
     return EBEM_OK;
+}
+
+// Autotuner: time every (warps per block, pairs per grab) candidate of the
+// persistent launch, and the per-instance two-pass schedule, once each on the
+// batch itself; keep the fastest and capture it in a CUDA graph.
+int batch_tune_and_capture(ebem_batch* b, cudaStream_t s) {
+    std::vector<int> wpbs = {2, 4};
+    const int chunks[3] = {1, 4, 16};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    EBEM_CUDA_TRY(cudaEventCreate(&e0));
+    EBEM_CUDA_TRY(cudaEventCreate(&e1));
+    int rc = batch_run_direct(b, wpbs.back(), 4, s);          // warm-up (module load, caches)
+    if (!rc) rc = batch_run_twopass(b, s);
+    float best = 1e30f;
+    auto timed = [&](auto&& run) -> float {
+        float ms = -1.0f;
+        cudaEventRecord(e0, s);
+        rc = run();
+        cudaEventRecord(e1, s);
+        if (!rc && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        return ms;
+    };
+    for (int w : wpbs)
+        for (int c : chunks) {
+            if (rc) break;
+            const float ms = timed([&] { return batch_run_direct(b, w, c, s); });
+            if (ms >= 0.0f && ms < best) { best = ms; b->wpb = w; b->chunk = c; b->sched = 0; }
+        }
+    if (!rc) {
+        const float ms = timed([&] { return batch_run_twopass(b, s); });
+        if (ms >= 0.0f && ms < best) { best = ms; b->sched = 1; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    b->tuned_ms = best;
+    b->tuned = true;
+    rc = batch_capture(b);
+    if (rc && b->sched == 1) {
+        // the per-instance schedule could not be captured: the persistent launch
+        cudaGetLastError();
+        b->sched = 0;
+        rc = batch_capture(b);
+    }
+    return rc;
 }
 
 }  // namespace
@@ -1209,6 +1257,7 @@ int ebem_batch_create(const ebem_mesh* const* meshes, const ebem_problem* probs,
         I.pair_begin = begin;
         begin += (long long)md.nt * md.nt;
         b->meshes.push_back(meshes[k]);
+        b->params.push_back(P);
         b->nlag.push_back(nl);
     }
     b->total = begin;
@@ -1230,6 +1279,11 @@ int ebem_batch_assemble(ebem_batch* b, double* const* E, void* stream) {
     EBEM_CUDA_TRY(cudaMemcpyAsync(b->d_insts, b->h_insts, sizeof(BatchInst) * b->n, cudaMemcpyHostToDevice, s));
     if (!b->tuned) {
         if (int rc = batch_tune_and_capture(b, s)) return rc;
+    } else if (b->sched == 1) {
+        bool same = true;
+        for (int k = 0; k < b->n; k++) same = same && b->cap_E[k] == E[k];
+        if (!same)
+            if (int rc = batch_capture(b)) return rc;
     }
     EBEM_CUDA_TRY(cudaGraphLaunch(b->exec, s));
     // the pinned table must not change before this call's copy has run
