@@ -236,6 +236,8 @@ def forms(core, problem, torch, w, dm, L, plain_rate):
                       "pair_integrals": int(sum(counts)),
                       "batch_ms": t_batch, "one_launch_per_instance_ms": t_seq, "speedup": t_seq / t_batch,
                       "batch_mixed_ms": t_b32, "pair_integrals_per_s": sum(counts) / t_batch * 1e3,
+                      "schedule": ("persistent launch over all instances" if info["warps_per_block"]
+                                   else "one two-pass assembly per instance"),
                       "tile": {"warps_per_block": info["warps_per_block"], "pairs_per_grab": info["pairs_per_grab"]}}
     plan.close(); plan32.close()
     del outs

@@ -1294,8 +1294,9 @@ int ebem_batch_assemble(ebem_batch* b, double* const* E, void* stream) {
 int ebem_batch_info(const ebem_batch* b, int* warps_per_block, int* pairs_per_grab, float* tuned_ms,
                     long long* pairs) {
     if (!b) return fail(EBEM_ERR_INVALID, "batch is NULL");
-    if (warps_per_block) *warps_per_block = b->wpb;
-    if (pairs_per_grab) *pairs_per_grab = b->chunk;
+    // 0 and 0: the per-instance schedule was chosen
+    if (warps_per_block) *warps_per_block = b->sched == 1 ? 0 : b->wpb;
+    if (pairs_per_grab) *pairs_per_grab = b->sched == 1 ? 0 : b->chunk;
     if (tuned_ms) *tuned_ms = b->tuned_ms;
     if (pairs) *pairs = b->total;
     return EBEM_OK;

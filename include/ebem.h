@@ -204,15 +204,20 @@ int ebem_assemble_sa_noalloc(const ebem_mesh* mesh, const ebem_problem* prob, in
  * instances, so small and large meshes share the GPU without tail effects.
  * ebem_batch_create records the instances (nlag may be NULL: L of each
  * instance; instance k assembles lags 0..nlag[k]-1) with one outer rule and
- * precision mode.  The first ebem_batch_assemble tunes the tile shape (warps
- * per block x pairs per grab, each candidate timed once on the batch) and
- * captures the launch in a CUDA graph; every call replays the graph.  E[k]:
+ * precision mode.  The first ebem_batch_assemble tunes the schedule: the
+ * persistent launch's tile shape (warps per block x pairs per grab) and, as
+ * one more candidate, one two-pass assembly per instance, each timed once on
+ * the batch; it captures the fastest in a CUDA graph and every call replays
+ * the graph (the persistent launch reads the outputs from a device table at
+ * run time; the per-instance schedule is recaptured when a call passes other
+ * output buffers than the captured ones).  E[k]:
  * device buffer of 9 N_k^2 nlag[k] doubles, same layout as ebem_assemble_sa,
  * every entry written; results equal ebem_assemble_sa's to rounding (the
  * same per-pair computation in another kernel).  The plan reads its meshes'
  * device data at every replay: destroy it before any of its meshes (using
  * the meshes in other calls meanwhile, with any rule, is fine).
- * ebem_batch_info reports the chosen shape, its tuning time and the pair count. */
+ * ebem_batch_info reports the chosen shape (0 and 0 for the per-instance
+ * schedule), its tuning time and the pair count. */
 typedef struct ebem_batch ebem_batch;
 int ebem_batch_create(const ebem_mesh* const* meshes, const ebem_problem* probs, const int* nlag, int n, int n_gh,
                       int prec, ebem_batch** out);
