@@ -12,15 +12,17 @@
 //   edge distance    SA/calcoloMatrice/operazioniGeometriche/calcoloDistanzaTriangolo.m
 //   children         SA/calcoloMatrice/BEMenerg_coreSA_calcIntgInt_fieldTriangle.m:13-84
 //
-// Work decomposition (B200 design, not the reference's): one thread per
-// (source i, field j) pair; consecutive lanes take consecutive source
-// triangles of the same field triangle, so a warp writes 3 x 32 x 3
-// contiguous doubles per block column.  A thread walks the time levels
-// t_k = k dt of its pair once, in increasing order; F(t_k) (the combined
-// kernel integral at one instant) depends on k only, so each level is
-// evaluated once and E_l = F_{l+1} - 2 F_l + F_{l-1} is emitted from a
-// three-level sliding window (the reference evaluates every instant three
-// times, once per lag that uses it).
+// Work decomposition (B200 design, not the reference's): one warp per
+// (source i, field j) pair walks the pair's time levels t_k = k dt once, in
+// increasing order, with the lanes on the children of the outer nodes
+// (sa_warp.cuh; level_pair below).  F(t_k), the combined kernel integral at
+// one instant, depends on k only, so each level is evaluated once and
+// E_l = F_{l+1} - 2 F_l + F_{l-1} is formed from three levels (the
+// reference evaluates every instant three times, once per lag that uses
+// it).  Dense outputs store the levels and write the blocks in a second,
+// coalesced pass (sa_twopass.cu); the other modes write the blocks directly.
+// A thread-per-pair kernel (sa_assemble_kernel) remains for builds with
+// EBEM_SA_KERNEL=1.
 #include "ebem_internal.h"
 
 #include <algorithm>
@@ -29,7 +31,7 @@
 #include "sa_warp.cuh"
 
 #ifndef EBEM_SA_KERNEL
-#define EBEM_SA_KERNEL 0    // 0: warp per pair when 3 n_gh <= 32, 1: always thread per pair
+#define EBEM_SA_KERNEL 0    // 0: the warp-per-pair level kernel, 1: thread per pair
 #endif
 #ifndef EBEM_SA_TWOPASS
 #define EBEM_SA_TWOPASS 1   // 1: dense assemblies store F(t_k) and emit the blocks in a second pass (sa_twopass.cu)
