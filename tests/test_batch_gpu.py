@@ -1,5 +1,6 @@
-"""Batched form: many instances of uneven size in one persistent,
-graph-captured launch with an autotuned tile shape, against the binary128
+"""Batched form: many instances of uneven size in one graph-captured
+schedule chosen by the autotuner (a persistent launch with a tuned tile
+shape, or one two-pass assembly per instance), against the binary128
 value of the reference's formulas on sampled blocks of every instance (all
 lags), and against the single-mesh assembly of each instance (the same
 per-pair computation in another kernel) in FP64 and in the mixed-precision
@@ -41,7 +42,8 @@ def test_batch_equals_single(ebem, n_gh, prec):
             assert torch.isfinite(g).all()
             assert float((g - s1).norm() / s1.norm()) <= (TOL_MIXED if prec else TOL)
     info = plan.info()
-    assert info["warps_per_block"] in (2, 4) and info["pairs_per_grab"] in (1, 4, 16)
+    # 0 / 0: the per-instance schedule won the tuning
+    assert (info["warps_per_block"], info["pairs_per_grab"]) in {(w, c) for w in (2, 4) for c in (1, 4, 16)} | {(0, 0)}
     assert info["tuned_ms"] > 0 and info["pairs"] == sum(d.N ** 2 for d in dms)
 
 
