@@ -102,6 +102,14 @@ def test_argument_checks_before_any_device_use(lib):
     assert lib.ebem_pp_sa(None, None, None, None, 1, None, 1, None, None) == -1
     assert lib.ebem_march(None, 3, 1, None, 1, None, None) == -1
     assert lib.ebem_batch_create(None, None, None, 0, 7, 0, C.byref(out)) == -1
+    # the selector's entry points and the composite-rule blocks
+    assert lib.ebem_sa_pair_blocks(None, None, 7, 4, None, 8, 3, None, None) == -1
+    assert lib.ebem_selector_sweeps(None, None, None, 8, None, None) == -1
+    assert lib.ebem_selector_labels(None, -1, 1e-10, 1.0, None, None, None) == -1
+    assert lib.ebem_selector_labels(None, 8, 1e-10, 1.0, None, None, None) == -1
+    assert lib.ebem_selector_infer(None, None, None, 0.9, 0, 4, None, None, None) == -1
+    assert lib.ebem_assemble_sa_selected(None, None, None, 4, None, 0, 4, None, 0, None, None) == -1
+    assert lib.ebem_selector_labels(None, 0, 1e-10, 1.0, None, None, None) == 0      # nothing to label
 
 
 def test_device_state_release_without_device(lib):
