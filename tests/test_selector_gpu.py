@@ -188,3 +188,40 @@ def test_trained_selector_gain(ebem):
         assert t_sel <= 1.05 * t_max
         del buf
         torch.cuda.empty_cache()
+
+
+def test_rule_selection_bound(ebem):
+    """What any selector over these rules can save, with the labels themselves
+    as the classes (a perfect network) on the sphere of 320 triangles
+    (configuration 2's material and time step): at the labels' tolerance the
+    density is within 1e-6 of the maximal rule, and the outer nodes the
+    selected lags use are still more than a fifth of the maximal rule's, so
+    no choice among these rules reaches the 5x of the forms' target (most
+    non-null blocks have a wavefront crossing their field triangle, where the
+    outer rule converges only algebraically)."""
+    import torch
+    from elastodynamicebem_b200 import problem
+    from elastodynamicebem_b200 import selector as S
+    w = problem.sphere_workload(7, 2)
+    dm = ebem.DeviceMesh(w.mesh)
+    N, L = dm.N, ebem.num_blocks(dm, w.params)
+    E = [ebem.assemble_sa_rule(dm, w.params, n, s, 0, L).clone().reshape(L, N, 3, N, 3) for n, s in S.RULES]
+    D = S.diagonal_scales(dm, w.params)
+    thr = S.TOL * torch.sqrt(D[:, None] * D[None, :])[None]                     # (1, N_src, N_fld)
+    nonnull = E[-1].abs().amax(dim=(2, 4)) > 0                                    # (L, N_src, N_fld)
+    lab = torch.full((L, N, N), len(S.RULES) - 1, dtype=torch.uint8, device="cuda")
+    for c in range(len(S.RULES) - 2, -1, -1):
+        lab[(E[c] - E[-1]).abs().amax(dim=(2, 4)) <= thr] = c
+    cls = lab.permute(2, 1, 0).reshape(N * N, L).contiguous()                    # row = field * N + source
+    Es, counts = ebem.assemble_sa_selected(dm, w.params, cls, S.RULES, 0, L)
+    b = ebem.rhs(dm, w.params, 7, w.datum)
+    phi = ebem.march(Es.clone(), b)
+    phi_max = ebem.march(ebem.assemble_sa_rule(dm, w.params, *S.RULES[-1], 0, L), b)
+    err = float((phi - phi_max).norm() / phi_max.norm())
+    nodes = torch.tensor([n * s for n, s in S.RULES], dtype=torch.float64, device="cuda")
+    used = float(nodes[lab[nonnull].long()].sum())
+    full = float(nonnull.sum()) * float(nodes[-1])
+    print(f"\nperfect labels on {w.name}: non-null lags per class {counts}; density error {err:.2e}; "
+          f"outer nodes used {used / full:.3f} of the maximal rule's")
+    assert err <= 1e-6
+    assert used / full > 0.2
