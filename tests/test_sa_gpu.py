@@ -117,11 +117,13 @@ def test_host_output_matches_device(ebem):
     m, prm = _case("screen32")
     dm = ebem.DeviceMesh(m)
     L = ebem.num_blocks(dm, prm)
-    dev = ebem.assemble_sa(dm, prm, 7, 0, L).cpu()
+    dev, cd = ebem.assemble_sa(dm, prm, 7, 0, L, count=True)
     n3 = 3 * m.numberTriangles
     host = torch.empty((L, n3, n3), dtype=torch.float64).pin_memory()
-    h = ebem.assemble_sa(dm, prm, 7, 0, L, out=host)
-    assert torch.equal(h, dev)
+    # the host path assembles in source-row sub-panels: the count sums them
+    h, ch = ebem.assemble_sa(dm, prm, 7, 0, L, out=host, count=True)
+    assert torch.equal(h, dev.cpu())
+    assert ch == cd
 
 
 def test_host_output_pipeline(ebem):
