@@ -631,7 +631,7 @@ __global__ void __launch_bounds__(128) pp_sa_kernel(const TriGeom* __restrict__ 
 // by value; pp_inst_level_kernel evaluates M once per (triangle, point,
 // distinct instant) and pp_inst_sum_kernel contracts, one block per
 // (time, point).
-__global__ void __launch_bounds__(128) pp_inst_level_kernel(const TriGeom* __restrict__ geo, int N,
+__global__ void __launch_bounds__(128, 6) pp_inst_level_kernel(const TriGeom* __restrict__ geo, int N,
                                                             const double* __restrict__ pts, int p0, int np, int nu,
                                                             const double* __restrict__ taus, double velP, double velS,
                                                             double c4, double* __restrict__ Mbuf) {
@@ -642,7 +642,11 @@ __global__ void __launch_bounds__(128) pp_inst_level_kernel(const TriGeom* __res
     // 0.97 ms for 64 points x 40 grid times on 320 triangles, 12.1 against
     // 11.7 ms for 256 points on 1280).  A buffer ordered (point, triangle,
     // instant), which makes these stores contiguous, made the contraction's
-    // loads strided: 1.8 -> 5.8 ms on 1280.
+    // loads strided: 1.8 -> 5.8 ms on 1280.  At most 80 registers (6 blocks
+    // of 128 threads per SM): with 200 registers 2 blocks fitted, 1.5 warps
+    // per scheduler waited on the FP64 dependencies of one evaluation, and
+    // the spills this cap adds cost less than the occupancy gains.
+    // 11.7 -> 7.0 ms on 1280 triangles (128 registers: 7.4 ms; 102: 7.2 ms).
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)N * np * nu) return;
     const int ui = (int)(idx % nu);
