@@ -431,7 +431,11 @@ __host__ __device__ __forceinline__ void k_pair(double out[9], const double x[3]
                              b3 * w[i] * x[k] - b4 * u[3 * i + k];
 }
 
-__global__ void __launch_bounds__(128) k_assemble_kernel(KArgs A) {
+// Register caps of the double-layer kernels, from an A/B of builds on the
+// 448- and 2800-triangle bars (rule 7/4/3): the thread kernel at 128
+// registers (4 blocks per SM: 725 -> 633 ms; 80 registers 721 ms), the warp
+// kernel at 80 (6 blocks per SM: 28.8 -> 23.4 ms; 128 registers 24.3 ms).
+__global__ void __launch_bounds__(128, 4) k_assemble_kernel(KArgs A) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= (long long)A.N * A.Nv) return;
     const int x = (int)(p % A.N), s = (int)(p / A.N);
@@ -511,7 +515,7 @@ __global__ void __launch_bounds__(128) k_assemble_kernel(KArgs A) {
 // Warp-per-pair variant of k_assemble_kernel: one warp per (triangle x,
 // vertex s), the lanes over the node pairs (star triangle of s, inner node,
 // outer node), the same per-node-pair arithmetic, a warp reduction per lag.
-__global__ void __launch_bounds__(128) k_assemble_warp_kernel(KArgs A) {
+__global__ void __launch_bounds__(128, 6) k_assemble_warp_kernel(KArgs A) {
     const int lane = threadIdx.x & 31;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -943,7 +947,10 @@ __device__ __forceinline__ void warp_add3(double* dst, double v0, double v1, dou
 // Block (x-tile, evaluation, chunk c) takes the slices n in
 // [c kchunk + 1, (c + 1) kchunk] and evaluates G at the levels n_lo - 1 .. n_hi
 // (one level more than its slices), so that short meshes still fill the GPU.
-__global__ void __launch_bounds__(128) pp_g_kernel(PPArgs A, int kchunk) {
+// kernelG / kernelP evaluations capped at 128 registers (4 blocks per SM):
+// 16 points x 4 times on the 448-triangle bar 3.51 -> 3.23 ms (80 registers:
+// 3.63 ms, the spills then cost more than the occupancy gains).
+__global__ void __launch_bounds__(128, 4) pp_g_kernel(PPArgs A, int kchunk) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int ev = blockIdx.y;                          // evaluation index q * npts + ip
     const int q = ev / A.npts, ip = ev % A.npts;
@@ -1004,7 +1011,7 @@ __global__ void __launch_bounds__(128) pp_g_kernel(PPArgs A, int kchunk) {
 // P part: minus the sum over slices n of clamp(P_{n-1} - 2 P_n + P_{n+1}) / (4 pi rho dt) b_n.
 // Chunked over the slices as pp_g_kernel; a chunk evaluates P at the levels
 // n_lo - 1 .. n_hi + 1.
-__global__ void __launch_bounds__(128) pp_p_kernel(PPArgs A, int kchunk) {
+__global__ void __launch_bounds__(128, 4) pp_p_kernel(PPArgs A, int kchunk) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int ev = blockIdx.y;
     const int q = ev / A.npts, ip = ev % A.npts;

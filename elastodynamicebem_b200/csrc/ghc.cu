@@ -103,7 +103,7 @@ __host__ __device__ __forceinline__ void ghc_pair(double nu[6], const double x[3
     nu[5] = g1 * x[2] * x[2] + g2;
 }
 
-__global__ void __launch_bounds__(128) ghc_assemble_kernel(GHCArgs A) {
+__global__ void __launch_bounds__(128, 6) ghc_assemble_kernel(GHCArgs A) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= (long long)A.N * A.N) return;
     const int i = (int)(p % A.N);          // source (outer rule)
@@ -189,8 +189,13 @@ __global__ void __launch_bounds__(128) ghc_assemble_kernel(GHCArgs A) {
 // take the node pairs (inner node q, outer node o) of the pair, the same
 // per-node-pair arithmetic as ghc_assemble_kernel, and a warp reduction per
 // lag gives the 6 entries (the thread kernel leaves half of each warp's
-// lanes idle on the skip test and keeps 7 warps per SM busy).
-__global__ void __launch_bounds__(128) ghc_assemble_warp_kernel(GHCArgs A) {
+// lanes idle on the skip test).  Both kernels are capped at 80 registers (6
+// blocks of 128 threads per SM); with the compiler's 157 and 170 registers
+// 3 blocks fitted and the FP64 dependency chains were not hidden: sphere of
+// 320 triangles, rule 7/16/3 13.7 -> 6.6 ms (warp kernel); bar of 2800
+// triangles, rule 7/4/3 188 -> 137 ms (thread kernel); 128 registers gave
+// 7.3 and 152 ms.
+__global__ void __launch_bounds__(128, 6) ghc_assemble_warp_kernel(GHCArgs A) {
     const int lane = threadIdx.x & 31;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
