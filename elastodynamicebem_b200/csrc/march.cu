@@ -568,6 +568,42 @@ __device__ __forceinline__ void sym_mv_add(double acc[3], const double M[6], con
     acc[2] += sgn * (M[2] * ph[0] + M[4] * ph[1] + M[5] * ph[2]);
 }
 
+// The instants at which M(tau) of triangle F seen from x is zero without
+// evaluating it: the P front (radius velP tau) has not reached the triangle.
+// M is zero when the closed form's case split finds no front at the node
+// (T_NONE), which needs velP tau <= sqrt(zeta^2 + dMIN^2) as the
+// projection computes them; that is at least the distance from x to the
+// triangle less the projection's tolerances (the plane distance snapped to
+// 0 below 1e-6, the inside test's 1e-6 on the barycentrics, the edge foot
+// tests' 1e-6, which can take a foot up to 1e-6 / |edge| <= 1e-6 maxL / (2
+// area) beyond an end), and that distance is at least the centroid distance
+// less the longest edge.  pp_reach returns that bound less a margin of half
+// the longest edge on top of the tolerances; an instant with velP tau below
+// it is skipped.  Rounded explicitly (no contraction): the evaluation pass
+// and the contraction must take the same decision for every instant.
+__device__ __forceinline__ double pp_reach(const TriGeom& F, const NodeW& x) {
+    const double d0 = __dsub_rn(x.x, F.ctr[0]), d1 = __dsub_rn(x.y, F.ctr[1]), d2 = __dsub_rn(x.z, F.ctr[2]);
+    const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
+    const double tol = __dadd_rn(__dadd_rn(__dmul_rn(0.5, F.maxL), 1.0e-5),
+                                 __dadd_rn(__ddiv_rn(__dmul_rn(1.0e-6, F.maxL), F.area), __dmul_rn(1.0e-12, r)));
+    return __dsub_rn(__dsub_rn(r, F.maxL), tol);     // a degenerate triangle (area 0) gives -inf: never skipped
+}
+
+__device__ __forceinline__ bool pp_before_front(double reach, double velP, double tau) {
+    return __dmul_rn(velP, tau) < reach;
+}
+
+// pp_block, or zero at an instant before the P front reaches the triangle.
+__device__ __forceinline__ void pp_block_or_zero(double M[6], const TriGeom& F, const NodeW& x, double reach,
+                                                 double tau, double velP, double velS, double c4) {
+    if (pp_before_front(reach, velP, tau)) {
+#pragma unroll
+        for (int e = 0; e < 6; e++) M[e] = 0.0;
+    } else {
+        pp_block(M, F, x, tau, velP, velS, c4);
+    }
+}
+
 __global__ void __launch_bounds__(128) pp_sa_kernel(const TriGeom* __restrict__ geo, int N, const double* __restrict__ pts,
                                                     int npts, const double* __restrict__ times, int ntimes,
                                                     const double* __restrict__ phi, int nT, double velP, double velS,
@@ -590,9 +626,10 @@ __global__ void __launch_bounds__(128) pp_sa_kernel(const TriGeom* __restrict__ 
         int nHat = (int)ceil(t / dt) - 1;
         if (nHat > nT - 1) nHat = nT - 1;
         double Mc[6], Mn[6];
-        pp_block(Mc, F, x, t, velP, velS, c4);
+        const double reach = pp_reach(F, x);
+        pp_block_or_zero(Mc, F, x, reach, t, velP, velS, c4);
         for (int k = 1; k <= nHat; k++) {
-            pp_block(Mn, F, x, __dsub_rn(t, __dmul_rn((double)k, dt)), velP, velS, c4);   // no fused multiply-add
+            pp_block_or_zero(Mn, F, x, reach, __dsub_rn(t, __dmul_rn((double)k, dt)), velP, velS, c4);   // no fused multiply-add
             const double* ph = phi + (size_t)(k - 1) * n3 + 3 * (size_t)j;
             double D[6];
 #pragma unroll
@@ -655,6 +692,9 @@ __global__ void __launch_bounds__(128, 6) pp_inst_level_kernel(const TriGeom* __
     const int p = p0 + pl;
     NodeW x;
     x.x = pts[3 * p]; x.y = pts[3 * p + 1]; x.z = pts[3 * p + 2]; x.w = 1.0;
+    // instants before the P front reaches the triangle (most of them) are
+    // neither evaluated nor stored: the contraction skips them too
+    if (pp_before_front(pp_reach(geo[j], x), velP, taus[ui])) return;
     double M[6];
     pp_block(M, geo[j], x, taus[ui], velP, velS, c4);
     double* dst = Mbuf + (((size_t)pl * nu + ui) * N + j) * 6;
@@ -662,17 +702,24 @@ __global__ void __launch_bounds__(128, 6) pp_inst_level_kernel(const TriGeom* __
     for (int e = 0; e < 6; e++) dst[e] = M[e];
 }
 
-__global__ void __launch_bounds__(128) pp_inst_sum_kernel(const double* __restrict__ Mbuf, int N, int p0, int np,
-                                                          int nu, const int* __restrict__ tab, int kmax,
+__global__ void __launch_bounds__(128) pp_inst_sum_kernel(const double* __restrict__ Mbuf, const TriGeom* __restrict__ geo,
+                                                          int N, const double* __restrict__ pts, int p0, int np, int nu,
+                                                          const double* __restrict__ taus, double velP,
+                                                          const int* __restrict__ tab, int kmax,
                                                           const int* __restrict__ nhat, int npts,
                                                           const double* __restrict__ phi, double* __restrict__ u) {
     const int q = blockIdx.x / np, pl = blockIdx.x - q * np;
     const int nh = nhat[q];
     const int* tq = tab + (size_t)q * kmax;
     const size_t n3 = 3 * (size_t)N;
+    const int p = p0 + pl;
+    NodeW x;
+    x.x = pts[3 * p]; x.y = pts[3 * p + 1]; x.z = pts[3 * p + 2]; x.w = 1.0;
     double acc[3] = {0, 0, 0};
-    for (int j = threadIdx.x; j < N; j += blockDim.x)
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        const double reach = pp_reach(geo[j], x);
         for (int k = 0; k <= nh; k++) {
+            if (pp_before_front(reach, velP, taus[tq[k]])) continue;    // M = 0, not stored
             const double* Mv = Mbuf + (((size_t)pl * nu + tq[k]) * N + j) * 6;
             const double* pk = phi + (size_t)k * n3 + 3 * (size_t)j;
             double d[3] = {pk[0], pk[1], pk[2]};
@@ -686,6 +733,7 @@ __global__ void __launch_bounds__(128) pp_inst_sum_kernel(const double* __restri
             for (int e = 0; e < 6; e++) Ml[e] = Mv[e];
             sym_mv_add(acc, Ml, d, 1.0);
         }
+    }
     __shared__ double red[3][4];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -759,8 +807,9 @@ static int launch_pp_sa_shared(const MeshData& m, const PhysParams& P, const dou
         const long long lv = (long long)m.nt * np * nu;
         pp_inst_level_kernel<<<(unsigned)((lv + 127) / 128), 128, 0, s>>>(m.d_geo, m.nt, d_pts, p0, np, nu, d_taus,
                                                                          P.velP, P.velS, 4 * kPi * P.rho, Mbuf);
-        pp_inst_sum_kernel<<<(unsigned)((long long)ntimes * np), 128, 0, s>>>(Mbuf, m.nt, p0, np, nu, d_tab, kmax, d_nh,
-                                                                              npts, d_phi, d_u);
+        pp_inst_sum_kernel<<<(unsigned)((long long)ntimes * np), 128, 0, s>>>(Mbuf, m.d_geo, m.nt, d_pts, p0, np, nu,
+                                                                              d_taus, P.velP, d_tab, kmax, d_nh, npts,
+                                                                              d_phi, d_u);
         e = cudaGetLastError();
     }
     ws_free(Mbuf, s);
