@@ -111,8 +111,9 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(long long* __r
         }
 }
 
-// in-place exclusive prefix sum of n values (n <= 2^30 blocks of 1024)
-static int exclusive_scan(long long* d, long long n, cudaStream_t s) {
+// in-place exclusive prefix sum of n values (n <= 2^30 blocks of 1024);
+// returns after the stream has finished it
+int exclusive_scan(long long* d, long long n, cudaStream_t s) {
     const long long nb = (n + kScanBlock - 1) / kScanBlock;
     long long* sums = nullptr;
     EBEM_CUDA_TRY(ws_malloc(&sums, nb * sizeof(long long), s));
@@ -122,7 +123,7 @@ static int exclusive_scan(long long* d, long long n, cudaStream_t s) {
     cudaError_t e = cudaGetLastError();
     ws_free(sums, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("band structure scan: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("prefix sum: ") + cudaGetErrorString(e));
     return EBEM_OK;
 }
 

@@ -179,6 +179,9 @@ struct BandOp {
     int* lo = nullptr;
 };
 int band_structure(const MeshData& m, const PhysParams& P, int L, BandOp* op, cudaStream_t s);
+// In-place exclusive prefix sum of n values on stream s (banded.cu); returns
+// after the stream has finished it.
+int exclusive_scan(long long* d, long long n, cudaStream_t s);
 void band_free(BandOp* op);
 int band_to_dense(const BandOp& op, int lag0, int nlag, double* d_E, cudaStream_t s);
 int band_march(const BandOp& op, const double* d_rhs, int nT, double* d_phi, cudaStream_t s);

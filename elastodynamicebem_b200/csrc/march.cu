@@ -604,7 +604,10 @@ __device__ __forceinline__ void pp_block_or_zero(double M[6], const TriGeom& F, 
     }
 }
 
-__global__ void __launch_bounds__(128) pp_sa_kernel(const TriGeom* __restrict__ geo, int N, const double* __restrict__ pts,
+// At most 128 registers (4 blocks of 128 threads per SM; 254 without the
+// cap): 40 scattered times at 256 points on the 1280-triangle sphere 37.1 ->
+// 27.6 ms.
+__global__ void __launch_bounds__(128, 4) pp_sa_kernel(const TriGeom* __restrict__ geo, int N, const double* __restrict__ pts,
                                                     int npts, const double* __restrict__ times, int ntimes,
                                                     const double* __restrict__ phi, int nT, double velP, double velS,
                                                     double dt, double c4, double* __restrict__ u) {
@@ -665,36 +668,75 @@ __global__ void __launch_bounds__(128) pp_sa_kernel(const TriGeom* __restrict__ 
 // fused multiply-add: the closed form's case selection is discontinuous
 // where a front radius equals the point's distance from the plane, so an
 // instant one unit in the last place off can change M there), deduplicated
-// by value; pp_inst_level_kernel evaluates M once per (triangle, point,
-// distinct instant) and pp_inst_sum_kernel contracts, one block per
-// (time, point).
-__global__ void __launch_bounds__(128, 6) pp_inst_level_kernel(const TriGeom* __restrict__ geo, int N,
+// by value; pp_inst_count_kernel finds, per (point, triangle) row, the first
+// instant that the P front reaches (the instants are sorted, so the skipped
+// ones come first), a prefix sum numbers the evaluated items, and
+// pp_inst_level_kernel evaluates M once per (triangle, point, distinct
+// evaluated instant); pp_inst_sum_kernel contracts, one block per (time,
+// point).
+__global__ void __launch_bounds__(128) pp_inst_count_kernel(const TriGeom* __restrict__ geo, int N,
                                                             const double* __restrict__ pts, int p0, int np, int nu,
-                                                            const double* __restrict__ taus, double velP, double velS,
-                                                            double c4, double* __restrict__ Mbuf) {
-    // instants fastest: the lanes of a warp take neighbouring instants of one
-    // (triangle, point), which mostly meet the fronts in the same way, and
-    // share its geometry loads (triangles fastest, the stores of a warp were
-    // contiguous but its lanes took more distinct branches: 1.34 against
-    // 0.97 ms for 64 points x 40 grid times on 320 triangles, 12.1 against
-    // 11.7 ms for 256 points on 1280).  A buffer ordered (point, triangle,
-    // instant), which makes these stores contiguous, made the contraction's
-    // loads strided: 1.8 -> 5.8 ms on 1280.  At most 80 registers (6 blocks
-    // of 128 threads per SM): with 200 registers 2 blocks fitted, 1.5 warps
-    // per scheduler waited on the FP64 dependencies of one evaluation, and
-    // the spills this cap adds cost less than the occupancy gains.
-    // 11.7 -> 7.0 ms on 1280 triangles (128 registers: 7.4 ms; 102: 7.2 ms).
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long long)N * np * nu) return;
-    const int ui = (int)(idx % nu);
-    const long long r = idx / nu;
-    const int j = (int)(r % N), pl = (int)(r / N);
+                                                            const double* __restrict__ taus, double velP,
+                                                            long long* __restrict__ cnt, int* __restrict__ first) {
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long rows = (long long)N * np;
+    if (r == 0) cnt[rows] = 0;            // becomes the total after the exclusive scan
+    if (r >= rows) return;
+    const int pl = (int)(r / N), j = (int)(r - (long long)pl * N);
     const int p = p0 + pl;
     NodeW x;
     x.x = pts[3 * p]; x.y = pts[3 * p + 1]; x.z = pts[3 * p + 2]; x.w = 1.0;
-    // instants before the P front reaches the triangle (most of them) are
-    // neither evaluated nor stored: the contraction skips them too
-    if (pp_before_front(pp_reach(geo[j], x), velP, taus[ui])) return;
+    const double reach = pp_reach(geo[j], x);
+    // the skip test is monotone in the sorted instants: first instant not skipped
+    int lo = 0, hi = nu;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (pp_before_front(reach, velP, taus[mid])) lo = mid + 1;
+        else hi = mid;
+    }
+    first[r] = lo;
+    cnt[r] = nu - lo;
+}
+
+__global__ void __launch_bounds__(128, 6) pp_inst_level_kernel(const TriGeom* __restrict__ geo, int N,
+                                                            const double* __restrict__ pts, int p0, int np, int nu,
+                                                            const double* __restrict__ taus, double velP, double velS,
+                                                            double c4, const long long* __restrict__ off,
+                                                            const int* __restrict__ first, long long total,
+                                                            double* __restrict__ Mbuf) {
+    // Items numbered row by row ((point, triangle) rows, triangles fastest),
+    // the evaluated instants of a row consecutive: the lanes of a warp take
+    // neighbouring instants of one (triangle, point), which mostly meet the
+    // fronts in the same way, and 32 evaluations whatever the skipped
+    // instants (97 % of them on the 1280-triangle sphere with 256 points;
+    // warps over all the instants of a row mixed skipped and evaluated lanes:
+    // 4.6 ms there).  Triangles fastest over all instants took more distinct
+    // branches (1.34 against 0.97 ms for 64 points x 40 grid times on 320
+    // triangles before the skip); a buffer ordered (point, triangle,
+    // instant), which makes the stores contiguous, made the contraction's
+    // loads strided (1.8 -> 5.8 ms on 1280).  At most 80 registers (6 blocks
+    // of 128 threads per SM): with 200 registers 2 blocks fitted, 1.5 warps
+    // per scheduler waited on the FP64 dependencies of one evaluation, and
+    // the spills this cap adds cost less than the occupancy gains (11.7 ->
+    // 7.0 ms on 1280 triangles before the skip; 128 registers: 7.4 ms).
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    // the row: last r with off[r] <= idx (off: exclusive prefix sums of the
+    // rows' counts, off[rows] = total; an empty row shares its offset with
+    // the next one)
+    const long long rows = (long long)N * np;
+    long long lo = 0, hi = rows;
+    while (hi - lo > 1) {
+        const long long mid = (lo + hi) >> 1;
+        if (off[mid] <= idx) lo = mid;
+        else hi = mid;
+    }
+    const long long r = lo;
+    const int ui = first[r] + (int)(idx - off[r]);
+    const int pl = (int)(r / N), j = (int)(r - (long long)pl * N);
+    const int p = p0 + pl;
+    NodeW x;
+    x.x = pts[3 * p]; x.y = pts[3 * p + 1]; x.z = pts[3 * p + 2]; x.w = 1.0;
     double M[6];
     pp_block(M, geo[j], x, taus[ui], velP, velS, c4);
     double* dst = Mbuf + (((size_t)pl * nu + ui) * N + j) * 6;
@@ -788,25 +830,43 @@ static int launch_pp_sa_shared(const MeshData& m, const PhysParams& P, const dou
     }
     const size_t per_point = (size_t)nu * m.nt * 6 * sizeof(double);
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)npts, ((size_t)1 << 30) / per_point));
-    int *d_tab = nullptr, *d_nh = nullptr;
+    int *d_tab = nullptr, *d_nh = nullptr, *d_first = nullptr;
     double *d_taus = nullptr, *Mbuf = nullptr;
+    long long* d_cnt = nullptr;
+    const long long rows_max = (long long)m.nt * chunk;
     if (ws_malloc(&d_tab, tab.size() * sizeof(int), s) != cudaSuccess ||
         ws_malloc(&d_nh, ntimes * sizeof(int), s) != cudaSuccess ||
-        ws_malloc(&d_taus, nu * sizeof(double), s) != cudaSuccess || ws_malloc(&Mbuf, per_point * chunk, s) != cudaSuccess) {
+        ws_malloc(&d_taus, nu * sizeof(double), s) != cudaSuccess ||
+        ws_malloc(&d_cnt, (rows_max + 1) * sizeof(long long), s) != cudaSuccess ||
+        ws_malloc(&d_first, rows_max * sizeof(int), s) != cudaSuccess || ws_malloc(&Mbuf, per_point * chunk, s) != cudaSuccess) {
         ws_free(d_tab, s);
         ws_free(d_nh, s);
         ws_free(d_taus, s);
+        ws_free(d_cnt, s);
+        ws_free(d_first, s);
         return fail(EBEM_ERR_NOMEM, "post-processing workspace allocation failed");
     }
     cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_nh, nh.data(), ntimes * sizeof(int), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_taus, uniq.data(), nu * sizeof(double), cudaMemcpyHostToDevice, s);
     cudaError_t e = cudaSuccess;
-    for (int p0 = 0; p0 < npts && e == cudaSuccess; p0 += chunk) {
+    int rc = EBEM_OK;
+    for (int p0 = 0; p0 < npts && e == cudaSuccess && rc == EBEM_OK; p0 += chunk) {
         const int np = std::min(chunk, npts - p0);
-        const long long lv = (long long)m.nt * np * nu;
-        pp_inst_level_kernel<<<(unsigned)((lv + 127) / 128), 128, 0, s>>>(m.d_geo, m.nt, d_pts, p0, np, nu, d_taus,
-                                                                         P.velP, P.velS, 4 * kPi * P.rho, Mbuf);
+        const long long rows = (long long)m.nt * np;
+        pp_inst_count_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(m.d_geo, m.nt, d_pts, p0, np, nu, d_taus,
+                                                                           P.velP, d_cnt, d_first);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) break;
+        rc = exclusive_scan(d_cnt, rows + 1, s);
+        if (rc) break;
+        long long total = 0;
+        e = cudaMemcpyAsync(&total, d_cnt + rows, sizeof(long long), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) break;
+        if (total > 0)
+            pp_inst_level_kernel<<<(unsigned)((total + 127) / 128), 128, 0, s>>>(
+                m.d_geo, m.nt, d_pts, p0, np, nu, d_taus, P.velP, P.velS, 4 * kPi * P.rho, d_cnt, d_first, total, Mbuf);
         pp_inst_sum_kernel<<<(unsigned)((long long)ntimes * np), 128, 0, s>>>(Mbuf, m.d_geo, m.nt, d_pts, p0, np, nu,
                                                                               d_taus, P.velP, d_tab, kmax, d_nh, npts,
                                                                               d_phi, d_u);
@@ -816,6 +876,9 @@ static int launch_pp_sa_shared(const MeshData& m, const PhysParams& P, const dou
     ws_free(d_taus, s);
     ws_free(d_tab, s);
     ws_free(d_nh, s);
+    ws_free(d_cnt, s);
+    ws_free(d_first, s);
+    if (rc) return rc;
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(EBEM_ERR_CUDA, std::string("post-processing kernels: ") + cudaGetErrorString(e));
     return EBEM_OK;
