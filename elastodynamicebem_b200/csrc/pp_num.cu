@@ -135,8 +135,10 @@ __device__ __forceinline__ void sym_apply(double acc[3], const double* M, const 
     acc[2] += M[2] * d[0] + M[4] * d[1] + M[5] * d[2];
 }
 
-// One block per (time q, point pl): the time sum of the variant.
-__global__ void __launch_bounds__(128) pp_num_sum_kernel(const double* __restrict__ Mbuf, int N, int p0, int np,
+// One block per (time q, point pl): the time sum of the variant.  Blocks of
+// 128 threads, or of 1024 when there are too few (time, point) pairs to
+// fill the GPU (one point at its 40 times: 40 blocks).
+__global__ void __launch_bounds__(1024) pp_num_sum_kernel(const double* __restrict__ Mbuf, int N, int p0, int np,
                                                          int nu, const int* __restrict__ tab, int kmax,
                                                          const int* __restrict__ nhat, int npts,
                                                          const double* __restrict__ phi, int layer,
@@ -172,7 +174,7 @@ __global__ void __launch_bounds__(128) pp_num_sum_kernel(const double* __restric
             }
         }
     }
-    __shared__ double red[3][4];
+    __shared__ double red[3][32];
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -254,13 +256,16 @@ int launch_pp_num(const MeshData& m, const PhysParams& P, int n_sub, int n_sing,
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_rule + nodes.size(), w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, s);
     const size_t shmem = (nodes.size() + w.size()) * sizeof(double);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
     for (int p0 = 0; p0 < npts && e == cudaSuccess; p0 += chunk) {
         const int np = std::min(chunk, npts - p0);
         const long long lv = (long long)m.nt * np * nu;
         pp_num_level_kernel<<<(unsigned)((lv + 127) / 128), 128, shmem, s>>>(
             m.d_coords, m.d_tris, m.d_geo, m.nt, d_pts, p0, np, nu, d_taus, d_rule, d_rule + nodes.size(), n_sub,
             n_sing, stride, layer, P.velP, P.velS, 4 * kPi * P.rho, Mbuf);
-        pp_num_sum_kernel<<<(unsigned)((long long)ntimes * np), 128, 0, s>>>(Mbuf, m.nt, p0, np, nu, d_tab, kmax,
+        const int sum_threads = ((long long)ntimes * np < 2LL * sms) ? 1024 : 128;
+        pp_num_sum_kernel<<<(unsigned)((long long)ntimes * np), sum_threads, 0, s>>>(Mbuf, m.nt, p0, np, nu, d_tab, kmax,
                                                                              d_nh, npts, d_phi, layer, d_u);
         e = cudaGetLastError();
     }
