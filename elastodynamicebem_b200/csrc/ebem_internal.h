@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -41,6 +42,27 @@ template <class T>
 cudaError_t ws_malloc(T** p, size_t bytes, cudaStream_t s) {
     return ws_malloc(reinterpret_cast<void**>(p), bytes, s);
 }
+
+// Several small host tables uploaded as one workspace block with one copy
+// (each table on a 16-byte boundary): a call that needs a handful of them
+// then pays one allocation and one host-to-device copy instead of one each.
+struct HostPack {
+    std::vector<unsigned char> bytes;
+    // appends n bytes from p; returns the table's byte offset in the block
+    size_t add(const void* p, size_t n) {
+        const size_t o = (bytes.size() + 15) & ~(size_t)15;
+        bytes.resize(o + n);
+        if (n) std::memcpy(bytes.data() + o, p, n);
+        return o;
+    }
+    // device copy on stream s into a new workspace block (ws_free it)
+    cudaError_t upload(unsigned char** d, cudaStream_t s) const {
+        cudaError_t e = ws_malloc(d, bytes.size() ? bytes.size() : 16, s);
+        if (e == cudaSuccess && !bytes.empty())
+            e = cudaMemcpyAsync(*d, bytes.data(), bytes.size(), cudaMemcpyHostToDevice, s);
+        return e;
+    }
+};
 
 #define EBEM_CUDA_TRY(expr)                                                        \
     do {                                                                           \

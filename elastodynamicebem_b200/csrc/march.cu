@@ -744,7 +744,9 @@ __global__ void __launch_bounds__(128, 6) pp_inst_level_kernel(const TriGeom* __
     for (int e = 0; e < 6; e++) dst[e] = M[e];
 }
 
-__global__ void __launch_bounds__(128) pp_inst_sum_kernel(const double* __restrict__ Mbuf, const TriGeom* __restrict__ geo,
+// Blocks of 128 threads, or of 1024 when there are too few (time, point)
+// pairs to fill the GPU.
+__global__ void __launch_bounds__(1024) pp_inst_sum_kernel(const double* __restrict__ Mbuf, const TriGeom* __restrict__ geo,
                                                           int N, const double* __restrict__ pts, int p0, int np, int nu,
                                                           const double* __restrict__ taus, double velP,
                                                           const int* __restrict__ tab, int kmax,
@@ -776,7 +778,7 @@ __global__ void __launch_bounds__(128) pp_inst_sum_kernel(const double* __restri
             sym_mv_add(acc, Ml, d, 1.0);
         }
     }
-    __shared__ double red[3][4];
+    __shared__ double red[3][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -830,25 +832,30 @@ static int launch_pp_sa_shared(const MeshData& m, const PhysParams& P, const dou
     }
     const size_t per_point = (size_t)nu * m.nt * 6 * sizeof(double);
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)npts, ((size_t)1 << 30) / per_point));
-    int *d_tab = nullptr, *d_nh = nullptr, *d_first = nullptr;
-    double *d_taus = nullptr, *Mbuf = nullptr;
+    // the tables in one upload: instants, index table, nHat
+    HostPack pk;
+    const size_t o_taus = pk.add(uniq.data(), nu * sizeof(double));
+    const size_t o_tab = pk.add(tab.data(), tab.size() * sizeof(int));
+    const size_t o_nh = pk.add(nh.data(), ntimes * sizeof(int));
+    unsigned char* d_pack = nullptr;
+    int* d_first = nullptr;
+    double* Mbuf = nullptr;
     long long* d_cnt = nullptr;
     const long long rows_max = (long long)m.nt * chunk;
-    if (ws_malloc(&d_tab, tab.size() * sizeof(int), s) != cudaSuccess ||
-        ws_malloc(&d_nh, ntimes * sizeof(int), s) != cudaSuccess ||
-        ws_malloc(&d_taus, nu * sizeof(double), s) != cudaSuccess ||
+    if (pk.upload(&d_pack, s) != cudaSuccess ||
         ws_malloc(&d_cnt, (rows_max + 1) * sizeof(long long), s) != cudaSuccess ||
         ws_malloc(&d_first, rows_max * sizeof(int), s) != cudaSuccess || ws_malloc(&Mbuf, per_point * chunk, s) != cudaSuccess) {
-        ws_free(d_tab, s);
-        ws_free(d_nh, s);
-        ws_free(d_taus, s);
+        cudaGetLastError();
+        ws_free(d_pack, s);
         ws_free(d_cnt, s);
         ws_free(d_first, s);
         return fail(EBEM_ERR_NOMEM, "post-processing workspace allocation failed");
     }
-    cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_nh, nh.data(), ntimes * sizeof(int), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_taus, uniq.data(), nu * sizeof(double), cudaMemcpyHostToDevice, s);
+    const double* d_taus = reinterpret_cast<const double*>(d_pack + o_taus);
+    const int* d_tab = reinterpret_cast<const int*>(d_pack + o_tab);
+    const int* d_nh = reinterpret_cast<const int*>(d_pack + o_nh);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
     cudaError_t e = cudaSuccess;
     int rc = EBEM_OK;
     for (int p0 = 0; p0 < npts && e == cudaSuccess && rc == EBEM_OK; p0 += chunk) {
@@ -867,15 +874,13 @@ static int launch_pp_sa_shared(const MeshData& m, const PhysParams& P, const dou
         if (total > 0)
             pp_inst_level_kernel<<<(unsigned)((total + 127) / 128), 128, 0, s>>>(
                 m.d_geo, m.nt, d_pts, p0, np, nu, d_taus, P.velP, P.velS, 4 * kPi * P.rho, d_cnt, d_first, total, Mbuf);
-        pp_inst_sum_kernel<<<(unsigned)((long long)ntimes * np), 128, 0, s>>>(Mbuf, m.d_geo, m.nt, d_pts, p0, np, nu,
-                                                                              d_taus, P.velP, d_tab, kmax, d_nh, npts,
-                                                                              d_phi, d_u);
+        const int sum_threads = ((long long)ntimes * np < 2LL * sms) ? 1024 : 128;
+        pp_inst_sum_kernel<<<(unsigned)((long long)ntimes * np), sum_threads, 0, s>>>(
+            Mbuf, m.d_geo, m.nt, d_pts, p0, np, nu, d_taus, P.velP, d_tab, kmax, d_nh, npts, d_phi, d_u);
         e = cudaGetLastError();
     }
     ws_free(Mbuf, s);
-    ws_free(d_taus, s);
-    ws_free(d_tab, s);
-    ws_free(d_nh, s);
+    ws_free(d_pack, s);
     ws_free(d_cnt, s);
     ws_free(d_first, s);
     if (rc) return rc;

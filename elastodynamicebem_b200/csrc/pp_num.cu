@@ -235,26 +235,26 @@ int launch_pp_num(const MeshData& m, const PhysParams& P, int n_sub, int n_sing,
         return fail(EBEM_ERR_INVALID, "inner rule: n_sub in {1,4,16,64}, n_sing in {1,3,7,12,19}");
     const size_t per_point = (size_t)nu * m.nt * 6 * sizeof(double);
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)npts, ((size_t)1 << 30) / per_point));
-    int *d_tab = nullptr, *d_nh = nullptr;
-    double *d_taus = nullptr, *Mbuf = nullptr, *d_rule = nullptr;
-    if (ws_malloc(&d_tab, tab.size() * sizeof(int), s) != cudaSuccess ||
-        ws_malloc(&d_nh, ntimes * sizeof(int), s) != cudaSuccess ||
-        ws_malloc(&d_taus, nu * sizeof(double), s) != cudaSuccess ||
-        ws_malloc(&d_rule, (nodes.size() + w.size()) * sizeof(double), s) != cudaSuccess ||
-        ws_malloc(&Mbuf, per_point * chunk, s) != cudaSuccess) {
-        ws_free(d_tab, s);
-        ws_free(d_nh, s);
-        ws_free(d_taus, s);
-        ws_free(d_rule, s);
+    // the tables in one upload: instants, rule nodes and weights, index table, nHat
+    HostPack pk;
+    const size_t o_taus = pk.add(uniq.data(), nu * sizeof(double));
+    std::vector<double> rule(nodes);                        // the nodes, then the weights
+    rule.insert(rule.end(), w.begin(), w.end());
+    const size_t o_nodes = pk.add(rule.data(), rule.size() * sizeof(double));
+    const size_t o_tab = pk.add(tab.data(), tab.size() * sizeof(int));
+    const size_t o_nh = pk.add(nh.data(), ntimes * sizeof(int));
+    unsigned char* d_pack = nullptr;
+    double* Mbuf = nullptr;
+    cudaError_t e = pk.upload(&d_pack, s);
+    if (e != cudaSuccess || ws_malloc(&Mbuf, per_point * chunk, s) != cudaSuccess) {
+        cudaGetLastError();
+        ws_free(d_pack, s);
         return fail(EBEM_ERR_NOMEM, "post-processing workspace allocation failed");
     }
-    cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_nh, nh.data(), ntimes * sizeof(int), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_taus, uniq.data(), nu * sizeof(double), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_rule, nodes.data(), nodes.size() * sizeof(double), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_rule + nodes.size(), w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+    const double* d_taus = reinterpret_cast<const double*>(d_pack + o_taus);
+    const double* d_rule = reinterpret_cast<const double*>(d_pack + o_nodes);
+    const int* d_tab = reinterpret_cast<const int*>(d_pack + o_tab);
+    const int* d_nh = reinterpret_cast<const int*>(d_pack + o_nh);
     const size_t shmem = (nodes.size() + w.size()) * sizeof(double);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device);
@@ -270,10 +270,7 @@ int launch_pp_num(const MeshData& m, const PhysParams& P, int n_sub, int n_sing,
         e = cudaGetLastError();
     }
     ws_free(Mbuf, s);
-    ws_free(d_rule, s);
-    ws_free(d_taus, s);
-    ws_free(d_tab, s);
-    ws_free(d_nh, s);
+    ws_free(d_pack, s);
     if (e != cudaSuccess)
         return fail(EBEM_ERR_CUDA, std::string("numerical post-processing kernels: ") + cudaGetErrorString(e));
     return EBEM_OK;
