@@ -134,6 +134,23 @@ def test_pp_grid_and_off_grid_times(ebem, oracle):
         assert rel(u, uo) <= 1e-9
 
 
+def test_pp_sphere1280_point_chunks(ebem, oracle):
+    """The benchmark sphere's 256 exterior points at its 40 grid times: the
+    instant path runs in two chunks of points (its buffer is capped at
+    1 GiB: 151 points of 1280 triangles x 115 instants), and 97 % of the
+    (triangle, point, instant) items lie before the P front and are skipped.
+    Points on both sides of the chunk boundary against the oracle."""
+    from elastodynamicebem_b200 import problem
+    w = problem.sphere_workload(7)
+    dm = ebem.DeviceMesh(w.mesh)
+    phi, L = ebem.timemarch_sa(dm, w.params, 7, w.datum)
+    u = ebem.pp_sa(dm, w.params, phi, w.points, w.times).cpu().numpy()          # (times, points, 3)
+    sel = [0, 77, 150, 151, 152, 255]
+    uo = oracle.pp_sa(w.mesh, w.params, phi.cpu().numpy().T, w.points[sel], w.times).transpose(2, 1, 0)
+    assert np.isfinite(u).all()
+    assert rel(u[:, sel], uo) <= 1e-9
+
+
 def test_workspace_pool_reuse_and_release(ebem, oracle):
     """Per-call workspaces come from the library's stream-ordered pool: repeated
     calls reuse it, ebem_release_workspace hands it back, and calls after the
