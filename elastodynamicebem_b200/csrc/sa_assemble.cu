@@ -328,8 +328,13 @@ __device__ __forceinline__ void store_entry(const SAArgs& A, int q, int i, int j
 // gained, and the results then depend on how pairs fall into groups (a
 // source-row sub-panel no longer reproduces the full assembly bit for bit).
 
+// Levels per chunk (per-level sums in shared memory).  24 rather than 48:
+// the 4 warps' sums take 5.4 KB less shared memory per block, which leaves
+// the 3 blocks per SM a larger L1 for the kernel's stack and loads (sphere
+// N=1280, L=40: 163.5 -> 160.2 ms per step, two A/B rounds on one box; 16
+// levels gave 163.2 ms: the chunks' set-up then costs what L1 gains).
 #ifndef EBEM_LEVEL_KC
-#define EBEM_LEVEL_KC 48         // levels per chunk (per-level sums in shared memory)
+#define EBEM_LEVEL_KC 24
 #endif
 #ifndef EBEM_LEVEL_WPB
 #define EBEM_LEVEL_WPB 4
