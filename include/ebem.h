@@ -330,8 +330,8 @@ int ebem_march(const double* E, int n3, int L, const double* rhs, int nT, double
 
 /* ebem_march with a choice of factorisation of E_0.  EBEM_FACTOR_LU is the
  * reference's lu with partial pivoting (BEMenerg_coreSA_timeMarching.m:46);
- * EBEM_FACTOR_CHOLESKY factors the symmetric part (E_0 + E_0^T) / 2, the
- * north star's "E_0 Cholesky factorisation": E_0 of the semi-analytic
+ * EBEM_FACTOR_CHOLESKY factors the symmetric part (E_0 + E_0^T) / 2 by
+ * Cholesky (half the work of the LU): E_0 of the semi-analytic
  * assembly (outer quadrature, exact inner integral) is not exactly symmetric,
  * so the two differ by the asymmetry's effect on the density.  Returns
  * EBEM_ERR_SINGULAR when the symmetric part is not positive definite. */

@@ -172,7 +172,7 @@ def test_workspace_pool_reuse_and_release(ebem, oracle):
 
 
 def test_cholesky_of_symmetric_part(ebem, oracle):
-    """The north star's Cholesky factorisation of E_0: it factors the
+    """A Cholesky factorisation of E_0 beside the LU: it factors the
     symmetric part (E_0 + E_0^T) / 2 (E_0 of the outer-quadrature /
     exact-inner assembly is not symmetric: 8.0e-3 relative on this mesh), and
     the marching with it equals a float64 numpy marching with that symmetric
