@@ -42,10 +42,10 @@ FLOPS_PER_PAIR_INTEGRAL_REF_SCHEDULE = 53_560.0
 # DRAM bytes (read + write) of the dominant kernel, the level pass of the
 # two-pass assembly (sa_level_kernel storing F(t_k) of every pair and level):
 # ncu on the sphere N=320 case (2,478,740 pair-integrals, one launch) measured
-# 13.07 MB read + 105.22 MB written; the writes are the stored levels, which
+# 11.78 MB read + 105.78 MB written; the writes are the stored levels, which
 # grow with the pair-integrals, so a launch's traffic is scaled by the
 # pair-integrals it processes.
-NCU_LEVEL_PASS_BYTES_N320 = 13.068032e6 + 105.216256e6
+NCU_LEVEL_PASS_BYTES_N320 = 11.780352e6 + 105.780480e6
 NCU_LEVEL_PASS_UNITS_N320 = 2_478_740
 
 
